@@ -1,0 +1,337 @@
+/* hj_oracle.c -- CPU oracle for the epsilon-join cardinality path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This file is the checker that the GPU engine is
+ * compared against. Only tests/, __graft_entry__.smoke() and bench.py's
+ * cpu_baseline leg may load it. The engine under hilbertjoin_b200/ never
+ * links, loads or calls it, and has no CPU fallback.
+ *
+ * It restates, in plain C, the algorithm of the hilbertJoin reference
+ * (perdacherMartin/hilbertJoin) for the count path:
+ *
+ *   - cell of a coordinate: floor(x / eps) in FP64, as epsilonGridCompare
+ *     does (hilbertjoin/egojoin.cpp:9-17);
+ *   - epsilon-grid order (EGO): lexicographic order of the cell vectors, dim 0
+ *     most significant (hilbertjoin/egojoin.cpp:159-168). The reference sorts
+ *     with an unstable parallel quicksort (egojoin.cpp:594-634); this oracle
+ *     sorts stably (ties keep input order), which is the order the GPU engine
+ *     produces, so permutations can be compared exactly;
+ *   - stripes: per point, contiguous ranges of the EGO order that can hold its
+ *     neighbours, one per combination of neighbour cells in the first
+ *     `active_dims` dimensions (prepareStripes, egojoin.cpp:270-464, and
+ *     prepareStripesNoSelf, egojoin.cpp:1126-1240). Two deliberate fixes: the
+ *     upper bound is inclusive (the reference's "first >=" search at
+ *     egojoin.cpp:408-412 excludes the cell of x+eps itself), and the
+ *     displacement is widened from eps to eps' = eps + 2^-40 (eps + max|x|), so
+ *     the ranges provably contain every pair the FP64 test accepts even when
+ *     floor(x/eps) jitters at cell borders;
+ *   - the pair test: the reference evaluates (eps^2 - |a-b|^2)/2 by norm
+ *     expansion and counts a pair when its sign bit is clear
+ *     (egojoin.h:329-392, egojoin.cpp:803-813), i.e. |a-b|^2 <= eps^2,
+ *     inclusive. This oracle -- and the engine's plain FP64 form -- evaluate
+ *     |a-b|^2 by direct difference: acc = fma(a_k - b_k, a_k - b_k, acc) for
+ *     k = 0..d-1 in FP64, and count iff acc <= eps*eps (FP64). On continuous
+ *     data both agree; on exact ties at eps the direct difference is the
+ *     defined semantics of this engine;
+ *   - count convention: self-join counts unordered pairs {a,b}, a != b
+ *     (the diagonal mask at egojoin.h:383-392); the two-set join counts ordered
+ *     pairs (a in A, b in B) (EGO_LOOP_TRAN_NOSELF, egojoin.h:482-553). The
+ *     reference only looks at the first 8*floor(n/8) EGO-sorted points of each
+ *     set (its loops run over floor(n/8) blocks); `tail_drop` reproduces that.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define HJO_EXPORT __attribute__((visibility("default")))
+
+/* The pair test, shared by every counting routine below. */
+static inline double dist2(const double *a, const double *b, uint32_t d) {
+    double acc = 0.0;
+    for (uint32_t k = 0; k < d; ++k) {
+        double df = a[k] - b[k];
+        acc = fma(df, df, acc);
+    }
+    return acc;
+}
+
+HJO_EXPORT double hjo_dist2(const double *a, const double *b, uint32_t d) { return dist2(a, b, d); }
+
+HJO_EXPORT double hjo_eps_wide(double eps, double maxabs) {
+    return eps + ldexp(eps + maxabs, -40);
+}
+
+static void set_threads(int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+}
+
+/* Brute-force self-join over all i < j. The inner loop runs over 8 partners j at
+ * a time against a transposed copy, so each pair keeps the exact sequential
+ * fma order while the compiler vectorises across pairs. */
+HJO_EXPORT uint64_t hjo_self_count_brute(const double *X, uint64_t n, uint32_t d, double eps, int nthreads) {
+    const double T = eps * eps;
+    set_threads(nthreads);
+    uint64_t npad = (n + 7) / 8 * 8;
+    double *XT = (double *)calloc((size_t)npad * d + 8, sizeof(double));
+    for (uint64_t i = 0; i < n; ++i)
+        for (uint32_t k = 0; k < d; ++k) XT[(size_t)k * npad + i] = X[(size_t)i * d + k];
+    uint64_t total = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : total)
+    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
+        uint64_t i = (uint64_t)ii, cnt = 0;
+        const double *a = X + (size_t)i * d;
+        uint64_t j0 = (i + 1) / 8 * 8;
+        for (uint64_t jb = j0; jb < n; jb += 8) {
+            double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (uint32_t k = 0; k < d; ++k) {
+                const double ak = a[k];
+                const double *bt = XT + (size_t)k * npad + jb;
+                for (int l = 0; l < 8; ++l) {
+                    double df = ak - bt[l];
+                    acc[l] = fma(df, df, acc[l]);
+                }
+            }
+            for (int l = 0; l < 8; ++l) {
+                uint64_t j = jb + (uint64_t)l;
+                if (j > i && j < n && acc[l] <= T) ++cnt;
+            }
+        }
+        total += cnt;
+    }
+    free(XT);
+    return total;
+}
+
+/* Brute-force two-set join: ordered pairs (a in A, b in B). */
+HJO_EXPORT uint64_t hjo_join_count_brute(const double *A, uint64_t nA, const double *B, uint64_t nB, uint32_t d,
+                                        double eps, int nthreads) {
+    const double T = eps * eps;
+    set_threads(nthreads);
+    uint64_t npad = (nB + 7) / 8 * 8;
+    double *BT = (double *)calloc((size_t)npad * d + 8, sizeof(double));
+    for (uint64_t i = 0; i < nB; ++i)
+        for (uint32_t k = 0; k < d; ++k) BT[(size_t)k * npad + i] = B[(size_t)i * d + k];
+    uint64_t total = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : total)
+    for (int64_t ii = 0; ii < (int64_t)nA; ++ii) {
+        uint64_t cnt = 0;
+        const double *a = A + (size_t)ii * d;
+        for (uint64_t jb = 0; jb < nB; jb += 8) {
+            double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (uint32_t k = 0; k < d; ++k) {
+                const double ak = a[k];
+                const double *bt = BT + (size_t)k * npad + jb;
+                for (int l = 0; l < 8; ++l) {
+                    double df = ak - bt[l];
+                    acc[l] = fma(df, df, acc[l]);
+                }
+            }
+            for (int l = 0; l < 8; ++l)
+                if (jb + (uint64_t)l < nB && acc[l] <= T) ++cnt;
+        }
+        total += cnt;
+    }
+    free(BT);
+    return total;
+}
+
+/* Per-row neighbour counts (all partners j != i in the same set) for a list of
+ * rows: lets a test check a sample of rows at sizes where the full brute force
+ * would take too long. */
+HJO_EXPORT void hjo_self_row_counts(const double *X, uint64_t n, uint32_t d, double eps, const uint64_t *rows,
+                                    uint64_t nrows, uint64_t *out, int nthreads) {
+    const double T = eps * eps;
+    set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t r = 0; r < (int64_t)nrows; ++r) {
+        uint64_t i = rows[r], cnt = 0;
+        for (uint64_t j = 0; j < n; ++j)
+            if (j != i && dist2(X + (size_t)i * d, X + (size_t)j * d, d) <= T) ++cnt;
+        out[r] = cnt;
+    }
+}
+
+/* ---------------------------------------------------------------- EGO order */
+
+HJO_EXPORT void hjo_cells(const double *X, uint64_t n, uint32_t d, double eps, double *cells) {
+    for (uint64_t i = 0; i < n * (uint64_t)d; ++i) cells[i] = floor(X[i] / eps);
+}
+
+typedef struct {
+    const double *cells;
+    uint32_t d;
+} ego_ctx;
+
+static int cmp_vec(const double *a, const double *b, uint32_t d) {
+    for (uint32_t t = 0; t < d; ++t) {
+        if (a[t] < b[t]) return -1;
+        if (a[t] > b[t]) return 1;
+    }
+    return 0;
+}
+
+/* Stable merge sort of indices by cell vector. */
+static void merge_sort_idx(uint64_t *idx, uint64_t *tmp, uint64_t n, const ego_ctx *c) {
+    for (uint64_t w = 1; w < n; w *= 2) {
+        for (uint64_t lo = 0; lo < n; lo += 2 * w) {
+            uint64_t mid = lo + w < n ? lo + w : n, hi = lo + 2 * w < n ? lo + 2 * w : n;
+            uint64_t i = lo, j = mid, o = lo;
+            while (i < mid && j < hi) {
+                if (cmp_vec(c->cells + idx[j] * c->d, c->cells + idx[i] * c->d, c->d) < 0)
+                    tmp[o++] = idx[j++];
+                else
+                    tmp[o++] = idx[i++];
+            }
+            while (i < mid) tmp[o++] = idx[i++];
+            while (j < hi) tmp[o++] = idx[j++];
+        }
+        memcpy(idx, tmp, n * sizeof(uint64_t));
+    }
+}
+
+/* perm[r] = input index of the point at EGO rank r (stable). */
+HJO_EXPORT void hjo_ego_order(const double *X, uint64_t n, uint32_t d, double eps, uint64_t *perm) {
+    double *cells = (double *)malloc(sizeof(double) * n * d + 8);
+    hjo_cells(X, n, d, eps, cells);
+    uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * n + 8);
+    for (uint64_t i = 0; i < n; ++i) perm[i] = i;
+    ego_ctx c = {cells, d};
+    merge_sort_idx(perm, tmp, n, &c);
+    free(tmp);
+    free(cells);
+}
+
+/* --------------------------------------------------------------- stripes */
+
+/* First rank r in [0,n) whose cell vector is >= q (strict=0) or > q (strict=1). */
+static uint64_t search(const double *sc, uint64_t n, uint32_t d, const double *q, int strict) {
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint64_t mid = lo + (hi - lo) / 2;
+        int c = cmp_vec(sc + mid * d, q, d);
+        if (c < 0 || (strict && c == 0))
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+/* Neighbour-cell bounds of one point: lo_t = cell(x_t - eps'), hi_t = cell(x_t + eps'). */
+static void point_bounds(const double *x, uint32_t d, double eps, double epsw, double *lo, double *hi) {
+    for (uint32_t t = 0; t < d; ++t) {
+        lo[t] = floor((x[t] - epsw) / eps);
+        hi[t] = floor((x[t] + epsw) / eps);
+    }
+}
+
+/* Counts via EGO order + stripes + the FP64 pair test. B is sorted once; for
+ * every point a of A, each combination of neighbour cells over the first
+ * k = active_dims dimensions gives one range [first >= (v, lo_k..), first >
+ * (v, hi_k..)) of B's EGO order (the stripe of that combination). The ranges
+ * of one point are disjoint because their first k cells differ. For a
+ * self-join only partners at a later EGO rank are taken. Returns the count and
+ * the number of candidate pairs tested (the work the stripes leave). */
+static uint64_t ego_count(const double *A, uint64_t nA, const double *B, uint64_t nB, uint32_t d, double eps,
+                          int active_dims, int self, uint64_t tail_drop, uint64_t *candidates) {
+    const double T = eps * eps;
+    double maxabs = 0.0;
+    for (uint64_t i = 0; i < nA * (uint64_t)d; ++i) maxabs = fmax(maxabs, fabs(A[i]));
+    for (uint64_t i = 0; i < nB * (uint64_t)d; ++i) maxabs = fmax(maxabs, fabs(B[i]));
+    const double epsw = hjo_eps_wide(eps, maxabs);
+
+    uint64_t *pb = (uint64_t *)malloc(sizeof(uint64_t) * nB + 8);
+    hjo_ego_order(B, nB, d, eps, pb);
+    double *sb = (double *)malloc(sizeof(double) * nB * d + 8); /* sorted B rows */
+    double *sc = (double *)malloc(sizeof(double) * nB * d + 8); /* sorted B cells */
+    for (uint64_t r = 0; r < nB; ++r) {
+        memcpy(sb + r * d, B + pb[r] * d, sizeof(double) * d);
+        for (uint32_t t = 0; t < d; ++t) sc[r * d + t] = floor(sb[r * d + t] / eps);
+    }
+    uint64_t *pa = pb;
+    const double *sa = sb;
+    double *sa_own = 0;
+    uint64_t *pa_own = 0;
+    if (!self) {
+        pa_own = (uint64_t *)malloc(sizeof(uint64_t) * nA + 8);
+        hjo_ego_order(A, nA, d, eps, pa_own);
+        sa_own = (double *)malloc(sizeof(double) * nA * d + 8);
+        for (uint64_t r = 0; r < nA; ++r) memcpy(sa_own + r * d, A + pa_own[r] * d, sizeof(double) * d);
+        pa = pa_own;
+        sa = sa_own;
+    }
+    uint64_t na_eff = nA, nb_eff = nB;
+    if (tail_drop) {
+        na_eff = nA / 8 * 8;
+        nb_eff = nB / 8 * 8;
+    }
+    uint32_t k = (uint32_t)active_dims < d ? (uint32_t)active_dims : d;
+    uint64_t total = 0, cand = 0;
+#pragma omp parallel reduction(+ : total, cand)
+    {
+        double *lo = (double *)malloc(sizeof(double) * d), *hi = (double *)malloc(sizeof(double) * d);
+        double *ql = (double *)malloc(sizeof(double) * d), *qh = (double *)malloc(sizeof(double) * d);
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t ii = 0; ii < (int64_t)na_eff; ++ii) {
+            const double *a = sa + (uint64_t)ii * d;
+            point_bounds(a, d, eps, epsw, lo, hi);
+            /* A combination only splits dims whose neighbour set is <= 3 cells wide
+             * (always, unless floor(x/eps) jitters); the first wider dim and all
+             * later ones stay ranges. */
+            uint32_t ke = 0;
+            while (ke < k && hi[ke] - lo[ke] <= 2.0) ++ke;
+            uint64_t ncomb = 1;
+            for (uint32_t t = 0; t < ke; ++t) ncomb *= (uint64_t)(hi[t] - lo[t] + 1.0);
+            for (uint64_t c = 0; c < ncomb; ++c) {
+                uint64_t rem = c;
+                for (int t = (int)ke - 1; t >= 0; --t) {
+                    uint64_t w = (uint64_t)(hi[t] - lo[t] + 1.0);
+                    ql[t] = qh[t] = lo[t] + (double)(rem % w);
+                    rem /= w;
+                }
+                for (uint32_t t = ke; t < d; ++t) {
+                    ql[t] = lo[t];
+                    qh[t] = hi[t];
+                }
+                uint64_t r0 = search(sc, nb_eff, d, ql, 0), r1 = search(sc, nb_eff, d, qh, 1);
+                if (self && r0 < (uint64_t)ii + 1) r0 = (uint64_t)ii + 1;
+                for (uint64_t r = r0; r < r1; ++r) {
+                    ++cand;
+                    if (dist2(a, sb + r * d, d) <= T) ++total;
+                }
+            }
+        }
+        free(lo);
+        free(hi);
+        free(ql);
+        free(qh);
+    }
+    if (candidates) *candidates = cand;
+    free(pb);
+    free(sb);
+    free(sc);
+    free(pa_own);
+    free(sa_own);
+    (void)pa;
+    return total;
+}
+
+HJO_EXPORT uint64_t hjo_self_count_ego(const double *X, uint64_t n, uint32_t d, double eps, int active_dims,
+                                      int tail_drop, int nthreads, uint64_t *candidates) {
+    set_threads(nthreads);
+    return ego_count(X, n, X, n, d, eps, active_dims, 1, (uint64_t)tail_drop, candidates);
+}
+
+HJO_EXPORT uint64_t hjo_join_count_ego(const double *A, uint64_t nA, const double *B, uint64_t nB, uint32_t d,
+                                      double eps, int active_dims, int tail_drop, int nthreads,
+                                      uint64_t *candidates) {
+    set_threads(nthreads);
+    return ego_count(A, nA, B, nB, d, eps, active_dims, 0, (uint64_t)tail_drop, candidates);
+}
