@@ -1,0 +1,662 @@
+// hj_engine.cu -- host side of the engine: per-thread device contexts, the
+// join pipeline (grid -> keys -> sort -> gather -> index -> distance kernels ->
+// count), and the C ABI of include/hj.h.
+//
+// The pipeline is the reference's test_ego_loop3_macro / test_ego_loop3_noself
+// (hilbertjoin/egojoin.cpp:777-838, :840-907) and its macros
+// EGO_PARALLEL_TRAN / EGO_PARALLEL_TRAN_NOSELF (hilbertjoin/egojoin.h:164-222,
+// :395-479) re-planned for one GPU: every stage is a device kernel on one
+// stream, the host only plans the key layout (after one small read-back of the
+// per-dimension cell ranges) and sizes the work list (one more read-back).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/hj.h"
+#include "hj_common.cuh"
+#include "hj_internal.h"
+
+namespace hj {
+
+thread_local std::string tl_error;
+
+static int fail(int code, const std::string &msg) {
+    tl_error = msg;
+    return code;
+}
+
+// ------------------------------------------------------------------ context
+
+struct Ctx {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+    std::vector<std::pair<void *, size_t>> slots;
+    cudaEvent_t ev[8] = {};
+    unsigned long long *d_small = nullptr;  // [16] counters
+    unsigned long long *h_small = nullptr;  // pinned [16]
+    bool ok = false;
+};
+
+static thread_local std::map<int, Ctx *> tl_ctx;
+
+static void *slot_alloc_impl(Ctx *c, cudaStream_t st, int slot, size_t bytes) {
+    if ((size_t)slot >= c->slots.size()) c->slots.resize(slot + 1, {nullptr, 0});
+    auto &s = c->slots[slot];
+    if (bytes == 0) bytes = 16;
+    if (s.second >= bytes) return s.first;
+    if (s.first) {
+        cudaStreamSynchronize(st);
+        cudaFree(s.first);
+        s.first = nullptr;
+        s.second = 0;
+    }
+    size_t cap = bytes + bytes / 8;
+    cap = (cap + 255) / 256 * 256;
+    void *p = nullptr;
+    if (cudaMalloc(&p, cap) != cudaSuccess) {
+        cudaGetLastError();
+        if (cudaMalloc(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        cap = bytes;
+    }
+    s.first = p;
+    s.second = cap;
+    return p;
+}
+
+struct AllocCtx {
+    Ctx *c;
+    cudaStream_t st;
+};
+static void *slot_alloc_cb(void *ctx, int slot, size_t bytes) {
+    AllocCtx *a = static_cast<AllocCtx *>(ctx);
+    return slot_alloc_impl(a->c, a->st, slot, bytes);
+}
+
+static int get_ctx(int device, Ctx **out) {
+    int dev = device;
+    if (dev < 0) {
+        if (cudaGetDevice(&dev) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(HJ_ERR_NO_DEVICE, "no CUDA device");
+        }
+    }
+    auto it = tl_ctx.find(dev);
+    if (it != tl_ctx.end() && it->second->ok) {
+        cudaSetDevice(dev);
+        *out = it->second;
+        return HJ_OK;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || dev >= ndev) {
+        cudaGetLastError();
+        return fail(HJ_ERR_NO_DEVICE, "no CUDA device");
+    }
+    cudaSetDevice(dev);
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, dev);
+    if (prop.major < 10) return fail(HJ_ERR_NO_DEVICE, "device is not sm_100 class (compute capability 10.x)");
+    Ctx *c = new Ctx();
+    c->device = dev;
+    c->num_sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return fail(HJ_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    for (auto &e : c->ev) cudaEventCreate(&e);
+    cudaMalloc(&c->d_small, 16 * sizeof(unsigned long long));
+    cudaMallocHost(&c->h_small, 16 * sizeof(unsigned long long));
+    if (!c->d_small || !c->h_small) return fail(HJ_ERR_OOM, "context allocation failed");
+    c->ok = true;
+    tl_ctx[dev] = c;
+    *out = c;
+    return HJ_OK;
+}
+
+// Slot ids (index-stage slots 40..49 live in hj_index.cu).
+enum {
+    kSlotInA = 1, kSlotInB, kSlotDimStats, kSlotGridOff, kSlotGridBits, kSlotGridWord, kSlotGridShift,
+    kSlotKeysWmA, kSlotKeysWmB, kSlotPermA, kSlotPermB, kSlotPermTmp, kSlotHist,
+    kSlotRowsA, kSlotRowsB, kSlotKeysA, kSlotKeysB, kSlotTilesA, kSlotTilesB,
+    kSlotTf32A, kSlotTf32B, kSlotHiA, kSlotLoA, kSlotHiB, kSlotLoB, kSlotNormA, kSlotNormB,
+    kSlotTmaxAA, kSlotTmaxAB, kSlotTmaxBA, kSlotTmaxBB, kSlotBand,
+};
+
+static int bitwidth(unsigned long long v) {
+    int b = 0;
+    while (b < 64 && (v >> b) != 0) ++b;
+    return b;
+}
+
+// Plans the packed key layout from the per-dim cell ranges.
+static int plan_grid(const std::vector<DimStats> &ds, uint32_t d, double eps, double maxabs, Grid *g) {
+    g->d = d;
+    g->eps = eps;
+    g->maxabs = maxabs;
+    g->eps_wide = eps + std::ldexp(eps + maxabs, -40);
+    g->off.resize(d);
+    g->bits.resize(d);
+    g->word.resize(d);
+    g->shift.resize(d);
+    g->range.resize(d);
+    uint32_t w = 0, left = 32;
+    for (uint32_t t = 0; t < d; ++t) {
+        long long lo = ds[t].cmin, hi = ds[t].cmax;
+        if (lo > hi) lo = hi = 0;  // empty set
+        long long range = hi - lo;
+        if (range < 0 || range > (1ll << 30)) return fail(HJ_ERR_INVALID_ARG,
+                                                           "eps too small for the coordinate range: more than 2^30 "
+                                                           "cells in one dimension");
+        uint32_t b = (uint32_t)bitwidth((unsigned long long)range + 4);
+        if (b > left) {
+            ++w;
+            left = 32;
+        }
+        g->off[t] = lo - 2;
+        g->bits[t] = b;
+        g->word[t] = w;
+        g->shift[t] = left - b;
+        g->range[t] = range;
+        left -= b;
+    }
+    g->W = w + 1;
+    // radix windows that can vary: word W-1 first (least significant), low bits first
+    g->passes.clear();
+    for (int ww = (int)g->W - 1; ww >= 0; --ww) {
+        for (uint32_t lowbit = 0; lowbit < 32; lowbit += 8) {
+            bool active = false;
+            for (uint32_t t = 0; t < d && !active; ++t) {
+                if ((int)g->word[t] != ww || g->range[t] == 0) continue;
+                uint32_t vb = (uint32_t)bitwidth((unsigned long long)g->range[t] + 2);
+                uint32_t f0 = g->shift[t], f1 = g->shift[t] + std::min(vb, g->bits[t]);
+                if (f0 < lowbit + 8 && f1 > lowbit) active = true;
+            }
+            if (active) g->passes.push_back({(uint32_t)ww, lowbit});
+        }
+    }
+    return HJ_OK;
+}
+
+struct JoinIn {
+    const void *a;  // device
+    const void *b;  // device (== a for self)
+    uint64_t na, nb;
+    int dtype_bytes;
+    uint32_t d;
+    double eps;
+    bool self;
+};
+
+static int form_is_tc(int f) { return f == HJ_FORM_TC_TF32 || f == HJ_FORM_TC_BF16X3; }
+
+static int check_cuda(const char *what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(HJ_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return HJ_OK;
+}
+
+static float ev_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+        cudaGetLastError();
+        return 0.f;
+    }
+    return ms;
+}
+
+// Sorts one set and gathers the layouts the chosen form needs.
+static int prepare_set(Ctx *c, cudaStream_t st, const void *x, uint64_t n, int dtype_bytes, const Grid &g,
+                       const GridDev &gd, int form, bool is_b, SortedSet *out, int *launches) {
+    SortedSet s;
+    s.n = n;
+    s.d = g.d;
+    s.dtype_bytes = dtype_bytes;
+    const uint32_t W = g.W;
+    uint32_t *keys_wm = (uint32_t *)slot_alloc_impl(c, st, is_b ? kSlotKeysWmB : kSlotKeysWmA, n * W * 4);
+    uint32_t *perm = (uint32_t *)slot_alloc_impl(c, st, is_b ? kSlotPermB : kSlotPermA, n * 4);
+    uint32_t *ptmp = (uint32_t *)slot_alloc_impl(c, st, kSlotPermTmp, n * 4);
+    uint32_t *hist = (uint32_t *)slot_alloc_impl(c, st, kSlotHist, radix_hist_entries(n) * 4);
+    s.keys = (uint32_t *)slot_alloc_impl(c, st, is_b ? kSlotKeysB : kSlotKeysA, n * W * 4);
+    s.rows = slot_alloc_impl(c, st, is_b ? kSlotRowsB : kSlotRowsA, n * g.d * dtype_bytes);
+    if (!keys_wm || !perm || !ptmp || !hist || !s.keys || !s.rows) return fail(HJ_ERR_OOM, "out of device memory");
+    s.perm = perm;
+    uint32_t flags = kGatherKeys | kGatherRows;
+    if (form == HJ_FORM_PLAIN_FP64) {
+        s.n_tiles64 = hj_ceil_div(n, kPlainTile);
+        s.tiles64 = (double *)slot_alloc_impl(c, st, is_b ? kSlotTilesB : kSlotTilesA,
+                                              s.n_tiles64 * g.d * kPlainTile * 8);
+        if (!s.tiles64) return fail(HJ_ERR_OOM, "out of device memory");
+        flags |= kGatherPlain;
+    } else {
+        s.npad_tc = hj_ceil_div(std::max<uint64_t>(n, 1), kTcTileB) * kTcTileB;
+        s.kpad_tf32 = (uint32_t)hj_ceil_div(g.d, 32) * 32;
+        s.kpad_bf16 = (uint32_t)hj_ceil_div(g.d, 64) * 64;
+        if (form == HJ_FORM_TC_TF32) {
+            s.tf32 = (float *)slot_alloc_impl(c, st, is_b ? kSlotTf32B : kSlotTf32A, s.npad_tc * s.kpad_tf32 * 4);
+            if (!s.tf32) return fail(HJ_ERR_OOM, "out of device memory");
+            flags |= kGatherTf32;
+        } else {
+            s.bf_hi = (uint16_t *)slot_alloc_impl(c, st, is_b ? kSlotHiB : kSlotHiA, s.npad_tc * s.kpad_bf16 * 2);
+            s.bf_lo = (uint16_t *)slot_alloc_impl(c, st, is_b ? kSlotLoB : kSlotLoA, s.npad_tc * s.kpad_bf16 * 2);
+            if (!s.bf_hi || !s.bf_lo) return fail(HJ_ERR_OOM, "out of device memory");
+            flags |= kGatherBf16;
+        }
+        s.norms = (float *)slot_alloc_impl(c, st, is_b ? kSlotNormB : kSlotNormA, s.npad_tc * 4);
+        s.tile_maxnorm_a = (float *)slot_alloc_impl(c, st, is_b ? kSlotTmaxBA : kSlotTmaxAA,
+                                                    (s.npad_tc / kTcTileA) * 4);
+        s.tile_maxnorm_b = (float *)slot_alloc_impl(c, st, is_b ? kSlotTmaxBB : kSlotTmaxAB,
+                                                    (s.npad_tc / kTcTileB) * 4);
+        if (!s.norms || !s.tile_maxnorm_a || !s.tile_maxnorm_b) return fail(HJ_ERR_OOM, "out of device memory");
+        flags |= kGatherNorms;
+    }
+    launch_pack_keys(x, dtype_bytes, n, g.d, g.eps, gd, W, keys_wm, st);
+    *launches += 1;
+    radix_sort_perm(keys_wm, n, g.passes, perm, ptmp, hist, st, launches);
+    launch_gather(x, dtype_bytes, n, g.d, perm, keys_wm, W, s, flags, st, launches);
+    *out = s;
+    return check_cuda("sort stage");
+}
+
+static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *count, hj_stats *stats,
+                    cudaEvent_t ev_h2d_start) {
+    cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
+    int form = opts ? opts->form : HJ_FORM_PLAIN_FP64;
+    int active_dims = opts ? opts->active_dims : -1;
+    const bool ref_compat = opts && opts->ref_compat;
+    if (active_dims < 0) active_dims = in.self ? 3 : 2;
+    if (active_dims > kMaxActiveDims) active_dims = kMaxActiveDims;
+    int launches = 0;
+    auto t_wall0 = std::chrono::steady_clock::now();
+    cudaEventRecord(c->ev[1], st);  // after H2D
+
+    const uint32_t d = in.d;
+    // 1. per-dim cell ranges (union of both sets), read back to plan the keys
+    DimStats *ds = (DimStats *)slot_alloc_impl(c, st, kSlotDimStats, d * sizeof(DimStats));
+    if (!ds) return fail(HJ_ERR_OOM, "out of device memory");
+    unsigned long long *d_maxabs = c->d_small + 0;
+    uint32_t *d_bad = reinterpret_cast<uint32_t *>(c->d_small + 1);
+    launch_dim_stats_init(ds, d, d_maxabs, d_bad, st);
+    launch_dim_stats(in.a, in.dtype_bytes, in.na, d, in.eps, ds, d_maxabs, d_bad, st);
+    launches += 2;
+    if (!in.self) {
+        launch_dim_stats(in.b, in.dtype_bytes, in.nb, d, in.eps, ds, d_maxabs, d_bad, st);
+        ++launches;
+    }
+    std::vector<DimStats> hds(d);
+    cudaMemcpyAsync(hds.data(), ds, d * sizeof(DimStats), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(c->h_small, c->d_small, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("cell statistics");
+    if (int r = check_cuda("cell statistics")) return r;
+    const uint32_t bad = (uint32_t)c->h_small[1];
+    if (bad & 1u) return fail(HJ_ERR_INVALID_ARG, "input holds a non-finite coordinate");
+    if (bad & 2u) return fail(HJ_ERR_INVALID_ARG, "a cell index floor(x/eps) exceeds 2^62");
+    double maxabs;
+    {
+        unsigned long long bits = c->h_small[0];
+        std::memcpy(&maxabs, &bits, 8);
+    }
+    if (form == HJ_FORM_AUTO) form = (d <= 256 && maxabs < 1e18) ? HJ_FORM_TC_TF32 : HJ_FORM_PLAIN_FP64;
+    if (form_is_tc(form) && d > 256) return fail(HJ_ERR_UNSUPPORTED, "tensor-core forms support d <= 256");
+    if (form_is_tc(form) && !(maxabs < 1e18)) return fail(HJ_ERR_UNSUPPORTED, "tensor-core forms need |x| < 1e18");
+    if (form == HJ_FORM_PLAIN_FP64 && d > 128) return fail(HJ_ERR_UNSUPPORTED, "plain FP64 form supports d <= 128");
+    Grid g;
+    if (int r = plan_grid(hds, d, in.eps, maxabs, &g)) return r;
+    GridDev gd;
+    gd.off = (long long *)slot_alloc_impl(c, st, kSlotGridOff, d * 8);
+    gd.bits = (uint32_t *)slot_alloc_impl(c, st, kSlotGridBits, d * 4);
+    gd.word = (uint32_t *)slot_alloc_impl(c, st, kSlotGridWord, d * 4);
+    gd.shift = (uint32_t *)slot_alloc_impl(c, st, kSlotGridShift, d * 4);
+    if (!gd.off || !gd.bits || !gd.word || !gd.shift) return fail(HJ_ERR_OOM, "out of device memory");
+    cudaMemcpyAsync(gd.off, g.off.data(), d * 8, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(gd.bits, g.bits.data(), d * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(gd.word, g.word.data(), d * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(gd.shift, g.shift.data(), d * 4, cudaMemcpyHostToDevice, st);
+
+    // 2. EGO sort + layouts
+    SortedSet A, B;
+    if (int r = prepare_set(c, st, in.a, in.na, in.dtype_bytes, g, gd, form, false, &A, &launches)) return r;
+    if (in.self) {
+        B = A;
+    } else if (int r = prepare_set(c, st, in.b, in.nb, in.dtype_bytes, g, gd, form, true, &B, &launches)) {
+        return r;
+    }
+    cudaEventRecord(c->ev[2], st);
+
+    // 3. index
+    uint64_t na_eff = in.na, nb_eff = in.nb;
+    if (ref_compat) {
+        na_eff = na_eff / 8 * 8;
+        nb_eff = nb_eff / 8 * 8;
+    }
+    const bool tc = form_is_tc(form);
+    const int tile_a = tc ? kTcTileA : kPlainTile, tile_b = tc ? kTcTileB : kPlainTile;
+    const uint32_t chunk = tc ? 32 : 16;
+    IndexResult idx;
+    AllocCtx actx{c, st};
+    std::string err;
+    int r = build_index(A, B, g, gd, in.self, na_eff, nb_eff, tile_a, tile_b, active_dims, chunk, slot_alloc_cb,
+                        &actx, st, &idx, &launches, &err);
+    if (r == 2) return fail(HJ_ERR_OOM, err);
+    if (r == 3) return fail(HJ_ERR_CUDA, err);
+    if (r) return fail(HJ_ERR_INVALID_ARG, err);
+    cudaEventRecord(c->ev[3], st);
+
+    // 4. distance kernels
+    unsigned long long *d_count = c->d_small + 2;
+    uint32_t *d_err = reinterpret_cast<uint32_t *>(c->d_small + 3);
+    unsigned long long *d_band = c->d_small + 4;
+    cudaMemsetAsync(c->d_small + 2, 0, 3 * sizeof(unsigned long long), st);
+    uint64_t band_total = 0;
+    double c_rel = 0, c_abs = 0;
+    if (!tc) {
+        launch_join_fp64(A, B, in.self, na_eff, nb_eff, in.eps * in.eps, idx, d_count, d_err, c->num_sms, st);
+        ++launches;
+        cudaEventRecord(c->ev[4], st);
+        cudaEventRecord(c->ev[5], st);
+    } else {
+        tc_band_constants(form, d, maxabs, &c_rel, &c_abs);
+        TcParams p{form, in.eps * in.eps, c_rel, c_abs};
+        uint64_t cap = std::max<uint64_t>(1ull << 20, idx.candidate_pairs / 4096);
+        for (int attempt = 0;; ++attempt) {
+            uint2 *band = (uint2 *)slot_alloc_impl(c, st, kSlotBand, cap * sizeof(uint2));
+            if (!band) return fail(HJ_ERR_OOM, "out of device memory (band queue)");
+            cudaMemsetAsync(c->d_small + 2, 0, 3 * sizeof(unsigned long long), st);
+            std::string terr;
+            if (launch_join_tc(A, B, in.self, na_eff, nb_eff, p, idx, d_count, band, cap, d_band, d_err, c->num_sms,
+                               st, &terr))
+                return fail(HJ_ERR_CUDA, terr);
+            ++launches;
+            cudaEventRecord(c->ev[4], st);
+            cudaMemcpyAsync(c->h_small + 4, d_band, 8, cudaMemcpyDeviceToHost, st);
+            if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("tensor-core join");
+            band_total = c->h_small[4];
+            if (band_total <= cap) {
+                launch_recheck(A, B, p.T, band, d_band, cap, d_count, st);
+                ++launches;
+                cudaEventRecord(c->ev[5], st);
+                break;
+            }
+            if (attempt >= 3) return fail(HJ_ERR_BAND_OVERFLOW, "band queue overflow");
+            cap = band_total + band_total / 4 + 1024;
+        }
+    }
+    cudaMemcpyAsync(c->h_small + 2, c->d_small + 2, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("distance kernel");
+    if (int rr = check_cuda("distance kernel")) return rr;
+    const uint32_t kerr = (uint32_t)c->h_small[3];
+    if (kerr & kErrTimeout) return fail(HJ_ERR_TIMEOUT, "a bounded device-side wait timed out");
+    if (kerr) return fail(HJ_ERR_CUDA, "device error word set");
+    *count = c->h_small[2];
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        if (ev_h2d_start) stats->h2d_ms = ev_ms(ev_h2d_start, c->ev[1]);
+        stats->sort_ms = ev_ms(c->ev[1], c->ev[2]);
+        stats->index_ms = ev_ms(c->ev[2], c->ev[3]);
+        stats->join_ms = ev_ms(c->ev[3], c->ev[4]);
+        stats->recheck_ms = ev_ms(c->ev[4], c->ev[5]);
+        stats->total_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_wall0).count() +
+            stats->h2d_ms;
+        double all = in.self ? (double)na_eff * (double)(na_eff > 0 ? na_eff - 1 : 0) / 2.0
+                             : (double)na_eff * (double)nb_eff;
+        stats->candidate_pairs = idx.candidate_pairs;
+        stats->tile_pairs = idx.tile_pairs;
+        stats->work_items = idx.n_items;
+        stats->loadpercent = all > 0 ? 100.0 * (double)idx.candidate_pairs / all : 0.0;
+        stats->band_pairs = band_total;
+        stats->band_fraction = idx.candidate_pairs ? (double)band_total / (double)idx.candidate_pairs : 0.0;
+        stats->band_halfwidth_rel = c_rel;
+        stats->form_used = form;
+        int s = active_dims;
+        int p3 = 1;
+        for (int i = 0; i < s; ++i) p3 *= 3;
+        stats->stripes = in.self ? (p3 + 1) / 2 : p3;
+        stats->kernel_launches = launches;
+    }
+    return HJ_OK;
+}
+
+static int validate(uint64_t na, uint64_t nb, uint32_t d, double eps) {
+    if (d == 0 || d > kMaxDim) return fail(HJ_ERR_INVALID_ARG, "d must be in [1, 1024]");
+    if (na >= (1ull << 31) || nb >= (1ull << 31)) return fail(HJ_ERR_INVALID_ARG, "n must be below 2^31");
+    if (!(eps > 0.0) || !std::isfinite(eps)) return fail(HJ_ERR_INVALID_ARG, "eps must be positive and finite");
+    return HJ_OK;
+}
+
+static int join_host(const void *a, uint64_t na, const void *b, uint64_t nb, int dtype_bytes, uint32_t d, double eps,
+                     bool self, const hj_opts *opts, uint64_t *count, hj_stats *stats) {
+    tl_error.clear();
+    if (!count || (na && !a) || (!self && nb && !b)) return fail(HJ_ERR_INVALID_ARG, "null pointer");
+    if (int r = validate(na, nb, d, eps)) return r;
+    Ctx *c;
+    if (int r = get_ctx(opts ? opts->device : -1, &c)) return r;
+    cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
+    *count = 0;
+    if (na == 0 || (!self && nb == 0)) {
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        return HJ_OK;
+    }
+    cudaEventRecord(c->ev[0], st);
+    void *da = slot_alloc_impl(c, st, kSlotInA, na * d * dtype_bytes);
+    void *db = self ? da : slot_alloc_impl(c, st, kSlotInB, nb * d * dtype_bytes);
+    if (!da || !db) return fail(HJ_ERR_OOM, "out of device memory");
+    cudaMemcpyAsync(da, a, na * d * dtype_bytes, cudaMemcpyHostToDevice, st);
+    if (!self) cudaMemcpyAsync(db, b, nb * d * dtype_bytes, cudaMemcpyHostToDevice, st);
+    if (int r = check_cuda("host to device copy")) return r;
+    JoinIn in{da, db, na, self ? na : nb, dtype_bytes, d, eps, self};
+    return run_join(c, in, opts, count, stats, c->ev[0]);
+}
+
+static int join_device(const void *a, uint64_t na, const void *b, uint64_t nb, int dtype_bytes, uint32_t d,
+                       double eps, bool self, const hj_opts *opts, uint64_t *count, hj_stats *stats) {
+    tl_error.clear();
+    if (!count || (na && !a) || (!self && nb && !b)) return fail(HJ_ERR_INVALID_ARG, "null pointer");
+    if (dtype_bytes != 4 && dtype_bytes != 8) return fail(HJ_ERR_INVALID_ARG, "dtype_bytes must be 4 or 8");
+    if (int r = validate(na, nb, d, eps)) return r;
+    Ctx *c;
+    if (int r = get_ctx(opts ? opts->device : -1, &c)) return r;
+    *count = 0;
+    if (na == 0 || (!self && nb == 0)) {
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        return HJ_OK;
+    }
+    JoinIn in{a, self ? a : b, na, self ? na : nb, dtype_bytes, d, eps, self};
+    return run_join(c, in, opts, count, stats, nullptr);
+}
+
+// Device EGO sort of one host set; perm (and sorted rows) copied back.
+static int ego_sort_host(const double *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts, uint64_t *perm,
+                         double *sorted) {
+    tl_error.clear();
+    if (!perm || (n && !pts)) return fail(HJ_ERR_INVALID_ARG, "null pointer");
+    if (int r = validate(n, n, d, eps)) return r;
+    Ctx *c;
+    if (int r = get_ctx(opts ? opts->device : -1, &c)) return r;
+    if (n == 0) return HJ_OK;
+    cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
+    void *dx = slot_alloc_impl(c, st, kSlotInA, n * d * 8);
+    DimStats *ds = (DimStats *)slot_alloc_impl(c, st, kSlotDimStats, d * sizeof(DimStats));
+    if (!dx || !ds) return fail(HJ_ERR_OOM, "out of device memory");
+    cudaMemcpyAsync(dx, pts, n * d * 8, cudaMemcpyHostToDevice, st);
+    unsigned long long *d_maxabs = c->d_small + 0;
+    uint32_t *d_bad = reinterpret_cast<uint32_t *>(c->d_small + 1);
+    launch_dim_stats_init(ds, d, d_maxabs, d_bad, st);
+    launch_dim_stats(dx, 8, n, d, eps, ds, d_maxabs, d_bad, st);
+    std::vector<DimStats> hds(d);
+    cudaMemcpyAsync(hds.data(), ds, d * sizeof(DimStats), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(c->h_small, c->d_small, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("cell statistics");
+    if ((uint32_t)c->h_small[1]) return fail(HJ_ERR_INVALID_ARG, "non-finite coordinate or cell out of range");
+    double maxabs;
+    std::memcpy(&maxabs, &c->h_small[0], 8);
+    Grid g;
+    if (int r = plan_grid(hds, d, eps, maxabs, &g)) return r;
+    GridDev gd;
+    gd.off = (long long *)slot_alloc_impl(c, st, kSlotGridOff, d * 8);
+    gd.bits = (uint32_t *)slot_alloc_impl(c, st, kSlotGridBits, d * 4);
+    gd.word = (uint32_t *)slot_alloc_impl(c, st, kSlotGridWord, d * 4);
+    gd.shift = (uint32_t *)slot_alloc_impl(c, st, kSlotGridShift, d * 4);
+    uint32_t *keys_wm = (uint32_t *)slot_alloc_impl(c, st, kSlotKeysWmA, n * g.W * 4);
+    uint32_t *dperm = (uint32_t *)slot_alloc_impl(c, st, kSlotPermA, n * 4);
+    uint32_t *ptmp = (uint32_t *)slot_alloc_impl(c, st, kSlotPermTmp, n * 4);
+    uint32_t *hist = (uint32_t *)slot_alloc_impl(c, st, kSlotHist, radix_hist_entries(n) * 4);
+    void *rows = sorted ? slot_alloc_impl(c, st, kSlotRowsA, n * d * 8) : nullptr;
+    if (!gd.off || !gd.bits || !gd.word || !gd.shift || !keys_wm || !dperm || !ptmp || !hist || (sorted && !rows))
+        return fail(HJ_ERR_OOM, "out of device memory");
+    cudaMemcpyAsync(gd.off, g.off.data(), d * 8, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(gd.bits, g.bits.data(), d * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(gd.word, g.word.data(), d * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(gd.shift, g.shift.data(), d * 4, cudaMemcpyHostToDevice, st);
+    int launches = 0;
+    launch_pack_keys(dx, 8, n, d, eps, gd, g.W, keys_wm, st);
+    radix_sort_perm(keys_wm, n, g.passes, dperm, ptmp, hist, st, &launches);
+    if (sorted) {
+        SortedSet s;
+        s.rows = rows;
+        launch_gather(dx, 8, n, d, dperm, keys_wm, g.W, s, kGatherRows, st, &launches);
+    }
+    std::vector<uint32_t> hp(n);
+    cudaMemcpyAsync(hp.data(), dperm, n * 4, cudaMemcpyDeviceToHost, st);
+    if (sorted) cudaMemcpyAsync(sorted, rows, n * d * 8, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("EGO sort");
+    if (int r = check_cuda("EGO sort")) return r;
+    for (uint64_t i = 0; i < n; ++i) perm[i] = hp[i];
+    return HJ_OK;
+}
+
+static int stripes_to_active_dims(int stripes) {
+    int s = 0, p3 = 1;
+    while (s < kMaxActiveDims && (p3 + 1) / 2 < stripes) {
+        ++s;
+        p3 *= 3;
+    }
+    return s;
+}
+
+}  // namespace hj
+
+using namespace hj;
+
+extern "C" {
+
+void hj_opts_init(hj_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->form = HJ_FORM_PLAIN_FP64;
+    o->active_dims = -1;
+    o->device = -1;
+}
+
+const char *hj_status_str(int s) {
+    switch (s) {
+        case HJ_OK: return "ok";
+        case HJ_ERR_INVALID_ARG: return "invalid argument";
+        case HJ_ERR_OOM: return "out of device memory";
+        case HJ_ERR_CUDA: return "CUDA error";
+        case HJ_ERR_TIMEOUT: return "device wait timed out";
+        case HJ_ERR_BAND_OVERFLOW: return "band queue overflow";
+        case HJ_ERR_NO_DEVICE: return "no usable device";
+        case HJ_ERR_UNSUPPORTED: return "unsupported input for this form";
+        case HJ_ERR_BUSY: return "rejected by admission";
+        case HJ_ERR_NOT_FOUND: return "not found";
+        default: return "unknown status";
+    }
+}
+
+const char *hj_last_error(void) { return hj::tl_error.c_str(); }
+
+const char *hj_version(void) { return "hj 1.0.0 sm_100a"; }
+
+int hj_device_sm_count(int device) {
+    int dev = device, sms = 0;
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return sms;
+}
+
+int hj_self_join_count(const double *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts, uint64_t *count,
+                       hj_stats *stats) {
+    return join_host(pts, n, pts, n, 8, d, eps, true, opts, count, stats);
+}
+
+int hj_self_join_count_f32(const float *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts,
+                           uint64_t *count, hj_stats *stats) {
+    return join_host(pts, n, pts, n, 4, d, eps, true, opts, count, stats);
+}
+
+int hj_join_count(const double *A, uint64_t nA, const double *B, uint64_t nB, uint32_t d, double eps,
+                  const hj_opts *opts, uint64_t *count, hj_stats *stats) {
+    return join_host(A, nA, B, nB, 8, d, eps, false, opts, count, stats);
+}
+
+int hj_join_count_f32(const float *A, uint64_t nA, const float *B, uint64_t nB, uint32_t d, double eps,
+                      const hj_opts *opts, uint64_t *count, hj_stats *stats) {
+    return join_host(A, nA, B, nB, 4, d, eps, false, opts, count, stats);
+}
+
+int hj_ego_sort(const double *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts, uint64_t *perm,
+                double *sorted) {
+    return ego_sort_host(pts, n, d, eps, opts, perm, sorted);
+}
+
+int hj_self_join_count_device(const void *pts, int dtype_bytes, uint64_t n, uint32_t d, double eps,
+                              const hj_opts *opts, uint64_t *count, hj_stats *stats) {
+    return join_device(pts, n, pts, n, dtype_bytes, d, eps, true, opts, count, stats);
+}
+
+int hj_join_count_device(const void *A, uint64_t nA, const void *B, uint64_t nB, int dtype_bytes, uint32_t d,
+                         double eps, const hj_opts *opts, uint64_t *count, hj_stats *stats) {
+    return join_device(A, nA, B, nB, dtype_bytes, d, eps, false, opts, count, stats);
+}
+
+void hj_test_ego_loop3_macro(size_t n, size_t d, double epsilon, double *array, size_t *countresult, int stripes,
+                             double *sortTime, double *indextime, double *loadpercent) {
+    hj_opts o;
+    hj_opts_init(&o);
+    o.ref_compat = 1;
+    o.active_dims = stripes_to_active_dims(stripes);
+    hj_stats s;
+    uint64_t c = 0;
+    int r = hj_self_join_count(array, n, (uint32_t)d, epsilon, &o, &c, &s);
+    if (countresult) *countresult = r == HJ_OK ? (size_t)c : 0;
+    if (sortTime) *sortTime = r == HJ_OK ? s.sort_ms / 1e3 : 0.0;
+    if (indextime) *indextime = r == HJ_OK ? s.index_ms / 1e3 : 0.0;
+    if (loadpercent) *loadpercent = r == HJ_OK ? s.loadpercent : 0.0;
+}
+
+void hj_test_ego_loop3_noself(const size_t nA, const size_t nB, const int d, const double epsilon, double *arrayA,
+                              double *arrayB, size_t *countresult, const int activedims, double *sortTime,
+                              double *indextime, double *loadpercent) {
+    (void)activedims;
+    hj_opts o;
+    hj_opts_init(&o);
+    o.ref_compat = 1;
+    o.active_dims = 2;
+    hj_stats s;
+    uint64_t c = 0;
+    int r = hj_join_count(arrayA, nA, arrayB, nB, (uint32_t)d, epsilon, &o, &c, &s);
+    if (countresult) *countresult = r == HJ_OK ? (size_t)c : 0;
+    if (sortTime) *sortTime = r == HJ_OK ? s.sort_ms / 1e3 : 0.0;
+    if (indextime) *indextime = r == HJ_OK ? s.index_ms / 1e3 : 0.0;
+    if (loadpercent) *loadpercent = r == HJ_OK ? s.loadpercent : 0.0;
+}
+
+}  // extern "C"

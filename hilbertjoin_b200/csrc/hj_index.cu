@@ -1,0 +1,399 @@
+// hj_index.cu -- stripe bounds and the block-pair work list.
+//
+// Replaces the reference's prepareStripes / prepareStripesNoSelf
+// (hilbertjoin/egojoin.cpp:270-464, :1126-1240), which binary-search, per point
+// and per stripe, the EGO position of the point displaced by a per-stripe
+// offset, aggregate the bounds to 8-point blocks and build min/max segment
+// trees, and the Hilbert loop FGF_HILBERT_FOR (hilbertjoin/hilloop.h:9-82) that
+// walks the (i-block, j-block) grid and prunes with those trees.
+//
+// Here the work is organised per A tile (the point tile of the distance
+// kernel). Every neighbour b of a point a has cell(b)_t in
+// [lo_t(a), hi_t(a)] = [cell(a_t - eps'), cell(a_t + eps')] for every dim t,
+// with eps' = eps + 2^-40 (eps + max|x|) slightly wider than eps so that the
+// bound also holds for the FP64 pair test and for floor(x/eps) jitter at cell
+// borders. A stripe fixes the cells of the first k = active_dims dims to one
+// combination v in the neighbour range and spans
+//   [first key >= (v, lo_k, .., lo_{d-1}),  first key > (v, hi_k, .., hi_{d-1}))
+// of B's EGO order (the reference's upper search uses ">=", which can miss the
+// cell of x + eps itself; this one is inclusive). Because adding the same
+// offset to every vector preserves lexicographic order, the union of a
+// stripe's ranges over all points of an A tile is obtained from two points
+// only: the lexicographic minimum of the lo vectors and the maximum of the
+// (lo_<k, hi_>=k) vectors. So each A tile costs 2 * 3^k binary searches, not
+// 2 * 3^k per point. The ranges are rounded out to B tiles, merged into runs,
+// split into work items of at most `chunk` B tiles, and the items sorted by the
+// Hilbert index of (A tile, B chunk), so that the items that run at the same
+// time on the GPU's SMs share their B tiles in L2 -- the role the Hilbert
+// traversal plays for the CPU caches in the reference.
+#include "hj_common.cuh"
+#include "hj_internal.h"
+
+namespace hj {
+
+struct BoundsArgs {
+    const void *rows;  // A sorted rows
+    int dtype_bytes;
+    uint64_t na;       // A rows considered
+    uint32_t d;
+    double eps, epsw;
+    GridDev g;
+    uint32_t W;
+    int k;             // active dims requested
+    const uint32_t *bkeys;  // B sorted keys [nb][W]
+    uint64_t nb;
+    int tile_a, tile_b;
+    int self;
+    uint2 *runs;       // [n_tiles][kMaxCombos]
+    uint32_t *nruns;   // [n_tiles]
+    unsigned long long *cand;  // candidate pairs (tile granularity)
+};
+
+__device__ __forceinline__ double crd(const BoundsArgs &a, uint64_t r, uint32_t t) {
+    return a.dtype_bytes == 8 ? static_cast<const double *>(a.rows)[r * a.d + t]
+                              : (double)static_cast<const float *>(a.rows)[r * a.d + t];
+}
+
+__device__ __forceinline__ uint32_t digit_of(const BoundsArgs &a, double cell, uint32_t t) {
+    long long v = (long long)cell - a.g.off[t];
+    long long mx = (1ll << a.g.bits[t]) - 1;
+    v = v < 0 ? 0 : (v > mx ? mx : v);
+    return (uint32_t)v;
+}
+
+__device__ __forceinline__ double cell_lo(const BoundsArgs &a, double x) { return floor((x - a.epsw) / a.eps); }
+__device__ __forceinline__ double cell_hi(const BoundsArgs &a, double x) { return floor((x + a.epsw) / a.eps); }
+
+// -1, 0, 1: lexicographic comparison of the lo-vectors of rows p and q.
+__device__ int cmp_lo(const BoundsArgs &a, uint64_t p, uint64_t q) {
+    for (uint32_t t = 0; t < a.d; ++t) {
+        double cp = cell_lo(a, crd(a, p, t)), cq = cell_lo(a, crd(a, q, t));
+        if (cp != cq) return cp < cq ? -1 : 1;
+    }
+    return 0;
+}
+// Same for the upper vectors (lo cells in dims < k, hi cells from dim k on).
+__device__ int cmp_up(const BoundsArgs &a, uint64_t p, uint64_t q, int k) {
+    for (uint32_t t = 0; t < a.d; ++t) {
+        double xp = crd(a, p, t), xq = crd(a, q, t);
+        double cp = (int)t < k ? cell_lo(a, xp) : cell_hi(a, xp);
+        double cq = (int)t < k ? cell_lo(a, xq) : cell_hi(a, xq);
+        if (cp != cq) return cp < cq ? -1 : 1;
+    }
+    return 0;
+}
+
+// First index in [0, n) whose key is >= q (strict = 0) or > q (strict = 1).
+// The query is the base words `base` with its first `np` words replaced by `pw`.
+__device__ uint64_t key_search(const uint32_t *__restrict__ keys, uint64_t n, uint32_t W, const uint32_t *base,
+                               const uint32_t *pw, int np, int strict) {
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint64_t mid = lo + ((hi - lo) >> 1);
+        const uint32_t *kr = keys + mid * W;
+        int c = 0;
+        for (uint32_t w = 0; w < W; ++w) {
+            uint32_t kw = __ldg(kr + w);
+            uint32_t qw = (int)w < np ? pw[w] : base[w];
+            if (kw != qw) {
+                c = kw < qw ? -1 : 1;
+                break;
+            }
+        }
+        if (c < 0 || (strict && c == 0))
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+constexpr int kBoundsWarps = 4;
+
+// One warp per A tile. Dynamic smem: per warp 2*W key words + kMaxCombos
+// intervals.
+__global__ void __launch_bounds__(kBoundsWarps * 32) k_tile_bounds(BoundsArgs a, uint64_t n_tiles) {
+    extern __shared__ uint32_t sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t tile = (uint64_t)blockIdx.x * kBoundsWarps + warp;
+    uint32_t *qlo = sm + (size_t)warp * (2 * a.W + 2 * kMaxCombos);
+    uint32_t *qhi = qlo + a.W;
+    uint2 *iv = reinterpret_cast<uint2 *>(qhi + a.W);
+    if (tile >= n_tiles) return;
+    const uint64_t p0 = tile * a.tile_a;
+    const uint64_t p1 = hj_umin(p0 + a.tile_a, a.na);
+    if (p0 >= p1) {
+        if (lane == 0) a.nruns[tile] = 0;
+        return;
+    }
+    // 1. effective active dims: dims whose neighbour range is at most 3 cells wide
+    int kt = a.k;
+    for (uint64_t p = p0 + lane; p < p1; p += 32) {
+        int ke = 0;
+        while (ke < kt) {
+            double x = crd(a, p, ke);
+            if (cell_hi(a, x) - cell_lo(a, x) > 2.0) break;
+            ++ke;
+        }
+        kt = ke;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) kt = min(kt, __shfl_xor_sync(0xffffffffu, kt, o));
+    // 2. lexicographic min of lo vectors, max of upper vectors
+    uint64_t pmin = p0 + hj_umin(lane, p1 - p0 - 1), pmax = pmin;
+    for (uint64_t p = p0 + lane + 32; p < p1; p += 32) {
+        if (cmp_lo(a, p, pmin) < 0) pmin = p;
+        if (cmp_up(a, p, pmax, kt) > 0) pmax = p;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        uint64_t qmin = __shfl_xor_sync(0xffffffffu, pmin, o);
+        uint64_t qmax = __shfl_xor_sync(0xffffffffu, pmax, o);
+        int c1 = cmp_lo(a, qmin, pmin);
+        if (c1 < 0 || (c1 == 0 && qmin < pmin)) pmin = qmin;
+        int c2 = cmp_up(a, qmax, pmax, kt);
+        if (c2 > 0 || (c2 == 0 && qmax < pmax)) pmax = qmax;
+    }
+    // 3. packed base queries
+    for (uint32_t w = lane; w < a.W; w += 32) {
+        qlo[w] = 0;
+        qhi[w] = 0;
+    }
+    __syncwarp();
+    for (uint32_t t = lane; t < a.d; t += 32) {
+        double xl = crd(a, pmin, t), xu = crd(a, pmax, t);
+        uint32_t dl = digit_of(a, cell_lo(a, xl), t);
+        uint32_t du = digit_of(a, (int)t < kt ? cell_lo(a, xu) : cell_hi(a, xu), t);
+        atomicOr(&qlo[a.g.word[t]], dl << a.g.shift[t]);
+        atomicOr(&qhi[a.g.word[t]], du << a.g.shift[t]);
+    }
+    __syncwarp();
+    // 4. one pair of searches per combination of the first kt dims
+    int ncomb = 1;
+    for (int t = 0; t < kt; ++t) ncomb *= 3;
+    const int np = kt > 0 ? (int)a.g.word[kt - 1] + 1 : 0;  // words holding active dims
+    for (int c = lane; c < ncomb; c += 32) {
+        uint32_t pl[kMaxActiveDims], ph[kMaxActiveDims];
+        for (int w = 0; w < np; ++w) {
+            pl[w] = qlo[w];
+            ph[w] = qhi[w];
+        }
+        int rem = c;
+        for (int t = kt - 1; t >= 0; --t) {
+            uint32_t delta = (uint32_t)(rem % 3);
+            rem /= 3;
+            uint32_t w = a.g.word[t], sh = a.g.shift[t];
+            uint32_t mask = ((1u << a.g.bits[t]) - 1u);
+            uint32_t fmax = mask;
+            uint32_t vl = min(((pl[w] >> sh) & mask) + delta, fmax);
+            uint32_t vh = min(((ph[w] >> sh) & mask) + delta, fmax);
+            pl[w] = (pl[w] & ~(mask << sh)) | (vl << sh);
+            ph[w] = (ph[w] & ~(mask << sh)) | (vh << sh);
+        }
+        uint64_t lower = key_search(a.bkeys, a.nb, a.W, qlo, pl, np, 0);
+        uint64_t upper = key_search(a.bkeys, a.nb, a.W, qhi, ph, np, 1);
+        if (a.self && lower < p0) lower = p0;
+        uint2 v = make_uint2(1u, 0u);  // empty
+        if (lower < upper) v = make_uint2((uint32_t)(lower / a.tile_b), (uint32_t)hj_ceil_div(upper, a.tile_b));
+        iv[c] = v;
+    }
+    __syncwarp();
+    // 5. merge the intervals into disjoint runs (lane 0)
+    if (lane == 0) {
+        int m = 0;
+        for (int c = 0; c < ncomb; ++c)
+            if (iv[c].x < iv[c].y) iv[m++] = iv[c];
+        for (int i = 1; i < m; ++i) {  // insertion sort by start
+            uint2 v = iv[i];
+            int j = i - 1;
+            while (j >= 0 && iv[j].x > v.x) {
+                iv[j + 1] = iv[j];
+                --j;
+            }
+            iv[j + 1] = v;
+        }
+        int r = 0;
+        unsigned long long cols = 0;
+        uint2 *out = a.runs + tile * kMaxCombos;
+        for (int i = 0; i < m; ++i) {
+            if (r > 0 && iv[i].x <= out[r - 1].y) {
+                out[r - 1].y = max(out[r - 1].y, iv[i].y);
+            } else {
+                out[r++] = iv[i];
+            }
+        }
+        for (int i = 0; i < r; ++i) {
+            uint64_t b0 = (uint64_t)out[i].x * a.tile_b, b1 = hj_umin((uint64_t)out[i].y * a.tile_b, a.nb);
+            cols += b1 > b0 ? b1 - b0 : 0;
+        }
+        a.nruns[tile] = (uint32_t)r;
+        atomicAdd(a.cand, cols * (p1 - p0));
+    }
+}
+
+__global__ void k_item_counts(const uint2 *__restrict__ runs, const uint32_t *__restrict__ nruns, uint64_t n_tiles,
+                              uint32_t chunk, uint32_t *counts, unsigned long long *tile_pairs) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_tiles) return;
+    uint32_t c = 0;
+    unsigned long long tp = 0;
+    for (uint32_t i = 0; i < nruns[t]; ++i) {
+        uint2 r = runs[t * kMaxCombos + i];
+        c += (uint32_t)hj_ceil_div(r.y - r.x, chunk);
+        tp += r.y - r.x;
+    }
+    counts[t] = c;
+    if (tp) atomicAdd(tile_pairs, tp);
+}
+
+// Hilbert index of (x, y) on a side-`side` grid (side a power of two); the
+// classic iterative conversion (rotate the quadrant, accumulate s*s*quadrant).
+__device__ __forceinline__ unsigned long long hilbert_index(unsigned long long side, unsigned long long x,
+                                                            unsigned long long y) {
+    unsigned long long dd = 0;
+    for (unsigned long long s = side >> 1; s > 0; s >>= 1) {
+        unsigned long long rx = (x & s) ? 1 : 0, ry = (y & s) ? 1 : 0;
+        dd += s * s * ((3 * rx) ^ ry);
+        if (ry == 0) {
+            if (rx == 1) {
+                x = side - 1 - x;
+                y = side - 1 - y;
+            }
+            unsigned long long tmp = x;
+            x = y;
+            y = tmp;
+        }
+    }
+    return dd;
+}
+
+__global__ void k_item_write(const uint2 *__restrict__ runs, const uint32_t *__restrict__ nruns,
+                             const uint32_t *__restrict__ offsets, uint64_t n_tiles, uint32_t chunk,
+                             unsigned long long side, uint32_t key_words, WorkItem *items, uint32_t *keys_wm,
+                             uint64_t n_items) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_tiles) return;
+    uint64_t o = offsets[t];
+    for (uint32_t i = 0; i < nruns[t]; ++i) {
+        uint2 r = runs[t * kMaxCombos + i];
+        for (uint32_t b = r.x; b < r.y; b += chunk) {
+            WorkItem it;
+            it.a = (uint32_t)t;
+            it.b0 = b;
+            it.b1 = min(b + chunk, r.y);
+            it.pad = 0;
+            items[o] = it;
+            unsigned long long h = hilbert_index(side, t, b / chunk);
+            if (key_words == 1) {
+                keys_wm[o] = (uint32_t)h;
+            } else {
+                keys_wm[o] = (uint32_t)(h >> 32);          // word 0: most significant
+                keys_wm[n_items + o] = (uint32_t)h;        // word 1
+            }
+            ++o;
+        }
+    }
+}
+
+__global__ void k_permute_items(const WorkItem *__restrict__ in, const uint32_t *__restrict__ perm, uint64_t n,
+                                WorkItem *out) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[perm[i]];
+}
+
+// Scratch slots requested through the caller's allocator.
+enum { kSlotRuns = 40, kSlotNruns, kSlotCounts, kSlotItemsTmp, kSlotItems, kSlotItemKeys, kSlotItemPerm,
+       kSlotItemPermTmp, kSlotItemHist, kSlotIdxStats };
+
+int build_index(const SortedSet &A, const SortedSet &B, const Grid &grid, const GridDev &gdev, bool self,
+                uint64_t na_eff, uint64_t nb_eff, int tile_a, int tile_b, int active_dims, uint32_t chunk,
+                void *(*alloc)(void *ctx, int slot, size_t bytes), void *actx, cudaStream_t st, IndexResult *out,
+                int *launches, std::string *err) {
+    *out = IndexResult();
+    const uint64_t n_tiles = hj_ceil_div(na_eff, tile_a);
+    if (n_tiles == 0 || nb_eff == 0) return 0;
+    int k = active_dims < 0 ? 0 : (active_dims > kMaxActiveDims ? kMaxActiveDims : active_dims);
+    if ((uint32_t)k > grid.d) k = (int)grid.d;
+    uint2 *runs = (uint2 *)alloc(actx, kSlotRuns, n_tiles * kMaxCombos * sizeof(uint2));
+    uint32_t *nruns = (uint32_t *)alloc(actx, kSlotNruns, n_tiles * sizeof(uint32_t));
+    uint32_t *counts = (uint32_t *)alloc(actx, kSlotCounts, (n_tiles + 1) * sizeof(uint32_t));
+    unsigned long long *stats = (unsigned long long *)alloc(actx, kSlotIdxStats, 4 * sizeof(unsigned long long));
+    if (!runs || !nruns || !counts || !stats) {
+        *err = "out of device memory (index scratch)";
+        return 2;
+    }
+    cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), st);
+    BoundsArgs ba;
+    ba.rows = A.rows;
+    ba.dtype_bytes = A.dtype_bytes;
+    ba.na = na_eff;
+    ba.d = grid.d;
+    ba.eps = grid.eps;
+    ba.epsw = grid.eps_wide;
+    ba.g = gdev;
+    ba.W = grid.W;
+    ba.k = k;
+    ba.bkeys = B.keys;
+    ba.nb = nb_eff;
+    ba.tile_a = tile_a;
+    ba.tile_b = tile_b;
+    ba.self = self ? 1 : 0;
+    ba.runs = runs;
+    ba.nruns = nruns;
+    ba.cand = stats;
+    size_t smem = (size_t)kBoundsWarps * (2 * grid.W + 2 * kMaxCombos) * sizeof(uint32_t);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_tile_bounds, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_tile_bounds<<<(unsigned)hj_ceil_div(n_tiles, kBoundsWarps), kBoundsWarps * 32, smem, st>>>(ba, n_tiles);
+    k_item_counts<<<(unsigned)hj_ceil_div(n_tiles, 256), 256, 0, st>>>(runs, nruns, n_tiles, chunk, counts,
+                                                                     stats + 1);
+    launch_scan_u32(counts, n_tiles, stats + 2, st);
+    unsigned long long hstats[4];
+    cudaMemcpyAsync(hstats, stats, sizeof(hstats), cudaMemcpyDeviceToHost, st);
+    if (launches) *launches += 3;
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        *err = std::string("index stage: ") + cudaGetErrorString(e);
+        return 3;
+    }
+    const uint64_t n_items = hstats[2];
+    out->candidate_pairs = hstats[0];
+    out->tile_pairs = hstats[1];
+    out->n_items = n_items;
+    if (n_items == 0) return 0;
+    if (n_items >= (1ull << 31)) {
+        *err = "work list too large";
+        return 1;
+    }
+    unsigned long long side = 1;
+    const uint64_t n_chunks_b = hj_ceil_div(hj_ceil_div(B.n, tile_b), chunk) + 1;
+    while (side < n_tiles || side < n_chunks_b) side <<= 1;
+    int hbits = 0;
+    while ((1ull << hbits) < side * side) ++hbits;
+    const uint32_t key_words = hbits > 32 ? 2 : 1;
+    WorkItem *tmp = (WorkItem *)alloc(actx, kSlotItemsTmp, n_items * sizeof(WorkItem));
+    WorkItem *items = (WorkItem *)alloc(actx, kSlotItems, n_items * sizeof(WorkItem));
+    uint32_t *keys = (uint32_t *)alloc(actx, kSlotItemKeys, n_items * key_words * sizeof(uint32_t));
+    uint32_t *perm = (uint32_t *)alloc(actx, kSlotItemPerm, n_items * sizeof(uint32_t));
+    uint32_t *ptmp = (uint32_t *)alloc(actx, kSlotItemPermTmp, n_items * sizeof(uint32_t));
+    uint32_t *hist = (uint32_t *)alloc(actx, kSlotItemHist, radix_hist_entries(n_items) * sizeof(uint32_t));
+    if (!tmp || !items || !keys || !perm || !ptmp || !hist) {
+        *err = "out of device memory (work list)";
+        return 2;
+    }
+    k_item_write<<<(unsigned)hj_ceil_div(n_tiles, 256), 256, 0, st>>>(runs, nruns, counts, n_tiles, chunk, side,
+                                                                     key_words, tmp, keys, n_items);
+    std::vector<std::pair<uint32_t, uint32_t>> passes;
+    if (key_words == 1) {
+        for (int b = 0; b < hbits; b += 8) passes.push_back({0u, (uint32_t)b});
+    } else {
+        for (int b = 0; b < 32; b += 8) passes.push_back({1u, (uint32_t)b});
+        for (int b = 0; b < hbits - 32; b += 8) passes.push_back({0u, (uint32_t)b});
+    }
+    radix_sort_perm(keys, n_items, passes, perm, ptmp, hist, st, launches);
+    k_permute_items<<<(unsigned)hj_ceil_div(n_items, 256), 256, 0, st>>>(tmp, perm, n_items, items);
+    if (launches) *launches += 2;
+    out->items = items;
+    return 0;
+}
+
+}  // namespace hj

@@ -1,0 +1,151 @@
+// hj_internal.h -- declarations shared by the engine's translation units:
+// device-side set layouts, the cell grid, and the kernel launch wrappers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+namespace hj {
+
+// Point-tile sizes of the two distance kernels.
+constexpr int kPlainTile = 64;   // plain FP64 kernel: 64 x 64 point tiles
+constexpr int kTcTileA = 128;    // tensor-core kernel: 128 A rows (UMMA M) ...
+constexpr int kTcTileB = 256;    // ... against 256 B rows (UMMA N)
+constexpr int kMaxActiveDims = 5;
+constexpr int kMaxCombos = 243;  // 3^kMaxActiveDims
+constexpr uint32_t kMaxDim = 1024;
+
+// Per-dimension summary of one set (or of the union of two sets) computed on
+// the device: cell index range and the largest |coordinate|.
+struct DimStats {
+    long long cmin, cmax;
+};
+
+// The epsilon grid shared by the sets of one join. Cell of a coordinate x in
+// dim t: c = floor(x / eps) (FP64). A packed key stores per dim the field
+// digit = clamp(c - off[t], 0, 2^bits[t] - 1), fields placed from the most
+// significant bit of word 0 downward in dim order (never split across words),
+// so comparing keys word by word as unsigned integers is the lexicographic
+// comparison of cell vectors (the EGO order of hilbertjoin/egojoin.cpp:9-17).
+// off[t] = min cell - 2 leaves room for the neighbour-cell queries (cell - 1,
+// cell + 1, and one more for cells that jitter at borders).
+struct Grid {
+    uint32_t d = 0;
+    double eps = 0, eps_wide = 0, maxabs = 0;
+    uint32_t W = 0;                    // 32-bit words per key
+    std::vector<long long> off;        // per dim
+    std::vector<uint32_t> bits, word, shift;
+    std::vector<long long> range;      // max cell - min cell per dim
+    // radix passes: (word, low bit) of each 8-bit digit window that can vary
+    std::vector<std::pair<uint32_t, uint32_t>> passes;
+};
+
+// Device copy of the grid's per-dim packing tables.
+struct GridDev {
+    long long *off = nullptr;
+    uint32_t *bits = nullptr, *word = nullptr, *shift = nullptr;
+};
+
+// A point set after EGO sorting, in every layout the kernels need. Rows are
+// in EGO rank order; `perm[r]` is the input index of rank r.
+struct SortedSet {
+    uint64_t n = 0;
+    uint32_t d = 0;
+    int dtype_bytes = 8;         // precision of the input (8 = FP64, 4 = FP32)
+    const void *rows = nullptr;  // sorted rows, input precision, [n][d]
+    uint32_t *keys = nullptr;    // sorted packed keys, [n][W]
+    uint32_t *perm = nullptr;
+    // plain FP64 kernel layout: [tile][d][64] (tile = 64 ranks), zero padded
+    double *tiles64 = nullptr;
+    uint64_t n_tiles64 = 0;
+    // tensor-core layouts: [npad][kpad] with npad a multiple of 256
+    float *tf32 = nullptr;       // TF32-rounded values in FP32 containers, kpad = roundup(d, 32)
+    uint16_t *bf_hi = nullptr;   // BF16 split, kpad16 = roundup(d, 64)
+    uint16_t *bf_lo = nullptr;
+    float *norms = nullptr;      // FP32(|x|^2 in FP64); padding rows hold kPadNorm
+    float *tile_maxnorm_a = nullptr;  // per 128-row tile
+    float *tile_maxnorm_b = nullptr;  // per 256-row tile
+    uint64_t npad_tc = 0;
+    uint32_t kpad_tf32 = 0, kpad_bf16 = 0;
+};
+
+constexpr float kPadNorm = 1.0e30f;
+
+// Work item of the persistent distance kernels: A tile `a` against the B tiles
+// [b0, b1). Produced by the index stage in Hilbert order.
+struct WorkItem {
+    uint32_t a, b0, b1, pad;
+};
+
+struct IndexResult {
+    WorkItem *items = nullptr;  // device, Hilbert ordered
+    uint64_t n_items = 0;
+    uint64_t tile_pairs = 0;
+    uint64_t candidate_pairs = 0;
+};
+
+// ---- launch wrappers (all asynchronous on `st` unless noted) ----------------
+
+// Per-dim min/max cell, max |x|, non-finite flag over a row-major set; results
+// accumulate into dstats[d], d_maxabs_bits, d_bad (initialised by the caller).
+void launch_dim_stats(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, DimStats *dstats,
+                      unsigned long long *d_maxabs_bits, uint32_t *d_bad, cudaStream_t st);
+void launch_dim_stats_init(DimStats *dstats, uint32_t d, unsigned long long *d_maxabs_bits, uint32_t *d_bad,
+                           cudaStream_t st);
+
+// Packed keys, word-major [W][n].
+void launch_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, const GridDev &g,
+                      uint32_t W, uint32_t *keys_wm, cudaStream_t st);
+
+// Stable LSD radix sort of a permutation by 8-bit windows of word-major keys.
+// `passes` in order (least significant first). Needs scratch: perm_tmp[n],
+// hist[256 * ceil(n/4096)]. Result in perm_out.
+void radix_sort_perm(const uint32_t *keys_wm, uint64_t n, const std::vector<std::pair<uint32_t, uint32_t>> &passes,
+                     uint32_t *perm_out, uint32_t *perm_tmp, uint32_t *hist, cudaStream_t st, int *launches);
+size_t radix_hist_entries(uint64_t n);
+// Exclusive scan of u32 entries in place (one block); total into *total if non-null.
+void launch_scan_u32(uint32_t *a, uint64_t count, unsigned long long *total, cudaStream_t st);
+
+// Gathers the sorted layouts of a set (flags select the layouts to build).
+enum GatherFlags : uint32_t { kGatherRows = 1, kGatherKeys = 2, kGatherPlain = 4, kGatherTf32 = 8, kGatherBf16 = 16,
+                              kGatherNorms = 32 };
+void launch_gather(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const uint32_t *perm,
+                   const uint32_t *keys_wm, uint32_t W, const SortedSet &out, uint32_t flags, cudaStream_t st,
+                   int *launches);
+
+// Index stage: per A tile the stripe ranges into B's EGO order, merged into
+// runs of B tiles; expanded into work items of at most `chunk` B tiles and
+// sorted in Hilbert order. Synchronises once on `st` (item count).
+struct IndexScratch;
+int build_index(const SortedSet &A, const SortedSet &B, const Grid &grid, const GridDev &gdev, bool self,
+                uint64_t na_eff, uint64_t nb_eff, int tile_a, int tile_b, int active_dims, uint32_t chunk,
+                void *(*alloc)(void *ctx, int slot, size_t bytes), void *alloc_ctx, cudaStream_t st,
+                IndexResult *out, int *launches, std::string *err);
+
+// Plain FP64 distance kernel over the work list. Adds into *d_count.
+void launch_join_fp64(const SortedSet &A, const SortedSet &B, bool self, uint64_t na_eff, uint64_t nb_eff,
+                      double T, const IndexResult &idx, unsigned long long *d_count, uint32_t *d_err,
+                      int num_sms, cudaStream_t st);
+
+// Tensor-core kernel + FP64 recheck of the band. Adds into *d_count; band pair
+// count into *d_band_total (may exceed `band_cap`: then the caller regrows).
+struct TcParams {
+    int form;             // HJ_FORM_TC_TF32 or HJ_FORM_TC_BF16X3
+    double T;             // eps * eps
+    double c_rel;         // band half-width: c_rel * (|a|^2 + |b|^2) + c_abs
+    double c_abs;
+};
+int launch_join_tc(const SortedSet &A, const SortedSet &B, bool self, uint64_t na_eff, uint64_t nb_eff,
+                   const TcParams &p, const IndexResult &idx, unsigned long long *d_count, uint2 *band,
+                   uint64_t band_cap, unsigned long long *d_band_total, uint32_t *d_err, int num_sms,
+                   cudaStream_t st, std::string *err);
+void launch_recheck(const SortedSet &A, const SortedSet &B, double T, const uint2 *band,
+                    const unsigned long long *d_band_total, uint64_t band_cap, unsigned long long *d_count,
+                    cudaStream_t st);
+// Error-bound constant of a tensor-core form for dimension d.
+void tc_band_constants(int form, uint32_t d, double maxabs, double *c_rel, double *c_abs);
+
+}  // namespace hj

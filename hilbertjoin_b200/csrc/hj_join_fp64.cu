@@ -1,0 +1,224 @@
+// hj_join_fp64.cu -- the plain FP64 distance kernel (HJ_FORM_PLAIN_FP64).
+//
+// Replaces the reference's 8x8 block-pair kernel EGO_LOOP_TRAN /
+// EGO_LOOP_TRAN_NOSELF (hilbertjoin/egojoin.h:311-392, :482-553) and its
+// count (egojoin.cpp:803-813, :871-881): 64 pairs per visit by norm expansion
+// on AVX-512 FMAs, early exit every KBLOCK dims once all 64 exceed eps^2,
+// counted by sign bit, summed per thread (egojoin.cpp:466-474).
+//
+// Here a persistent CTA of 256 threads takes work items (an A tile of 64 EGO
+// ranks against a run of B tiles of 64 ranks) in Hilbert order. The A tile is
+// staged once per item and the B tiles are double-buffered, each by one 1D
+// bulk copy (cp.async.bulk, the non-tensor TMA) of its [d][64] FP64 block into
+// shared memory, completion tracked by mbarriers. Each thread owns a 4 x 4
+// block of pairs and evaluates the pair test exactly as the oracle defines it:
+// acc = fma(a_k - b_k, a_k - b_k, acc) in IEEE FP64, k = 0..d-1 in order,
+// count iff acc <= eps*eps. The partial sums never decrease, so a warp whose
+// 512 pairs all exceed eps^2 after some dims stops early (checked every 8
+// dims) without changing any decision. Counts are reduced by warp shuffles and
+// one 64-bit atomic per warp.
+#include "hj_common.cuh"
+#include "hj_internal.h"
+
+namespace hj {
+
+struct PlainArgs {
+    const double *A, *B;  // [tile][d][64]
+    uint32_t d;
+    double T;
+    const WorkItem *items;
+    uint64_t n_items;
+    uint64_t na, nb;
+    int self;
+    unsigned long long *count;
+    uint32_t *err;
+};
+
+constexpr int kPlainThreads = 256;
+constexpr int kPlainWarps = kPlainThreads / 32;
+
+// Waits for a bulk copy to land regardless of the error word, bounded in time:
+// used only to drain copies still in flight before the CTA exits.
+__device__ __forceinline__ void drain_wait(uint64_t *bar, uint32_t parity) {
+    uint64_t t0 = globaltimer_ns();
+    while (!mbar_try_wait(bar, parity)) {
+        if (globaltimer_ns() - t0 > kWaitLimitNs) break;
+    }
+}
+
+__global__ void __launch_bounds__(kPlainThreads, 2) k_join_fp64(PlainArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar_a, bar_full[2], bar_empty[2];
+    const uint32_t d = a.d;
+    const uint32_t tile_elems = d * kPlainTile;
+    const uint32_t tile_bytes = tile_elems * 8u;
+    double *sA = reinterpret_cast<double *>(smem_raw);
+    double *sB[2] = {sA + tile_elems, sA + 2 * tile_elems};
+    const uint32_t tid = threadIdx.x, lane = tid & 31u;
+    const uint32_t ty = tid >> 4, tx = tid & 15u;
+    volatile uint32_t *err = a.err;
+
+    if (tid == 0) {
+        mbar_init(&bar_a, 1);
+        mbar_init(&bar_full[0], 1);
+        mbar_init(&bar_full[1], 1);
+        mbar_init(&bar_empty[0], kPlainWarps);
+        mbar_init(&bar_empty[1], kPlainWarps);
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    // Producer state (thread 0): the next B tile to load in this CTA's sequence.
+    uint64_t p_item = blockIdx.x;
+    uint32_t p_bt = 0, p_end = 0;
+    uint32_t issued = 0;
+    if (tid == 0 && p_item < a.n_items) {
+        WorkItem w = a.items[p_item];
+        p_bt = w.b0;
+        p_end = w.b1;
+    }
+    auto issue_next = [&](uint32_t consumed) {
+        // loads `consumed` and `consumed + 1` in flight; load j reuses the stage
+        // of load j - 2, so it waits until all warps have released that one
+        while (p_item < a.n_items && issued < consumed + 2) {
+            const uint32_t s = issued & 1u, u = issued >> 1;
+            if (u >= 1) mbar_wait(&bar_empty[s], (u - 1) & 1u, err);
+            mbar_arrive_expect_tx(&bar_full[s], tile_bytes);
+            bulk_g2s(sB[s], a.B + (uint64_t)p_bt * tile_elems, tile_bytes, &bar_full[s]);
+            ++issued;
+            if (++p_bt >= p_end) {
+                p_item += gridDim.x;
+                if (p_item < a.n_items) {
+                    WorkItem w = a.items[p_item];
+                    p_bt = w.b0;
+                    p_end = w.b1;
+                }
+            }
+        }
+    };
+    if (tid == 0) issue_next(0);
+
+    unsigned long long cnt = 0;
+    uint32_t consumed = 0, a_phase = 0;
+    const double T = a.T;
+    for (uint64_t it = blockIdx.x; it < a.n_items; it += gridDim.x) {
+        const WorkItem w = a.items[it];
+        __syncthreads();  // all warps are done with the previous A tile
+        if (tid == 0) {
+            mbar_arrive_expect_tx(&bar_a, tile_bytes);
+            bulk_g2s(sA, a.A + (uint64_t)w.a * tile_elems, tile_bytes, &bar_a);
+        }
+        mbar_wait(&bar_a, a_phase, err);
+        a_phase ^= 1u;
+        const uint64_t ia0 = (uint64_t)w.a * kPlainTile + ty * 4;
+        for (uint32_t bt = w.b0; bt < w.b1; ++bt) {
+            const uint32_t s = consumed & 1u;
+            if (tid == 0) issue_next(consumed);
+            mbar_wait(&bar_full[s], (consumed >> 1) & 1u, err);
+            const double *pa = sA + ty * 4;
+            const double *pb = sB[s] + tx * 4;
+            double acc[4][4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+            uint32_t k = 0;
+            while (k < d) {
+                const uint32_t kend = k + 8 <= d ? k + 8 : d;
+                if (kend - k == 8) {
+#pragma unroll
+                    for (int kk = 0; kk < 8; ++kk) {
+                        const double2 a01 = *reinterpret_cast<const double2 *>(pa + (k + kk) * kPlainTile);
+                        const double2 a23 = *reinterpret_cast<const double2 *>(pa + (k + kk) * kPlainTile + 2);
+                        const double2 b01 = *reinterpret_cast<const double2 *>(pb + (k + kk) * kPlainTile);
+                        const double2 b23 = *reinterpret_cast<const double2 *>(pb + (k + kk) * kPlainTile + 2);
+                        const double av[4] = {a01.x, a01.y, a23.x, a23.y};
+                        const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) {
+                                const double df = __dsub_rn(av[i], bv[j]);
+                                acc[i][j] = __fma_rn(df, df, acc[i][j]);
+                            }
+                    }
+                } else {
+                    for (uint32_t kk = k; kk < kend; ++kk) {
+                        const double2 a01 = *reinterpret_cast<const double2 *>(pa + kk * kPlainTile);
+                        const double2 a23 = *reinterpret_cast<const double2 *>(pa + kk * kPlainTile + 2);
+                        const double2 b01 = *reinterpret_cast<const double2 *>(pb + kk * kPlainTile);
+                        const double2 b23 = *reinterpret_cast<const double2 *>(pb + kk * kPlainTile + 2);
+                        const double av[4] = {a01.x, a01.y, a23.x, a23.y};
+                        const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) {
+                                const double df = __dsub_rn(av[i], bv[j]);
+                                acc[i][j] = __fma_rn(df, df, acc[i][j]);
+                            }
+                    }
+                }
+                k = kend;
+                if (k < d) {
+                    bool live = false;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) live |= acc[i][j] <= T;
+                    if (!__any_sync(0xffffffffu, live)) break;
+                }
+            }
+            const uint64_t jb0 = (uint64_t)bt * kPlainTile + tx * 4;
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const uint64_t pi = ia0 + i, pj = jb0 + j;
+                    const bool valid = pi < a.na && pj < a.nb && (!a.self || pj > pi);
+                    cnt += (valid && acc[i][j] <= T) ? 1ull : 0ull;
+                }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bar_empty[s]);
+            ++consumed;
+        }
+    }
+    cnt = warp_sum_u64(cnt);
+    if (lane == 0 && cnt) atomicAdd(a.count, cnt);
+    // Every issued copy has been consumed unless a wait gave up; then drain.
+    if (tid == 0 && *err != 0) {
+        for (uint32_t j = consumed; j < issued; ++j) drain_wait(&bar_full[j & 1u], (j >> 1) & 1u);
+    }
+}
+
+void launch_join_fp64(const SortedSet &A, const SortedSet &B, bool self, uint64_t na_eff, uint64_t nb_eff,
+                      double T, const IndexResult &idx, unsigned long long *d_count, uint32_t *d_err, int num_sms,
+                      cudaStream_t st) {
+    if (idx.n_items == 0) return;
+    PlainArgs a;
+    a.A = A.tiles64;
+    a.B = B.tiles64;
+    a.d = A.d;
+    a.T = T;
+    a.items = idx.items;
+    a.n_items = idx.n_items;
+    a.na = na_eff;
+    a.nb = nb_eff;
+    a.self = self ? 1 : 0;
+    a.count = d_count;
+    a.err = d_err;
+    const size_t smem = (size_t)3 * A.d * kPlainTile * sizeof(double);
+    static thread_local int configured_smem = 0;
+    if ((int)smem > configured_smem) {
+        cudaFuncSetAttribute(k_join_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        configured_smem = (int)smem;
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_join_fp64, kPlainThreads, smem);
+    if (per_sm < 1) per_sm = 1;
+    uint64_t grid = (uint64_t)per_sm * num_sms;
+    if (grid > idx.n_items) grid = idx.n_items;
+    k_join_fp64<<<(unsigned)grid, kPlainThreads, smem, st>>>(a);
+}
+
+}  // namespace hj

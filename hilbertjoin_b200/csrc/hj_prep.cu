@@ -1,0 +1,396 @@
+// hj_prep.cu -- epsilon-grid-order (EGO) stage of the join: per-dimension cell
+// statistics, packed cell keys, a stable LSD radix sort of the permutation, and
+// the gather of every sorted layout the distance kernels read.
+//
+// Replaces the reference's epsilonGridOrdering + omp_qsort
+// (hilbertjoin/egojoin.cpp:159-168, :594-634), an unstable in-place quicksort
+// of whole d-double rows that compares floor(x/eps) dimension by dimension
+// (epsilonGridCompare, egojoin.cpp:9-17). Here the comparison is done once per
+// point, when its cell vector is packed into 32-bit key words whose unsigned
+// order is the lexicographic cell order; the sort then only moves 4-byte
+// indices, and every data layout is written once, by the gather.
+#include <cuda_bf16.h>
+
+#include "hj_common.cuh"
+#include "hj_internal.h"
+
+namespace hj {
+
+template <typename T>
+__device__ __forceinline__ double load_coord(const void *x, uint64_t i) {
+    return (double)static_cast<const T *>(x)[i];
+}
+
+__device__ __forceinline__ double coord(const void *x, int dtype_bytes, uint64_t i) {
+    return dtype_bytes == 8 ? static_cast<const double *>(x)[i] : (double)static_cast<const float *>(x)[i];
+}
+
+// ------------------------------------------------------------ dim stats
+
+__global__ void k_dim_stats_init(DimStats *s, uint32_t d, unsigned long long *maxabs, uint32_t *bad) {
+    for (uint32_t t = threadIdx.x + blockIdx.x * blockDim.x; t < d; t += blockDim.x * gridDim.x) {
+        s[t].cmin = LLONG_MAX;
+        s[t].cmax = LLONG_MIN;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *maxabs = 0ull;
+        *bad = 0u;
+    }
+}
+
+// Cells beyond +-2^62 cannot be represented; such inputs are rejected.
+constexpr double kCellLimit = 4.611686018427388e18;
+
+__global__ void k_dim_stats(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, DimStats *s,
+                            unsigned long long *maxabs_bits, uint32_t *bad) {
+    extern __shared__ long long sh[];  // [2][d]
+    long long *smin = sh, *smax = sh + d;
+    for (uint32_t t = threadIdx.x; t < d; t += blockDim.x) {
+        smin[t] = LLONG_MAX;
+        smax[t] = LLONG_MIN;
+    }
+    __syncthreads();
+    const uint64_t total = n * d;
+    double amax = 0.0;
+    uint32_t lbad = 0;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        double v = coord(x, dtype_bytes, e);
+        if (!isfinite(v)) {
+            lbad = 1;
+            continue;
+        }
+        double c = floor(v / eps);
+        if (!(fabs(c) < kCellLimit)) {
+            lbad = 2;
+            continue;
+        }
+        amax = fmax(amax, fabs(v));
+        uint32_t t = (uint32_t)(e % d);
+        long long ci = (long long)c;
+        atomicMin(&smin[t], ci);
+        atomicMax(&smax[t], ci);
+    }
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < d; t += blockDim.x) {
+        if (smin[t] != LLONG_MAX) {
+            atomicMin(&s[t].cmin, smin[t]);
+            atomicMax(&s[t].cmax, smax[t]);
+        }
+    }
+    // non-negative doubles order like their bit patterns
+    if (amax > 0.0) atomicMax(maxabs_bits, (unsigned long long)__double_as_longlong(amax));
+    if (lbad) atomicOr(bad, lbad);
+}
+
+void launch_dim_stats_init(DimStats *dstats, uint32_t d, unsigned long long *d_maxabs_bits, uint32_t *d_bad,
+                           cudaStream_t st) {
+    k_dim_stats_init<<<(d + 255) / 256, 256, 0, st>>>(dstats, d, d_maxabs_bits, d_bad);
+}
+
+void launch_dim_stats(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, DimStats *dstats,
+                      unsigned long long *d_maxabs_bits, uint32_t *d_bad, cudaStream_t st) {
+    uint64_t total = n * d;
+    int blocks = (int)std::min<uint64_t>(hj_ceil_div(total, 256 * 8), 148 * 8);
+    if (blocks < 1) blocks = 1;
+    k_dim_stats<<<blocks, 256, 2 * d * sizeof(long long), st>>>(x, dtype_bytes, n, d, eps, dstats, d_maxabs_bits,
+                                                                 d_bad);
+}
+
+// ------------------------------------------------------------ key packing
+
+// One thread per point: digit of every dim, OR-ed into the running key word.
+__global__ void k_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, GridDev g,
+                            uint32_t W, uint32_t *keys_wm) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t cur_word = 0, acc = 0;
+    for (uint32_t t = 0; t < d; ++t) {
+        uint32_t w = g.word[t];
+        if (w != cur_word) {
+            keys_wm[(uint64_t)cur_word * n + i] = acc;
+            for (uint32_t z = cur_word + 1; z < w; ++z) keys_wm[(uint64_t)z * n + i] = 0u;
+            cur_word = w;
+            acc = 0;
+        }
+        double c = floor(coord(x, dtype_bytes, i * d + t) / eps);
+        long long dig = (long long)c - g.off[t];
+        acc |= (uint32_t)dig << g.shift[t];
+    }
+    keys_wm[(uint64_t)cur_word * n + i] = acc;
+    for (uint32_t z = cur_word + 1; z < W; ++z) keys_wm[(uint64_t)z * n + i] = 0u;
+}
+
+void launch_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, const GridDev &g,
+                      uint32_t W, uint32_t *keys_wm, cudaStream_t st) {
+    if (n == 0) return;
+    k_pack_keys<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(x, dtype_bytes, n, d, eps, g, W, keys_wm);
+}
+
+// ------------------------------------------------------------ radix sort
+//
+// Stable LSD radix sort of a permutation. Each pass orders by one 8-bit window
+// of one key word, read through the current permutation. Three kernels per
+// pass: per-tile digit histograms, one exclusive scan over (digit, tile), and a
+// stable scatter that ranks equal digits in index order (warp match + per-warp
+// prefix), so ties keep their previous order and the sort is stable overall.
+
+constexpr int kRsThreads = 256;
+constexpr int kRsTile = 4096;  // items per block
+constexpr int kRsWarps = kRsThreads / 32;
+
+size_t radix_hist_entries(uint64_t n) { return 256 * (size_t)hj_ceil_div(n, kRsTile); }
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const uint32_t *__restrict__ keyw,
+                                                       const uint32_t *__restrict__ perm_in, uint64_t n,
+                                                       uint32_t shift, uint32_t *__restrict__ hist,
+                                                       uint32_t nblocks) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    uint64_t base = (uint64_t)blockIdx.x * kRsTile;
+    uint64_t end = base + kRsTile < n ? base + kRsTile : n;
+    for (uint64_t i = base + threadIdx.x; i < end; i += kRsThreads) {
+        uint32_t src = perm_in ? perm_in[i] : (uint32_t)i;
+        atomicAdd(&h[(keyw[src] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    hist[(size_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of `count` u32 entries in place, one block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_scan_u32(uint32_t *a, uint64_t count, unsigned long long *total_out) {
+    __shared__ unsigned long long part[1024];
+    const uint64_t per = hj_ceil_div(count, 1024);
+    const uint64_t b = threadIdx.x * per, e = b + per < count ? b + per : count;
+    unsigned long long s = 0;
+    for (uint64_t i = b; i < e; ++i) s += a[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        unsigned long long v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0ull;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned long long run = threadIdx.x ? part[threadIdx.x - 1] : 0ull;
+    for (uint64_t i = b; i < e; ++i) {
+        uint32_t v = a[i];
+        a[i] = (uint32_t)run;
+        run += v;
+    }
+    if (total_out && threadIdx.x == 1023) *total_out = part[1023];
+}
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint32_t *__restrict__ keyw,
+                                                          const uint32_t *__restrict__ perm_in, uint64_t n,
+                                                          uint32_t shift, const uint32_t *__restrict__ hist,
+                                                          uint32_t nblocks, uint32_t *__restrict__ perm_out) {
+    __shared__ uint32_t s_base[256];
+    __shared__ uint32_t s_wcnt[kRsWarps][256];
+    const uint32_t t = threadIdx.x, warp = t >> 5, lane = t & 31u;
+    s_base[t] = hist[(size_t)t * nblocks + blockIdx.x];
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint64_t base = (uint64_t)blockIdx.x * kRsTile;
+    for (int r = 0; r < kRsTile / kRsThreads; ++r) {
+        uint64_t i = base + (uint64_t)r * kRsThreads + t;
+        bool valid = i < n;
+        uint32_t src = 0, dig = 256u;
+        if (valid) {
+            src = perm_in ? perm_in[i] : (uint32_t)i;
+            dig = (keyw[src] >> shift) & 255u;
+        }
+#pragma unroll
+        for (int w = 0; w < kRsWarps; ++w) s_wcnt[w][t] = 0;
+        __syncthreads();
+        uint32_t peers = __match_any_sync(0xffffffffu, dig);
+        uint32_t rank = __popc(peers & lt_mask);
+        if (valid && rank == 0) s_wcnt[warp][dig] = __popc(peers);
+        __syncthreads();
+        {
+            uint32_t run = s_base[t];
+#pragma unroll
+            for (int w = 0; w < kRsWarps; ++w) {
+                uint32_t c = s_wcnt[w][t];
+                s_wcnt[w][t] = run;
+                run += c;
+            }
+            s_base[t] = run;
+        }
+        __syncthreads();
+        if (valid) perm_out[s_wcnt[warp][dig] + rank] = src;
+        __syncthreads();
+    }
+}
+
+void launch_scan_u32(uint32_t *a, uint64_t count, unsigned long long *total, cudaStream_t st) {
+    k_scan_u32<<<1, 1024, 0, st>>>(a, count, total);
+}
+
+__global__ void k_iota(uint32_t *p, uint64_t n) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = (uint32_t)i;
+}
+
+void radix_sort_perm(const uint32_t *keys_wm, uint64_t n, const std::vector<std::pair<uint32_t, uint32_t>> &passes,
+                     uint32_t *perm_out, uint32_t *perm_tmp, uint32_t *hist, cudaStream_t st, int *launches) {
+    if (n == 0) return;
+    const uint32_t nb = (uint32_t)hj_ceil_div(n, kRsTile);
+    if (passes.empty()) {
+        k_iota<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(perm_out, n);
+        if (launches) *launches += 1;
+        return;
+    }
+    // ping-pong so that the last pass writes perm_out
+    const size_t np = passes.size();
+    uint32_t *bufs[2] = {perm_out, perm_tmp};
+    const uint32_t *src = nullptr;
+    for (size_t p = 0; p < np; ++p) {
+        uint32_t *dst = bufs[(np - 1 - p) & 1];
+        const uint32_t *kw = keys_wm + (size_t)passes[p].first * n;
+        const uint32_t shift = passes[p].second;
+        k_rs_hist<<<nb, kRsThreads, 0, st>>>(kw, src, n, shift, hist, nb);
+        k_scan_u32<<<1, 1024, 0, st>>>(hist, (uint64_t)nb * 256, nullptr);
+        k_rs_scatter<<<nb, kRsThreads, 0, st>>>(kw, src, n, shift, hist, nb, dst);
+        if (launches) *launches += 3;
+        src = dst;
+    }
+}
+
+// ------------------------------------------------------------ gather
+
+// Sorted keys row-major [n][W] (for binary searches) and sorted rows.
+__global__ void k_gather_keys_rows(const void *x, int dtype_bytes, uint64_t n, uint32_t d,
+                                   const uint32_t *__restrict__ perm, const uint32_t *__restrict__ keys_wm,
+                                   uint32_t W, uint32_t *__restrict__ keys_rm, void *rows_out) {
+    uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    uint32_t src = perm[r];
+    if (keys_rm)
+        for (uint32_t w = 0; w < W; ++w) keys_rm[r * W + w] = keys_wm[(uint64_t)w * n + src];
+    if (rows_out) {
+        if (dtype_bytes == 8) {
+            const double *xs = static_cast<const double *>(x) + (uint64_t)src * d;
+            double *o = static_cast<double *>(rows_out) + r * d;
+            for (uint32_t k = 0; k < d; ++k) o[k] = xs[k];
+        } else {
+            const float *xs = static_cast<const float *>(x) + (uint64_t)src * d;
+            float *o = static_cast<float *>(rows_out) + r * d;
+            for (uint32_t k = 0; k < d; ++k) o[k] = xs[k];
+        }
+    }
+}
+
+// Plain layout [tile][d][64]: element (rank r, dim k) at ((r/64)*d + k)*64 + r%64.
+// One thread per output element, so the writes are coalesced.
+__global__ void k_gather_plain(const void *x, int dtype_bytes, uint64_t n, uint32_t d,
+                               const uint32_t *__restrict__ perm, double *__restrict__ out, uint64_t n_tiles) {
+    uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t total = n_tiles * d * 64;
+    if (e >= total) return;
+    uint32_t lane = (uint32_t)(e & 63u);
+    uint64_t q = e >> 6;
+    uint32_t k = (uint32_t)(q % d);
+    uint64_t tile = q / d;
+    uint64_t r = tile * 64 + lane;
+    double v = 0.0;
+    if (r < n) v = coord(x, dtype_bytes, (uint64_t)perm[r] * d + k);
+    out[e] = v;
+}
+
+__device__ __forceinline__ float to_tf32_rn(float v) {
+    uint32_t u;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(v));
+    return __uint_as_float(u);
+}
+
+// Tensor-core layouts, one thread per (row, k) element of the padded matrix:
+// TF32 rows [npad][kp32], BF16 hi/lo rows [npad][kp16].
+__global__ void k_gather_tc(const void *x, int dtype_bytes, uint64_t n, uint32_t d,
+                            const uint32_t *__restrict__ perm, uint64_t npad, uint32_t kp, float *tf32,
+                            uint16_t *bf_hi, uint16_t *bf_lo) {
+    uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= npad * kp) return;
+    uint64_t r = e / kp;
+    uint32_t k = (uint32_t)(e % kp);
+    float v = 0.0f;
+    if (r < n && k < d) v = (float)coord(x, dtype_bytes, (uint64_t)perm[r] * d + k);
+    if (tf32) tf32[e] = to_tf32_rn(v);
+    if (bf_hi) {
+        __nv_bfloat16 h = __float2bfloat16_rn(v);
+        float rem = v - __bfloat162float(h);  // exact: h holds the leading bits of v
+        __nv_bfloat16 l = __float2bfloat16_rn(rem);
+        bf_hi[e] = __bfloat16_as_ushort(h);
+        bf_lo[e] = __bfloat16_as_ushort(l);
+    }
+}
+
+// |x|^2 per sorted row in FP64 (input precision widened exactly), stored as
+// FP32; padding rows get kPadNorm so that they never pass a threshold.
+__global__ void k_norms(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const uint32_t *__restrict__ perm,
+                        uint64_t npad, float *norms) {
+    uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= npad) return;
+    if (r >= n) {
+        norms[r] = kPadNorm;
+        return;
+    }
+    uint64_t src = perm[r];
+    double s = 0.0;
+    for (uint32_t k = 0; k < d; ++k) {
+        double v = coord(x, dtype_bytes, src * d + k);
+        s = fma(v, v, s);
+    }
+    norms[r] = (float)s;
+}
+
+__global__ void k_tile_max(const float *__restrict__ v, uint64_t npad, int tile, float *out) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t * tile >= npad) return;
+    float m = -3.4e38f;
+    for (int i = 0; i < tile; ++i) m = fmaxf(m, v[t * tile + i]);
+    out[t] = m;
+}
+
+void launch_gather(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const uint32_t *perm,
+                   const uint32_t *keys_wm, uint32_t W, const SortedSet &o, uint32_t flags, cudaStream_t st,
+                   int *launches) {
+    int L = 0;
+    if (n == 0) return;
+    if (flags & (kGatherKeys | kGatherRows)) {
+        k_gather_keys_rows<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(
+            x, dtype_bytes, n, d, perm, keys_wm, W, (flags & kGatherKeys) ? o.keys : nullptr,
+            (flags & kGatherRows) ? const_cast<void *>(o.rows) : nullptr);
+        ++L;
+    }
+    if (flags & kGatherPlain) {
+        uint64_t total = o.n_tiles64 * d * 64;
+        k_gather_plain<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.tiles64,
+                                                                         o.n_tiles64);
+        ++L;
+    }
+    if (flags & kGatherTf32) {
+        uint64_t total = o.npad_tc * o.kpad_tf32;
+        k_gather_tc<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.npad_tc,
+                                                                      o.kpad_tf32, o.tf32, nullptr, nullptr);
+        ++L;
+    }
+    if (flags & kGatherBf16) {
+        uint64_t total = o.npad_tc * o.kpad_bf16;
+        k_gather_tc<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.npad_tc,
+                                                                      o.kpad_bf16, nullptr, o.bf_hi, o.bf_lo);
+        ++L;
+    }
+    if (flags & kGatherNorms) {
+        k_norms<<<(unsigned)hj_ceil_div(o.npad_tc, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.npad_tc,
+                                                                      o.norms);
+        k_tile_max<<<(unsigned)hj_ceil_div(o.npad_tc / kTcTileA, 256), 256, 0, st>>>(o.norms, o.npad_tc, kTcTileA,
+                                                                                    o.tile_maxnorm_a);
+        k_tile_max<<<(unsigned)hj_ceil_div(o.npad_tc / kTcTileB, 256), 256, 0, st>>>(o.norms, o.npad_tc, kTcTileB,
+                                                                                    o.tile_maxnorm_b);
+        L += 3;
+    }
+    if (launches) *launches += L;
+}
+
+}  // namespace hj

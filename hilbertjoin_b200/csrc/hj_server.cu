@@ -1,0 +1,291 @@
+// hj_server.cu -- the join-serving loop (no reference counterpart).
+//
+// Point sets are uploaded once and stay resident on the device. Joins are
+// submitted from any host thread into a queue and return a request id at once.
+// A pool of `max_inflight` worker threads, each with its own device context and
+// CUDA stream, takes requests in arrival order as soon as (a) a worker is free
+// and (b) the request's working-memory estimate fits in what is left of the
+// memory budget; its kernels then run concurrently with the other admitted
+// requests' kernels on the same device (continuous batching across streams). A
+// request larger than the whole budget is rejected with HJ_ERR_BUSY. Every
+// request's count is computed by the same pipeline as a standalone call, so a
+// result does not depend on what else is in flight.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "../../include/hj.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct DevSet {
+    void *ptr = nullptr;
+    uint64_t n = 0;
+    uint32_t d = 0;
+    int dtype_bytes = 8;
+    int users = 0;        // queued or running requests referencing the set
+    bool released = false;
+};
+
+struct Request {
+    uint64_t id = 0;
+    uint64_t a = 0, b = 0;
+    double eps = 0;
+    uint64_t mem = 0;
+    Clock::time_point t_submit, t_start, t_end;
+    bool done = false;
+    hj_result res{};
+};
+
+}  // namespace
+
+struct hj_server {
+    hj_server_opts opts{};
+    int device = 0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<uint64_t> queue;
+    std::map<uint64_t, Request> reqs;
+    std::map<uint64_t, DevSet> sets;
+    uint64_t next_id = 1, next_set = 1;
+    uint64_t mem_in_use = 0;
+    bool stop = false;
+    std::vector<std::thread> workers;
+};
+
+static uint64_t request_bytes(const DevSet &a, const DevSet &b, bool self) {
+    // sorted rows + one distance layout + keys/permutations per point, plus the
+    // work list and band queue
+    auto per_set = [](const DevSet &s) -> uint64_t {
+        return s.n * (uint64_t)s.d * 20ull + s.n * 64ull;
+    };
+    uint64_t m = per_set(a) + (self ? 0 : per_set(b));
+    return m + (64ull << 20);
+}
+
+static void worker_main(hj_server *s) {
+    cudaSetDevice(s->device);
+    for (;;) {
+        uint64_t id = 0;
+        Request rq;
+        DevSet sa, sb;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            for (;;) {
+                if (s->stop) return;
+                if (!s->queue.empty()) {
+                    Request &front = s->reqs[s->queue.front()];
+                    if (s->mem_in_use + front.mem <= s->opts.memory_budget_bytes || s->mem_in_use == 0) break;
+                }
+                s->cv_work.wait(lk);
+            }
+            id = s->queue.front();
+            s->queue.pop_front();
+            Request &r = s->reqs[id];
+            s->mem_in_use += r.mem;
+            r.t_start = Clock::now();
+            rq = r;
+            sa = s->sets[r.a];
+            sb = s->sets[r.b];
+            s->cv_work.notify_all();
+        }
+        hj_opts o;
+        hj_opts_init(&o);
+        o.form = s->opts.form;
+        o.device = s->device;
+        uint64_t count = 0;
+        hj_stats st;
+        int status;
+        if (rq.a == rq.b)
+            status = hj_self_join_count_device(sa.ptr, sa.dtype_bytes, sa.n, sa.d, rq.eps, &o, &count, &st);
+        else
+            status = hj_join_count_device(sa.ptr, sa.n, sb.ptr, sb.n, sa.dtype_bytes, sa.d, rq.eps, &o, &count, &st);
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            Request &r = s->reqs[id];
+            r.t_end = Clock::now();
+            r.done = true;
+            r.res.count = count;
+            r.res.status = status;
+            r.res.form_used = status == HJ_OK ? st.form_used : -1;
+            r.res.queue_ms = std::chrono::duration<double, std::milli>(r.t_start - r.t_submit).count();
+            r.res.run_ms = std::chrono::duration<double, std::milli>(r.t_end - r.t_start).count();
+            r.res.latency_ms = std::chrono::duration<double, std::milli>(r.t_end - r.t_submit).count();
+            r.res.candidate_pairs = status == HJ_OK ? st.candidate_pairs : 0;
+            r.res.band_pairs = status == HJ_OK ? st.band_pairs : 0;
+            s->mem_in_use -= r.mem;
+            for (uint64_t sid : {r.a, r.b}) {
+                auto it = s->sets.find(sid);
+                if (it != s->sets.end()) {
+                    if (--it->second.users == 0 && it->second.released) {
+                        cudaFree(it->second.ptr);
+                        s->sets.erase(it);
+                    }
+                }
+                if (r.a == r.b) break;
+            }
+        }
+        s->cv_done.notify_all();
+        s->cv_work.notify_all();
+    }
+}
+
+extern "C" {
+
+void hj_server_opts_init(hj_server_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->memory_budget_bytes = 40ull << 30;
+    o->max_inflight = 8;
+    o->device = -1;
+    o->form = HJ_FORM_PLAIN_FP64;
+}
+
+int hj_server_create(const hj_server_opts *opts, hj_server **out) {
+    if (!out) return HJ_ERR_INVALID_ARG;
+    hj_server_opts o;
+    hj_server_opts_init(&o);
+    if (opts) o = *opts;
+    if (o.memory_budget_bytes == 0) o.memory_budget_bytes = 40ull << 30;
+    if (o.max_inflight <= 0) o.max_inflight = 8;
+    int dev = o.device;
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return HJ_ERR_NO_DEVICE;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || dev >= ndev) {
+        cudaGetLastError();
+        return HJ_ERR_NO_DEVICE;
+    }
+    hj_server *s = new hj_server();
+    s->opts = o;
+    s->device = dev;
+    for (int i = 0; i < o.max_inflight; ++i) s->workers.emplace_back(worker_main, s);
+    *out = s;
+    return HJ_OK;
+}
+
+int hj_server_destroy(hj_server *s) {
+    if (!s) return HJ_ERR_INVALID_ARG;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    for (auto &t : s->workers) t.join();
+    cudaSetDevice(s->device);
+    for (auto &kv : s->sets) cudaFree(kv.second.ptr);
+    delete s;
+    return HJ_OK;
+}
+
+int hj_set_upload(hj_server *s, const void *pts, int dtype_bytes, uint64_t n, uint32_t d, uint64_t *set_id) {
+    if (!s || !set_id || (n && !pts) || (dtype_bytes != 4 && dtype_bytes != 8) || d == 0) return HJ_ERR_INVALID_ARG;
+    cudaSetDevice(s->device);
+    void *p = nullptr;
+    size_t bytes = n * d * (size_t)dtype_bytes;
+    if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) {
+        cudaGetLastError();
+        return HJ_ERR_OOM;
+    }
+    if (bytes && cudaMemcpy(p, pts, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(p);
+        return HJ_ERR_CUDA;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    uint64_t id = s->next_set++;
+    DevSet ds;
+    ds.ptr = p;
+    ds.n = n;
+    ds.d = d;
+    ds.dtype_bytes = dtype_bytes;
+    s->sets[id] = ds;
+    *set_id = id;
+    return HJ_OK;
+}
+
+int hj_set_release(hj_server *s, uint64_t set_id) {
+    if (!s) return HJ_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->sets.find(set_id);
+    if (it == s->sets.end() || it->second.released) return HJ_ERR_NOT_FOUND;
+    if (it->second.users == 0) {
+        cudaSetDevice(s->device);
+        cudaFree(it->second.ptr);
+        s->sets.erase(it);
+    } else {
+        it->second.released = true;  // freed when its last request finishes
+    }
+    return HJ_OK;
+}
+
+int hj_submit(hj_server *s, uint64_t set_a, uint64_t set_b, double eps, uint64_t *request_id) {
+    if (!s || !request_id) return HJ_ERR_INVALID_ARG;
+    if (set_b == 0) set_b = set_a;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto ia = s->sets.find(set_a), ib = s->sets.find(set_b);
+    if (ia == s->sets.end() || ib == s->sets.end() || ia->second.released || ib->second.released)
+        return HJ_ERR_NOT_FOUND;
+    if (ia->second.d != ib->second.d || ia->second.dtype_bytes != ib->second.dtype_bytes)
+        return HJ_ERR_INVALID_ARG;
+    Request r;
+    r.id = s->next_id++;
+    r.a = set_a;
+    r.b = set_b;
+    r.eps = eps;
+    r.mem = request_bytes(ia->second, ib->second, set_a == set_b);
+    r.t_submit = Clock::now();
+    if (r.mem > s->opts.memory_budget_bytes) return HJ_ERR_BUSY;
+    ia->second.users++;
+    if (set_b != set_a) ib->second.users++;
+    s->reqs[r.id] = r;
+    s->queue.push_back(r.id);
+    *request_id = r.id;
+    s->cv_work.notify_one();
+    return HJ_OK;
+}
+
+int hj_poll(hj_server *s, uint64_t request_id, int *done, hj_result *result) {
+    if (!s || !done) return HJ_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(request_id);
+    if (it == s->reqs.end()) return HJ_ERR_NOT_FOUND;
+    *done = it->second.done ? 1 : 0;
+    if (it->second.done) {
+        if (result) *result = it->second.res;
+        s->reqs.erase(it);
+    }
+    return HJ_OK;
+}
+
+int hj_wait(hj_server *s, uint64_t request_id, double timeout_ms, hj_result *result) {
+    if (!s) return HJ_ERR_INVALID_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto pred = [&] {
+        auto it = s->reqs.find(request_id);
+        return it == s->reqs.end() || it->second.done;
+    };
+    if (timeout_ms < 0)
+        s->cv_done.wait(lk, pred);
+    else if (!s->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), pred))
+        return HJ_ERR_TIMEOUT;
+    auto it = s->reqs.find(request_id);
+    if (it == s->reqs.end()) return HJ_ERR_NOT_FOUND;
+    if (result) *result = it->second.res;
+    s->reqs.erase(it);
+    return HJ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,211 @@
+/* hj.h -- C ABI of the B200 epsilon-join cardinality engine (libhj.so).
+ *
+ * The engine counts pairs of points in R^d whose Euclidean distance is at most
+ * eps: unordered pairs {a, b}, a != b, within one set (self-join), or ordered
+ * pairs (a in A, b in B) between two sets. It replaces the count path of the
+ * hilbertJoin reference (perdacherMartin/hilbertJoin): the library functions
+ * test_ego_loop3_macro / test_ego_loop3_noself behind the executables
+ * hilbertSelfJoinCardinality / hilbertJoinCardinality.
+ *
+ * Pair test (every form returns exactly this count): with acc = 0 and, for
+ * k = 0 .. d-1, acc = fma(a_k - b_k, a_k - b_k, acc) evaluated in IEEE FP64,
+ * a pair counts iff acc <= eps * eps (FP64). FP32 inputs are widened to FP64
+ * exactly first.
+ *
+ * Conventions: every function returns an hj_status; none exits the process.
+ * Inputs are const and never modified (the reference sorts its input in place,
+ * hilbertjoin/egojoin.cpp:159-168, and leaves it permuted). No allocation
+ * slack is required of the caller (the reference requires +16384 bytes,
+ * main.cpp:59). Calls are reentrant: each calling host thread gets its own
+ * device context and stream unless it passes its own stream.
+ */
+#ifndef HJ_H
+#define HJ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HJ_API __attribute__((visibility("default")))
+#else
+#define HJ_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The reference has no error reporting: it calls exit(1) on
+ * allocation, I/O and argument errors (util/allocation.cpp:14-15,
+ * util/dataIo.cpp:125,136, util/arguments.cpp:21). */
+typedef enum {
+    HJ_OK = 0,
+    HJ_ERR_INVALID_ARG = 1,   /* null pointer, n or d out of range, eps <= 0 or not finite,
+                                 a non-finite coordinate, or a cell index out of int32 range */
+    HJ_ERR_OOM = 2,           /* device allocation failed */
+    HJ_ERR_CUDA = 3,          /* a CUDA call failed; hj_last_error() has the text */
+    HJ_ERR_TIMEOUT = 4,       /* a bounded device-side wait gave up (kernel returned early) */
+    HJ_ERR_BAND_OVERFLOW = 5, /* tensor-core band queue still too small after regrowth */
+    HJ_ERR_NO_DEVICE = 6,     /* no usable sm_100 device */
+    HJ_ERR_UNSUPPORTED = 7,   /* the requested form cannot run this input (see hj_opts.form) */
+    HJ_ERR_BUSY = 8,          /* serving: request rejected by admission (memory budget) */
+    HJ_ERR_NOT_FOUND = 9      /* serving: unknown handle or request id */
+} hj_status;
+
+/* How pair distances are evaluated. Every form returns the exact count of the
+ * pair test above. */
+typedef enum {
+    /* FP64 direct difference on CUDA cores, early exit every 8 dims once all
+     * pairs of a warp exceed eps^2 (the reference's KBLOCK early exit,
+     * hilbertjoin/egojoin.h:350-359). The drop-in form. */
+    HJ_FORM_PLAIN_FP64 = 0,
+    /* dist^2 = |a|^2 + |b|^2 - 2 a.b with a.b on tcgen05 tensor cores in TF32
+     * (operands rounded to TF32, FP32 accumulation); every pair within a
+     * derived error bound of eps^2 is re-evaluated with the FP64 pair test. */
+    HJ_FORM_TC_TF32 = 1,
+    /* As TF32, with a.b as the BF16 split three-product
+     * a_hi.b_hi + a_hi.b_lo + a_lo.b_hi (a = a_hi + a_lo), FP32 accumulation. */
+    HJ_FORM_TC_BF16X3 = 2,
+    /* HJ_FORM_TC_TF32 when the input allows it (d <= 256, coordinates within
+     * +-2^60), else HJ_FORM_PLAIN_FP64. */
+    HJ_FORM_AUTO = 3
+} hj_form;
+
+typedef struct {
+    int32_t form;          /* hj_form; default HJ_FORM_PLAIN_FP64 */
+    int32_t active_dims;   /* stripes split the first active_dims dims into neighbour cells
+                              (the reference's -s; (3^s+1)/2 stripes, main.cpp:54).
+                              -1 = default (3 for self-joins, 2 for two-set joins,
+                              as egojoin.cpp:847 hard-codes) */
+    int32_t ref_compat;    /* nonzero: count only among the first 8*floor(n/8) EGO-sorted
+                              points of each set, as the reference's block loops do */
+    int32_t device;        /* CUDA device ordinal; -1 = current */
+    void *stream;          /* cudaStream_t to run on; NULL = the calling thread's own stream */
+    uint64_t reserved[4];
+} hj_opts;
+
+/* Per-call statistics (all optional). Times are device times of each stage
+ * measured with CUDA events. */
+typedef struct {
+    double h2d_ms;          /* host -> device copy of the input */
+    double sort_ms;         /* cell keys + stable LSD radix sort + gather (the reference's SORTTIME) */
+    double index_ms;        /* stripe bounds + block-pair work list (the reference's INDEXTIME) */
+    double join_ms;         /* distance kernel(s) */
+    double recheck_ms;      /* FP64 re-evaluation of band pairs (tensor-core forms) */
+    double total_ms;        /* whole call, host wall clock */
+    double loadpercent;     /* candidate pairs / all pairs * 100 (the reference's LOADPERCENT
+                               is on 8-point blocks, egojoin.cpp:797) */
+    uint64_t candidate_pairs; /* point pairs inside the block-pair work list */
+    uint64_t tile_pairs;    /* block pairs in the work list */
+    uint64_t work_items;    /* items of the persistent kernel's work list */
+    uint64_t band_pairs;    /* pairs sent to the FP64 recheck */
+    double band_fraction;   /* band_pairs / candidate_pairs */
+    double band_halfwidth_rel; /* tensor-core bound: |dist2 - est| <= c * (|a|^2 + |b|^2) + abs; this is c */
+    int32_t form_used;      /* hj_form actually run */
+    int32_t stripes;        /* stripe count (3^s+1)/2 for self-joins, 3^s for two-set joins */
+    int32_t kernel_launches;/* kernels this call launched */
+    int32_t reserved_i;
+    uint64_t reserved[4];
+} hj_stats;
+
+HJ_API void hj_opts_init(hj_opts *o);
+HJ_API const char *hj_status_str(int status);
+/* Text of the last error on this host thread ("" if none). */
+HJ_API const char *hj_last_error(void);
+/* Library version, e.g. "hj 1.0.0 sm_100a". */
+HJ_API const char *hj_version(void);
+/* Number of SMs of a device (-1 = current), 0 if there is none. */
+HJ_API int hj_device_sm_count(int device);
+
+/* Self-join count over n points of dimension d, row-major (point i at
+ * pts[i*d .. i*d+d-1]). Replaces test_ego_loop3_macro
+ * (hilbertjoin/egojoin.h:56, egojoin.cpp:777-838). */
+HJ_API int hj_self_join_count(const double *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts,
+                       uint64_t *count, hj_stats *stats);
+HJ_API int hj_self_join_count_f32(const float *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts,
+                           uint64_t *count, hj_stats *stats);
+
+/* Two-set join count, ordered pairs (a in A, b in B). Replaces
+ * test_ego_loop3_noself (hilbertjoin/egojoin.h:64, egojoin.cpp:840-907). */
+HJ_API int hj_join_count(const double *A, uint64_t nA, const double *B, uint64_t nB, uint32_t d, double eps,
+                  const hj_opts *opts, uint64_t *count, hj_stats *stats);
+HJ_API int hj_join_count_f32(const float *A, uint64_t nA, const float *B, uint64_t nB, uint32_t d, double eps,
+                      const hj_opts *opts, uint64_t *count, hj_stats *stats);
+
+/* Epsilon-grid order of a point set computed on the device: perm[r] is the
+ * input index of the point at rank r, ranks ordered lexicographically by the
+ * cell vector floor(x/eps) (dim 0 most significant), ties in input order
+ * (stable). If `sorted` is non-null it receives the rows in that order.
+ * Replaces epsilonGridOrdering (hilbertjoin/egojoin.cpp:159-168), which sorts
+ * the caller's array in place with an unstable quicksort. */
+HJ_API int hj_ego_sort(const double *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts, uint64_t *perm,
+                       double *sorted);
+
+/* The same calls on inputs already in device memory (row-major, d per row).
+ * `dtype_bytes` is 8 (FP64) or 4 (FP32). The pointers must be device (or
+ * managed) memory of the device the call runs on. */
+HJ_API int hj_self_join_count_device(const void *pts, int dtype_bytes, uint64_t n, uint32_t d, double eps,
+                              const hj_opts *opts, uint64_t *count, hj_stats *stats);
+HJ_API int hj_join_count_device(const void *A, uint64_t nA, const void *B, uint64_t nB, int dtype_bytes, uint32_t d,
+                         double eps, const hj_opts *opts, uint64_t *count, hj_stats *stats);
+
+/* Drop-in replacements with the reference's exact argument lists. The count
+ * uses the reference's convention (first 8*floor(n/8) EGO-sorted points). The
+ * input is left untouched (the reference leaves it sorted). Times are in
+ * seconds like the reference's. `stripes` is (3^s+1)/2 as main.cpp:54 computes
+ * it; `activedims` is ignored exactly as the reference ignores it (it
+ * hard-codes 2, egojoin.cpp:847). Errors are reported as *countresult = 0 and
+ * hj_last_error(). */
+HJ_API void hj_test_ego_loop3_macro(size_t n, size_t d, double epsilon, double *array, size_t *countresult, int stripes,
+                             double *sortTime, double *indextime, double *loadpercent);
+HJ_API void hj_test_ego_loop3_noself(const size_t nA, const size_t nB, const int d, const double epsilon, double *arrayA,
+                              double *arrayB, size_t *countresult, const int activedims, double *sortTime,
+                              double *indextime, double *loadpercent);
+
+/* ---------------------------------------------------------------- serving
+ * A request loop with device-resident point sets: sets are uploaded once and
+ * referenced by handle; joins are submitted from any thread, admitted against
+ * a device-memory budget, and run as soon as a slot frees, overlapping on the
+ * device (continuous batching). No reference counterpart. */
+typedef struct hj_server hj_server;
+
+typedef struct {
+    uint64_t memory_budget_bytes; /* admission budget for per-request working memory (0 = 40 GiB) */
+    int32_t max_inflight;         /* concurrent requests on the device (0 = 8) */
+    int32_t device;               /* -1 = current */
+    int32_t form;                 /* hj_form for every request */
+    int32_t reserved_i;
+    uint64_t reserved[4];
+} hj_server_opts;
+
+typedef struct {
+    uint64_t count;
+    int32_t status;      /* hj_status of the request */
+    int32_t form_used;
+    double queue_ms;     /* submit -> start on device */
+    double run_ms;       /* start -> result ready */
+    double latency_ms;   /* submit -> result ready */
+    uint64_t candidate_pairs;
+    uint64_t band_pairs;
+} hj_result;
+
+HJ_API void hj_server_opts_init(hj_server_opts *o);
+HJ_API int hj_server_create(const hj_server_opts *opts, hj_server **out);
+HJ_API int hj_server_destroy(hj_server *s);
+/* Uploads a point set (host, row-major; dtype_bytes 4 or 8). The set stays on
+ * the device until hj_set_release. */
+HJ_API int hj_set_upload(hj_server *s, const void *pts, int dtype_bytes, uint64_t n, uint32_t d, uint64_t *set_id);
+HJ_API int hj_set_release(hj_server *s, uint64_t set_id);
+/* Queues a self-join (set_b == set_a or set_b == 0) or a two-set join.
+ * Returns at once with a request id. */
+HJ_API int hj_submit(hj_server *s, uint64_t set_a, uint64_t set_b, double eps, uint64_t *request_id);
+/* Non-blocking: HJ_OK with *done = 1 and the result once finished. */
+HJ_API int hj_poll(hj_server *s, uint64_t request_id, int *done, hj_result *result);
+/* Blocks until the request finishes (timeout_ms < 0: no limit). */
+HJ_API int hj_wait(hj_server *s, uint64_t request_id, double timeout_ms, hj_result *result);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HJ_H */
