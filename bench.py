@@ -1,0 +1,357 @@
+"""Benchmark of the epsilon-join cardinality path on B200.
+
+Workload (the configuration the headline metric is quoted on): self-join of
+n = 1,000,000 points in d = 64, coordinates i.i.d. uniform [0,1) drawn from
+seed 22 and stored as FP32, eps calibrated from the first 10,000 points so
+that a point has ~32 neighbours (eps = 2.279504; grid pruning is ineffective,
+every one of the n(n-1)/2 pairs is evaluated). A step is one complete join:
+cell keys, EGO sort, stripe index, distance kernel, FP64 recheck of the band,
+count read back.
+
+Metric: pair-distance evaluations per second = n(n-1)/2 per step / step time.
+`value` is measured on inputs already resident in device memory with CUDA
+events on the stream the engine runs on; `e2e` through the public C-ABI call
+with the input in pinned host memory (host->device copy and the count's
+read-back inside the timed region, synchronous calls, host clock).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--form tf32|bf16x3|plain]
+    python bench.py --impl reference ...     (the reference's AVX-512 CPU path)
+
+With N > 1 (torchrun), every rank runs its own replica of the workload on its
+GPU (weak scaling, no data-path collective); rank 0 prints the line with the
+maximum time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_POINTS = 1_000_000
+DIM = 64
+SEED = 22
+NEIGHBOURS = 32
+EPS_CALIBRATED = 2.279504  # calibrate_eps(first 10k points, n=1M, 32 neighbours); re-derived at start-up
+METRIC = "pair-dist evals/s (self-join 1M x 64, exact count)"
+UNIT = "pair-dist evals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="tf32", choices=["tf32", "bf16x3", "plain"])
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison step")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--n", type=int, default=N_POINTS, help=argparse.SUPPRESS)
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def workload(n: int):
+    from hilbertjoin_b200 import workloads as W
+    x = W.uniform(n, DIM, SEED, dtype=np.float32)
+    eps = W.calibrate_eps(x, N_POINTS, NEIGHBOURS)
+    return x, eps
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            self.out.flush()
+            rows = [r.split(",") for r in open(self.out.name).read().strip().splitlines() if r.strip()]
+        except OSError:
+            rows = []
+        finally:
+            try:
+                os.unlink(self.out.name)
+            except OSError:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for i, nm in enumerate(names):
+                if len(r) > 5 + i and "Active" in r[5 + i] and "Not" not in r[5 + i]:
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_baseline(x: np.ndarray, eps: float, budget_s: float = 8.0):
+    """The reference's own CPU path (built from its sources in oracle/_ref) on a
+    bounded sample of the workload: the first n_s points, same eps (still the
+    dense regime, every pair evaluated). Falls back to the oracle's C port when
+    the reference binary cannot run on this host."""
+    import oracle
+    cores = os.cpu_count() or 1
+    exe = oracle.pick_ref_binary(4, cores)
+    xs = x.astype(np.float64)
+    if exe is not None:
+        n_s = 20_000
+        r = oracle.ref_self_count(xs[:n_s], eps, stripes=14, kblock=4, threads=cores)
+        rate = (n_s * (n_s - 1) / 2) / max(r["alg_s"], 1e-6)
+        n_s = int(min(len(xs), max(20_000, np.sqrt(2 * rate * budget_s))))
+        r = oracle.ref_self_count(xs[:n_s], eps, stripes=14, kblock=4, threads=cores)
+        pairs = n_s * (n_s - 1) / 2
+        return {"value": pairs / r["alg_s"], "unit": UNIT, "cores": int(r["threads"]), "kind": "reference",
+                "sample": f"first {n_s} points of the workload, same eps (dense: {pairs:.3e} pairs); "
+                          f"test_ego_loop3_macro, KBLOCK=4, NUM_THREADS={r['threads']}, AVX-512; time = its ALGTIME",
+                "count": r["count"], "alg_s": r["alg_s"]}
+    n_s = 6000
+    t = time.perf_counter()
+    c = oracle.self_count_brute(xs[:n_s], eps, threads=cores)
+    dt = time.perf_counter() - t
+    pairs = n_s * (n_s - 1) / 2
+    return {"value": pairs / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {n_s} points, FP64 brute-force port (reference binary unavailable on this host)",
+            "count": c, "alg_s": dt}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if ws > 1 and rank != 0:
+        return
+    x, eps = workload(N_POINTS)
+    steps = []
+    budget = max(2.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(x, eps, budget_s=budget)
+        if i >= args.warmup:
+            steps.append(r)
+    vals = [s["value"] for s in steps]
+    v = statistics.median(vals)
+    secs = [s["alg_s"] for s in steps]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(secs),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "self-join 1M x 64 uniform FP32 (seed 22), eps for 32 "
+                                            "neighbours; bounded CPU sample per step", "eps": eps},
+            "cpu_baseline": {k: steps[-1][k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    import hilbertjoin_b200 as hj
+
+    n = args.n
+    x, eps = workload(n)
+    if n == N_POINTS:
+        assert abs(eps - EPS_CALIBRATED) < 1e-6, eps
+    pairs = n * (n - 1) / 2
+    xd = torch.from_numpy(x).to(dev)
+    xh = torch.from_numpy(x).pin_memory()
+    xh_np = xh.numpy()
+    stream = torch.cuda.current_stream(dev)
+
+    def step_dev(form):
+        return hj.self_join_count(xd, eps, form=form, return_stats=True)
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up
+    for _ in range(args.warmup):
+        c0, st0 = step_dev(args.form)
+    # timed region: device-resident input
+    counts, kernel_ms, launches = [], [], []
+    props = torch.cuda.get_device_properties(dev)
+    gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(dev.index)
+    with ClockSampler(gpu_id) as clk:
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            c, st = step_dev(args.form)
+            counts.append(c)
+            kernel_ms.append(st["kernel_ms"])
+            launches.append(st["kernel_launches"])
+        e1.record(stream)
+        barrier()
+    clocks = clk.summary()
+    ms = e0.elapsed_time(e1) / args.steps
+    if ws > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    assert len(set(counts)) == 1, counts
+    value = pairs * ws / (ms / 1e3)
+
+    # e2e: the public C-ABI call on pinned host memory (copy in, count out)
+    for _ in range(1):
+        hj.self_join_count(xh_np, eps, form=args.form)
+    barrier()
+    t0 = time.perf_counter()
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(e2e_steps):
+        ce = hj.self_join_count(xh_np, eps, form=args.form)
+    barrier()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    if ws > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    assert ce == counts[0]
+
+    # the plain FP64 form on the same input (the north star's comparison)
+    plain = None
+    if not args.no_plain and args.form != "plain" and rank == 0:
+        step_dev("plain")
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        cp, stp = step_dev("plain")
+        p1.record(stream)
+        torch.cuda.synchronize()
+        pms = p0.elapsed_time(p1)
+        assert cp == counts[0], (cp, counts[0])
+        plain = {"value": pairs / (pms / 1e3), "ms_per_step": pms, "kernel_ms": stp["kernel_ms"],
+                 "count": cp}
+
+    peaks, peak_src = load_peaks()
+    kms = statistics.mean(kernel_ms)
+    if args.form == "plain":
+        flops = 3.0 * DIM * pairs  # direct difference: sub + fma per dim and pair
+        roof = {"bound": "fp64", "achieved": flops / (kms / 1e3) / 1e12, "peak": 37.0, "unit": "TFLOP/s",
+                "peak_source": "datasheet FP64 37 TFLOP/s (assumption; no measured FP64 peak)"}
+    else:
+        flops = 2.0 * DIM * pairs  # Gram form: one multiply-add per dim and pair
+        sustained = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops"))
+        if args.form == "tf32":
+            peak = sustained / 2.0
+            src = f"{peak_src} bf16_tflops_sustained / 2 (TF32 dense = half of BF16)"
+        else:
+            peak = sustained / 3.0
+            src = f"{peak_src} bf16_tflops_sustained / 3 (three BF16 products per algorithmic multiply-add)"
+        roof = {"bound": "tensor", "achieved": flops / (kms / 1e3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                "peak_source": src}
+    roof["frac"] = roof["achieved"] / roof["peak"]
+    roof["kernel"] = "k_join_tc" if args.form != "plain" else "k_join_fp64"
+    roof["kernel_ms"] = kms
+    roof["algorithmic_flops_per_launch"] = flops
+    roof["traffic"] = None
+    tpath = os.path.join(ROOT, "profiles", f"traffic_{roof['kernel']}_{args.form}.json")
+    if os.path.exists(tpath):
+        try:
+            tj = json.load(open(tpath))
+            roof["traffic"] = tj.get("bytes_per_launch_full_size")
+            roof["traffic_source"] = tj.get("source")
+        except (OSError, ValueError):
+            pass
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        try:
+            cpu = cpu_baseline(x, eps)
+        except Exception as e:  # the baseline never blocks the GPU line
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": {"tf32": "tf32", "bf16x3": "bf16x3", "plain": "f64"}[args.form],
+            "data": "synthetic (seeded uniform, FP32)",
+            "config": {"workload": f"self-join {n} x {DIM}, uniform [0,1) FP32 seed {SEED}, eps for {NEIGHBOURS} "
+                                   f"neighbours (dense regime, all pairs evaluated)", "n": n, "d": DIM,
+                       "eps": eps, "form": args.form, "count": counts[0],
+                       "l2": "input 256 MB > 126 MB L2 (no flush needed)",
+                       "parallelism": "replicas" if ws > 1 else "single GPU"},
+            "e2e": {"value": pairs * ws / (e2e_ms / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(x.nbytes), "d2h_bytes_per_step": 8 + 8,
+                    "ms_per_step": e2e_ms, "timing": "host clock around synchronous C-ABI calls"},
+            "gpu_launches": int(sum(launches)),
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "plain_fp64": plain,
+            "vs_plain_fp64": (value / plain["value"]) if plain else None,
+            "stats": {k: st0[k] for k in ("sort_ms", "index_ms", "join_ms", "recheck_ms", "band_pairs",
+                                          "band_halfwidth_rel", "max_abs_err_band", "fp64_items",
+                                          "candidate_pairs", "work_items")},
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -44,10 +44,12 @@ class Opts(ctypes.Structure):
 
 class Stats(ctypes.Structure):
     _fields_ = [("h2d_ms", ctypes.c_double), ("sort_ms", ctypes.c_double), ("index_ms", ctypes.c_double),
-                ("join_ms", ctypes.c_double), ("recheck_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+                ("join_ms", ctypes.c_double), ("kernel_ms", ctypes.c_double),
+                ("recheck_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
                 ("loadpercent", ctypes.c_double), ("candidate_pairs", ctypes.c_uint64),
                 ("tile_pairs", ctypes.c_uint64), ("work_items", ctypes.c_uint64), ("band_pairs", ctypes.c_uint64),
                 ("band_fraction", ctypes.c_double), ("band_halfwidth_rel", ctypes.c_double),
+                ("max_abs_err_band", ctypes.c_double), ("fp64_items", ctypes.c_uint64),
                 ("form_used", ctypes.c_int32), ("stripes", ctypes.c_int32), ("kernel_launches", ctypes.c_int32),
                 ("reserved_i", ctypes.c_int32), ("reserved", ctypes.c_uint64 * 4)]
 
@@ -93,6 +95,9 @@ def lib() -> ctypes.CDLL:
         "hj_join_count_f32": (I, [P, U64, P, U64, U32, D, pO, pU64, pS]),
         "hj_self_join_count_device": (I, [P, I, U64, U32, D, pO, pU64, pS]),
         "hj_join_count_device": (I, [P, U64, P, U64, I, U32, D, pO, pU64, pS]),
+        "hj_debug_tc_estimates": (I, [P, U64, P, U64, U32, I, P]),
+        "hj_ego_sort": (I, [P, U64, U32, D, pO, P, P]),
+        "hj_device_sm_count": (I, [I]),
         "hj_test_ego_loop3_macro": (None, [ctypes.c_size_t, ctypes.c_size_t, D, P, ctypes.POINTER(ctypes.c_size_t),
                                            I, ctypes.POINTER(D), ctypes.POINTER(D), ctypes.POINTER(D)]),
         "hj_test_ego_loop3_noself": (None, [ctypes.c_size_t, ctypes.c_size_t, I, D, P, P,
@@ -199,6 +204,29 @@ def join_count(a, b, eps: float, form="plain", active_dims=None, ref_compat=Fals
         _check(fn(xa.ctypes.data_as(ctypes.c_void_p), xa.shape[0], xb.ctypes.data_as(ctypes.c_void_p), xb.shape[0],
                   xa.shape[1], float(eps), ctypes.byref(opts), ctypes.byref(c), ctypes.byref(o)))
     return (int(c.value), o.to_dict()) if return_stats else int(c.value)
+
+
+def ego_sort(points, eps: float, device=None):
+    """(perm, sorted_rows): the device epsilon-grid order of `points` (stable)."""
+    x = np.ascontiguousarray(np.asarray(points, dtype=np.float64))
+    perm = np.zeros(x.shape[0], dtype=np.uint64)
+    srt = np.zeros_like(x)
+    opts = _opts("plain", None, False, device, None)
+    _check(lib().hj_ego_sort(x.ctypes.data_as(ctypes.c_void_p), x.shape[0], x.shape[1], float(eps),
+                             ctypes.byref(opts), perm.ctypes.data_as(ctypes.c_void_p),
+                             srt.ctypes.data_as(ctypes.c_void_p)))
+    return perm, srt
+
+
+def tc_estimates(a, b, form="tf32") -> np.ndarray:
+    """Testing hook: the tensor-core dist^2 estimate of every pair (FP32 inputs)."""
+    xa = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+    xb = np.ascontiguousarray(np.asarray(b, dtype=np.float32))
+    out = np.zeros((xa.shape[0], xb.shape[0]), dtype=np.float32)
+    _check(lib().hj_debug_tc_estimates(xa.ctypes.data_as(ctypes.c_void_p), xa.shape[0],
+                                       xb.ctypes.data_as(ctypes.c_void_p), xb.shape[0], xa.shape[1],
+                                       FORMS[form], out.ctypes.data_as(ctypes.c_void_p)))
+    return out
 
 
 def test_ego_loop3_macro(array, eps: float, stripes: int = 14):

@@ -131,7 +131,7 @@ enum {
     kSlotKeysWmA, kSlotKeysWmB, kSlotPermA, kSlotPermB, kSlotPermTmp, kSlotHist,
     kSlotRowsA, kSlotRowsB, kSlotKeysA, kSlotKeysB, kSlotTilesA, kSlotTilesB,
     kSlotTf32A, kSlotTf32B, kSlotHiA, kSlotLoA, kSlotHiB, kSlotLoB, kSlotNormA, kSlotNormB,
-    kSlotTmaxAA, kSlotTmaxAB, kSlotTmaxBA, kSlotTmaxBB, kSlotBand,
+    kSlotTmaxAA, kSlotTmaxAB, kSlotTmaxBA, kSlotTmaxBB, kSlotBand, kSlotCenter, kSlotGminA, kSlotGminB,
 };
 
 static int bitwidth(unsigned long long v) {
@@ -218,13 +218,18 @@ static float ev_ms(cudaEvent_t a, cudaEvent_t b) {
 
 // Sorts one set and gathers the layouts the chosen form needs.
 static int prepare_set(Ctx *c, cudaStream_t st, const void *x, uint64_t n, int dtype_bytes, const Grid &g,
-                       const GridDev &gd, int form, bool is_b, SortedSet *out, int *launches) {
+                       const GridDev &gd, const double *center, double norm_scale, int form, bool is_b,
+                       SortedSet *out, int *launches) {
     SortedSet s;
     s.n = n;
     s.d = g.d;
     s.dtype_bytes = dtype_bytes;
+    s.src = x;
+    s.center = center;
     const uint32_t W = g.W;
-    uint32_t *keys_wm = (uint32_t *)slot_alloc_impl(c, st, is_b ? kSlotKeysWmB : kSlotKeysWmA, n * W * 4);
+    const bool norm_order = form == HJ_FORM_TC_TF32 || form == HJ_FORM_TC_BF16X3;
+    uint32_t *keys_wm = (uint32_t *)slot_alloc_impl(c, st, is_b ? kSlotKeysWmB : kSlotKeysWmA,
+                                                    n * (W + (norm_order ? 1 : 0)) * 4);
     uint32_t *perm = (uint32_t *)slot_alloc_impl(c, st, is_b ? kSlotPermB : kSlotPermA, n * 4);
     uint32_t *ptmp = (uint32_t *)slot_alloc_impl(c, st, kSlotPermTmp, n * 4);
     uint32_t *hist = (uint32_t *)slot_alloc_impl(c, st, kSlotHist, radix_hist_entries(n) * 4);
@@ -258,15 +263,38 @@ static int prepare_set(Ctx *c, cudaStream_t st, const void *x, uint64_t n, int d
                                                     (s.npad_tc / kTcTileA) * 4);
         s.tile_maxnorm_b = (float *)slot_alloc_impl(c, st, is_b ? kSlotTmaxBB : kSlotTmaxAB,
                                                     (s.npad_tc / kTcTileB) * 4);
-        if (!s.norms || !s.tile_maxnorm_a || !s.tile_maxnorm_b) return fail(HJ_ERR_OOM, "out of device memory");
+        s.group_minnorm = (float *)slot_alloc_impl(c, st, is_b ? kSlotGminB : kSlotGminA, (s.npad_tc / 32) * 4);
+        if (!s.norms || !s.tile_maxnorm_a || !s.tile_maxnorm_b || !s.group_minnorm)
+            return fail(HJ_ERR_OOM, "out of device memory");
         flags |= kGatherNorms;
     }
     launch_pack_keys(x, dtype_bytes, n, g.d, g.eps, gd, W, keys_wm, st);
     *launches += 1;
-    radix_sort_perm(keys_wm, n, g.passes, perm, ptmp, hist, st, launches);
+    if (norm_order) {
+        // least significant key: the quantised norm (ties within a cell by norm)
+        launch_norm_key(x, dtype_bytes, n, g.d, center, norm_scale, keys_wm + (size_t)W * n, st);
+        std::vector<std::pair<uint32_t, uint32_t>> passes = {{W, 0u}, {W, 8u}};
+        passes.insert(passes.end(), g.passes.begin(), g.passes.end());
+        radix_sort_perm(keys_wm, n, passes, perm, ptmp, hist, st, launches);
+        *launches += 1;
+    } else {
+        radix_sort_perm(keys_wm, n, g.passes, perm, ptmp, hist, st, launches);
+    }
     launch_gather(x, dtype_bytes, n, g.d, perm, keys_wm, W, s, flags, st, launches);
     *out = s;
     return check_cuda("sort stage");
+}
+
+// The plain FP64 tile layout of a set prepared for a tensor-core form, for the
+// work items routed to the FP64 kernel (padded to the 256-rank B tiles).
+static int ensure_plain_tiles(Ctx *c, cudaStream_t st, SortedSet *s, bool is_b, int *launches) {
+    if (s->tiles64) return HJ_OK;
+    s->n_tiles64 = s->npad_tc / kPlainTile;
+    s->tiles64 = (double *)slot_alloc_impl(c, st, is_b ? kSlotTilesB : kSlotTilesA,
+                                           s->n_tiles64 * s->d * kPlainTile * 8);
+    if (!s->tiles64) return fail(HJ_ERR_OOM, "out of device memory");
+    launch_gather(s->src, s->dtype_bytes, s->n, s->d, s->perm, nullptr, 0, *s, kGatherPlain, st, launches);
+    return check_cuda("plain layout");
 }
 
 static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *count, hj_stats *stats,
@@ -324,12 +352,37 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
     cudaMemcpyAsync(gd.word, g.word.data(), d * 4, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(gd.shift, g.shift.data(), d * 4, cudaMemcpyHostToDevice, st);
 
+    // per-dim midpoint of the coordinate range: the shift of the tensor-core operands
+    double *center = (double *)slot_alloc_impl(c, st, kSlotCenter, d * 8);
+    if (!center) return fail(HJ_ERR_OOM, "out of device memory");
+    double norm_scale = 0.0;
+    {
+        std::vector<double> hc(d);
+        double nmax = 0.0;
+        for (uint32_t t = 0; t < d; ++t) {
+            if (hds[t].cmin > hds[t].cmax) {
+                hc[t] = 0.0;
+                continue;
+            }
+            const double lo = double_from_ordered(hds[t].xmin), hi = double_from_ordered(hds[t].xmax);
+            hc[t] = 0.5 * lo + 0.5 * hi;
+            const double r = std::fmax(hi - hc[t], hc[t] - lo);
+            nmax += r * r;
+        }
+        norm_scale = nmax > 0 ? 65535.0 / (nmax * 1.001) : 0.0;
+        cudaMemcpyAsync(center, hc.data(), d * 8, cudaMemcpyHostToDevice, st);
+        cudaStreamSynchronize(st);  // hc goes out of scope
+    }
+
     // 2. EGO sort + layouts
     SortedSet A, B;
-    if (int r = prepare_set(c, st, in.a, in.na, in.dtype_bytes, g, gd, form, false, &A, &launches)) return r;
+    if (int r = prepare_set(c, st, in.a, in.na, in.dtype_bytes, g, gd, center, norm_scale, form, false, &A,
+                            &launches))
+        return r;
     if (in.self) {
         B = A;
-    } else if (int r = prepare_set(c, st, in.b, in.nb, in.dtype_bytes, g, gd, form, true, &B, &launches)) {
+    } else if (int r = prepare_set(c, st, in.b, in.nb, in.dtype_bytes, g, gd, center, norm_scale, form, true, &B,
+                                   &launches)) {
         return r;
     }
     cudaEventRecord(c->ev[2], st);
@@ -353,58 +406,104 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
     if (r) return fail(HJ_ERR_INVALID_ARG, err);
     cudaEventRecord(c->ev[3], st);
 
-    // 4. distance kernels
+    // 4. distance kernels. d_small: [2] count of the tensor-core kernel and the
+    // recheck, [3] error word, [4] band pairs, [5] max band error bits,
+    // [6] count of the FP64 kernel.
     unsigned long long *d_count = c->d_small + 2;
     uint32_t *d_err = reinterpret_cast<uint32_t *>(c->d_small + 3);
     unsigned long long *d_band = c->d_small + 4;
-    cudaMemsetAsync(c->d_small + 2, 0, 3 * sizeof(unsigned long long), st);
-    uint64_t band_total = 0;
+    unsigned long long *d_count_fp = c->d_small + 6;
+    cudaMemsetAsync(c->d_small + 2, 0, 5 * sizeof(unsigned long long), st);
+    uint64_t band_total = 0, fp_items = 0;
     double c_rel = 0, c_abs = 0;
+    const double T = in.eps * in.eps;
+    cudaEventRecord(c->ev[6], st);
     if (!tc) {
-        launch_join_fp64(A, B, in.self, na_eff, nb_eff, in.eps * in.eps, idx, d_count, d_err, c->num_sms, st);
+        launch_join_fp64(A, B, in.self, na_eff, nb_eff, T, idx, d_count_fp, d_err, c->num_sms, st);
         ++launches;
         cudaEventRecord(c->ev[4], st);
         cudaEventRecord(c->ev[5], st);
     } else {
         tc_band_constants(form, d, maxabs, &c_rel, &c_abs);
-        TcParams p{form, in.eps * in.eps, c_rel, c_abs};
-        uint64_t cap = std::max<uint64_t>(1ull << 20, idx.candidate_pairs / 4096);
+        TcParams p{form, T, c_rel, c_abs};
+        // Items whose error band would exceed half of eps^2 (eps^2 tiny against
+        // the squared norms: the cancellation limit of the norm expansion) run
+        // on the FP64 kernel instead.
+        IndexResult idx_tc, idx_fp;
         for (int attempt = 0;; ++attempt) {
-            uint2 *band = (uint2 *)slot_alloc_impl(c, st, kSlotBand, cap * sizeof(uint2));
-            if (!band) return fail(HJ_ERR_OOM, "out of device memory (band queue)");
-            cudaMemsetAsync(c->d_small + 2, 0, 3 * sizeof(unsigned long long), st);
-            std::string terr;
-            if (launch_join_tc(A, B, in.self, na_eff, nb_eff, p, idx, d_count, band, cap, d_band, d_err, c->num_sms,
-                               st, &terr))
-                return fail(HJ_ERR_CUDA, terr);
-            ++launches;
-            cudaEventRecord(c->ev[4], st);
-            cudaMemcpyAsync(c->h_small + 4, d_band, 8, cudaMemcpyDeviceToHost, st);
-            if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("tensor-core join");
-            band_total = c->h_small[4];
-            if (band_total <= cap) {
-                launch_recheck(A, B, p.T, band, d_band, cap, d_count, st);
+            const double limit = attempt == 0 ? 0.5 * T : -1.0;  // -1: everything to FP64
+            int sr = split_items_by_precision(idx, A, B, c_rel, c_abs, limit, slot_alloc_cb, &actx, st, &idx_tc,
+                                              &idx_fp);
+            if (sr == 2) return fail(HJ_ERR_OOM, "out of device memory (work list split)");
+            if (sr) return check_cuda("work list split");
+            launches += 2;
+            fp_items = idx_fp.n_items;
+            cudaMemsetAsync(c->d_small + 2, 0, 5 * sizeof(unsigned long long), st);
+            if (idx_fp.n_items) {
+                if (int rr = ensure_plain_tiles(c, st, &A, false, &launches)) return rr;
+                if (in.self)
+                    B.tiles64 = A.tiles64, B.n_tiles64 = A.n_tiles64;
+                else if (int rr = ensure_plain_tiles(c, st, &B, true, &launches))
+                    return rr;
+                launch_join_fp64(A, B, in.self, na_eff, nb_eff, T, idx_fp, d_count_fp, d_err, c->num_sms, st);
                 ++launches;
+            }
+            if (idx_tc.n_items == 0) {
+                cudaEventRecord(c->ev[4], st);
                 cudaEventRecord(c->ev[5], st);
                 break;
             }
-            if (attempt >= 3) return fail(HJ_ERR_BAND_OVERFLOW, "band queue overflow");
-            cap = band_total + band_total / 4 + 1024;
+            const uint64_t cand_tc = idx_tc.tile_pairs * (uint64_t)kTcTileA * kTcTileB;
+            uint64_t cap = std::max<uint64_t>(1ull << 20, cand_tc / 4096);
+            const uint64_t cap_limit = std::max<uint64_t>(1ull << 27, cand_tc / 64);
+            bool done = false, fallback = false;
+            for (int grow = 0; grow < 4; ++grow) {
+                uint2 *band = (uint2 *)slot_alloc_impl(c, st, kSlotBand, cap * kBandEntryBytes);
+                if (!band) return fail(HJ_ERR_OOM, "out of device memory (band queue)");
+                cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), st);
+                cudaMemsetAsync(d_band, 0, 2 * sizeof(unsigned long long), st);
+                std::string terr;
+                cudaEventRecord(c->ev[6], st);
+                if (launch_join_tc(A, B, in.self, na_eff, nb_eff, p, idx_tc, d_count, band, cap, d_band, d_err,
+                                   c->num_sms, st, &terr))
+                    return fail(HJ_ERR_CUDA, terr);
+                ++launches;
+                cudaEventRecord(c->ev[4], st);
+                cudaMemcpyAsync(c->h_small + 4, d_band, 8, cudaMemcpyDeviceToHost, st);
+                if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("tensor-core join");
+                band_total = c->h_small[4];
+                if (band_total <= cap) {
+                    launch_recheck(A, B, T, band, d_band, cap, d_count,
+                                   reinterpret_cast<unsigned int *>(c->d_small + 5), st);
+                    ++launches;
+                    cudaEventRecord(c->ev[5], st);
+                    done = true;
+                    break;
+                }
+                if (band_total > cap_limit) {  // band too wide to be worth rechecking
+                    fallback = true;
+                    break;
+                }
+                cap = band_total + band_total / 4 + 1024;
+            }
+            if (done) break;
+            if (!fallback || attempt >= 1) return fail(HJ_ERR_BAND_OVERFLOW, "band queue overflow");
         }
     }
-    cudaMemcpyAsync(c->h_small + 2, c->d_small + 2, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(c->h_small + 2, c->d_small + 2, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("distance kernel");
     if (int rr = check_cuda("distance kernel")) return rr;
     const uint32_t kerr = (uint32_t)c->h_small[3];
     if (kerr & kErrTimeout) return fail(HJ_ERR_TIMEOUT, "a bounded device-side wait timed out");
     if (kerr) return fail(HJ_ERR_CUDA, "device error word set");
-    *count = c->h_small[2];
+    *count = c->h_small[2] + c->h_small[6];
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
         if (ev_h2d_start) stats->h2d_ms = ev_ms(ev_h2d_start, c->ev[1]);
         stats->sort_ms = ev_ms(c->ev[1], c->ev[2]);
         stats->index_ms = ev_ms(c->ev[2], c->ev[3]);
         stats->join_ms = ev_ms(c->ev[3], c->ev[4]);
+        stats->kernel_ms = ev_ms(c->ev[6], c->ev[4]);
         stats->recheck_ms = ev_ms(c->ev[4], c->ev[5]);
         stats->total_ms =
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_wall0).count() +
@@ -418,7 +517,14 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
         stats->band_pairs = band_total;
         stats->band_fraction = idx.candidate_pairs ? (double)band_total / (double)idx.candidate_pairs : 0.0;
         stats->band_halfwidth_rel = c_rel;
+        {
+            uint32_t eb = (uint32_t)c->h_small[5];
+            float ef;
+            std::memcpy(&ef, &eb, 4);
+            stats->max_abs_err_band = tc ? (double)ef : 0.0;
+        }
         stats->form_used = form;
+        stats->fp64_items = fp_items;
         int s = active_dims;
         int p3 = 1;
         for (int i = 0; i < s; ++i) p3 *= 3;
@@ -615,6 +721,35 @@ int hj_join_count_f32(const float *A, uint64_t nA, const float *B, uint64_t nB, 
 int hj_ego_sort(const double *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts, uint64_t *perm,
                 double *sorted) {
     return ego_sort_host(pts, n, d, eps, opts, perm, sorted);
+}
+
+int hj_debug_tc_estimates(const float *A, uint64_t nA, const float *B, uint64_t nB, uint32_t d, int form,
+                          float *out) {
+    tl_error.clear();
+    if (!A || !B || !out || nA == 0 || nB == 0) return fail(HJ_ERR_INVALID_ARG, "null pointer or empty set");
+    if (form != HJ_FORM_TC_TF32 && form != HJ_FORM_TC_BF16X3) return fail(HJ_ERR_INVALID_ARG, "not a tensor-core form");
+    Ctx *c;
+    if (int r = get_ctx(-1, &c)) return r;
+    float *dbg = nullptr;
+    if (cudaMalloc(&dbg, nA * nB * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(HJ_ERR_OOM, "out of device memory");
+    }
+    double mx = 0;
+    for (uint64_t i = 0; i < nA * d; ++i) mx = std::fmax(mx, std::fabs((double)A[i]));
+    for (uint64_t i = 0; i < nB * d; ++i) mx = std::fmax(mx, std::fabs((double)B[i]));
+    hj_opts o;
+    hj_opts_init(&o);
+    o.form = form;
+    o.active_dims = 0;
+    uint64_t cnt;
+    set_tc_debug_output(dbg);
+    int r = hj_join_count_f32(A, nA, B, nB, d, 4.0 * (mx + 1.0) * std::sqrt((double)d), &o, &cnt, nullptr);
+    set_tc_debug_output(nullptr);
+    if (r == HJ_OK && cudaMemcpy(out, dbg, nA * nB * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+        r = check_cuda("debug copy");
+    cudaFree(dbg);
+    return r;
 }
 
 int hj_self_join_count_device(const void *pts, int dtype_bytes, uint64_t n, uint32_t d, double eps,

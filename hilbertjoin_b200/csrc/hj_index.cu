@@ -303,7 +303,78 @@ __global__ void k_permute_items(const WorkItem *__restrict__ in, const uint32_t 
 
 // Scratch slots requested through the caller's allocator.
 enum { kSlotRuns = 40, kSlotNruns, kSlotCounts, kSlotItemsTmp, kSlotItems, kSlotItemKeys, kSlotItemPerm,
-       kSlotItemPermTmp, kSlotItemHist, kSlotIdxStats };
+       kSlotItemPermTmp, kSlotItemHist, kSlotIdxStats, kSlotSplitFlags, kSlotSplitTc, kSlotSplitFp, kSlotSplitStats };
+
+__global__ void k_item_precision_flags(const WorkItem *__restrict__ items, uint64_t n, const float *__restrict__ tmax_a,
+                                       const float *__restrict__ tmax_b, double c_rel, double c_abs, double limit,
+                                       uint32_t *flags, unsigned long long *tile_pairs_fp) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const WorkItem w = items[i];
+    float mb = 0.f;
+    for (uint32_t b = w.b0; b < w.b1; ++b) mb = fmaxf(mb, tmax_b[b]);
+    const double tau = c_rel * ((double)tmax_a[w.a] + (double)mb) + c_abs;
+    const bool tc = tau <= limit;
+    flags[i] = tc ? 1u : 0u;
+    if (!tc) atomicAdd(tile_pairs_fp, (unsigned long long)(w.b1 - w.b0));
+}
+
+// flags[] holds the exclusive prefix count of tensor-core items.
+__global__ void k_item_split(const WorkItem *__restrict__ items, uint64_t n, const uint32_t *__restrict__ flags_scan,
+                             unsigned long long n_tc, WorkItem *tc_out, WorkItem *fp_out) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t before = flags_scan[i];
+    const uint32_t next = i + 1 < n ? flags_scan[i + 1] : (uint32_t)n_tc;
+    const WorkItem w = items[i];
+    if (next != before) {
+        tc_out[before] = w;
+    } else {
+        const uint64_t k = 2 * (i - before);
+        const uint32_t r = kTcTileA / kPlainTile, c = kTcTileB / kPlainTile;
+        for (uint32_t h = 0; h < r; ++h) {
+            WorkItem p;
+            p.a = w.a * r + h;
+            p.b0 = w.b0 * c;
+            p.b1 = w.b1 * c;
+            p.pad = 0;
+            fp_out[k + h] = p;
+        }
+    }
+}
+
+int split_items_by_precision(const IndexResult &in, const SortedSet &A, const SortedSet &B, double c_rel,
+                             double c_abs, double limit, void *(*alloc)(void *ctx, int slot, size_t bytes),
+                             void *actx, cudaStream_t st, IndexResult *tc_out, IndexResult *fp_out) {
+    *tc_out = in;
+    *fp_out = IndexResult();
+    if (in.n_items == 0) return 0;
+    const uint64_t n = in.n_items;
+    uint32_t *flags = (uint32_t *)alloc(actx, kSlotSplitFlags, (n + 1) * sizeof(uint32_t));
+    unsigned long long *stats = (unsigned long long *)alloc(actx, kSlotSplitStats, 2 * sizeof(unsigned long long));
+    if (!flags || !stats) return 2;
+    cudaMemsetAsync(stats, 0, 2 * sizeof(unsigned long long), st);
+    k_item_precision_flags<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(in.items, n, A.tile_maxnorm_a,
+                                                                         B.tile_maxnorm_b, c_rel, c_abs, limit,
+                                                                         flags, stats + 1);
+    launch_scan_u32(flags, n, stats, st);
+    unsigned long long h[2];
+    cudaMemcpyAsync(h, stats, sizeof(h), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return 3;
+    const uint64_t n_tc = h[0], n_fp = n - n_tc;
+    if (n_fp == 0) return 0;
+    WorkItem *tc = (WorkItem *)alloc(actx, kSlotSplitTc, (n_tc + 1) * sizeof(WorkItem));
+    WorkItem *fp = (WorkItem *)alloc(actx, kSlotSplitFp, 2 * n_fp * sizeof(WorkItem));
+    if (!tc || !fp) return 2;
+    k_item_split<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(in.items, n, flags, n_tc, tc, fp);
+    tc_out->items = tc;
+    tc_out->n_items = n_tc;
+    tc_out->tile_pairs = in.tile_pairs - h[1];
+    fp_out->items = fp;
+    fp_out->n_items = 2 * n_fp;
+    fp_out->tile_pairs = h[1] * (kTcTileA / kPlainTile) * (kTcTileB / kPlainTile);
+    return 0;
+}
 
 int build_index(const SortedSet &A, const SortedSet &B, const Grid &grid, const GridDev &gdev, bool self,
                 uint64_t na_eff, uint64_t nb_eff, int tile_a, int tile_b, int active_dims, uint32_t chunk,

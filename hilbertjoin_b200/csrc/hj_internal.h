@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string.h>
+
 #include <string>
 #include <vector>
 
@@ -22,7 +24,21 @@ constexpr uint32_t kMaxDim = 1024;
 // the device: cell index range and the largest |coordinate|.
 struct DimStats {
     long long cmin, cmax;
+    unsigned long long xmin, xmax;  // coordinate range, order-preserving encoding of the FP64 bits
 };
+
+// FP64 <-> unsigned integer with the same order (for atomic min/max).
+__host__ __device__ inline unsigned long long ordered_from_double(double v) {
+    unsigned long long u;
+    memcpy(&u, &v, 8);
+    return (u >> 63) ? ~u : (u | (1ull << 63));
+}
+__host__ __device__ inline double double_from_ordered(unsigned long long u) {
+    u = (u >> 63) ? (u & ~(1ull << 63)) : ~u;
+    double v;
+    memcpy(&v, &u, 8);
+    return v;
+}
 
 // The epsilon grid shared by the sets of one join. Cell of a coordinate x in
 // dim t: c = floor(x / eps) (FP64). A packed key stores per dim the field
@@ -55,6 +71,7 @@ struct SortedSet {
     uint64_t n = 0;
     uint32_t d = 0;
     int dtype_bytes = 8;         // precision of the input (8 = FP64, 4 = FP32)
+    const void *src = nullptr;   // the input rows (device), in input order
     const void *rows = nullptr;  // sorted rows, input precision, [n][d]
     uint32_t *keys = nullptr;    // sorted packed keys, [n][W]
     uint32_t *perm = nullptr;
@@ -65,9 +82,11 @@ struct SortedSet {
     float *tf32 = nullptr;       // TF32-rounded values in FP32 containers, kpad = roundup(d, 32)
     uint16_t *bf_hi = nullptr;   // BF16 split, kpad16 = roundup(d, 64)
     uint16_t *bf_lo = nullptr;
-    float *norms = nullptr;      // FP32(|x|^2 in FP64); padding rows hold kPadNorm
+    const double *center = nullptr;  // per-dim shift of the tensor-core operands (shared by A and B)
+    float *norms = nullptr;      // FP32(|x - center|^2 in FP64); padding rows hold kPadNorm
     float *tile_maxnorm_a = nullptr;  // per 128-row tile
     float *tile_maxnorm_b = nullptr;  // per 256-row tile
+    float *group_minnorm = nullptr;   // per 32-row group: min |x - center|^2
     uint64_t npad_tc = 0;
     uint32_t kpad_tf32 = 0, kpad_bf16 = 0;
 };
@@ -79,6 +98,15 @@ constexpr float kPadNorm = 1.0e30f;
 struct WorkItem {
     uint32_t a, b0, b1, pad;
 };
+
+// Splits a tensor-core work list (128 x 256 tiles) by precision: items whose
+// error bound c_rel * (max |a|^2 + max |b|^2) + c_abs exceeds `limit` go, as
+// 64 x 64 items, to the plain FP64 kernel. Order (Hilbert) is preserved in both
+// lists. Synchronises once on `st`.
+struct IndexResult;
+int split_items_by_precision(const IndexResult &tc_in, const SortedSet &A, const SortedSet &B, double c_rel,
+                             double c_abs, double limit, void *(*alloc)(void *ctx, int slot, size_t bytes),
+                             void *actx, cudaStream_t st, IndexResult *tc_out, IndexResult *fp_out);
 
 struct IndexResult {
     WorkItem *items = nullptr;  // device, Hilbert ordered
@@ -99,6 +127,12 @@ void launch_dim_stats_init(DimStats *dstats, uint32_t d, unsigned long long *d_m
 // Packed keys, word-major [W][n].
 void launch_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, const GridDev &g,
                       uint32_t W, uint32_t *keys_wm, cudaStream_t st);
+
+// Quantised |x - center|^2 (16 bits, key = min(65535, floor(norm * scale))),
+// the least significant sort key of the tensor-core forms: points of one cell
+// end up ordered by norm, so that 32 consecutive ranks have near-equal norms.
+void launch_norm_key(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const double *center, double scale,
+                     uint32_t *key_out, cudaStream_t st);
 
 // Stable LSD radix sort of a permutation by 8-bit windows of word-major keys.
 // `passes` in order (least significant first). Needs scratch: perm_tmp[n],
@@ -138,13 +172,18 @@ struct TcParams {
     double c_rel;         // band half-width: c_rel * (|a|^2 + |b|^2) + c_abs
     double c_abs;
 };
+// Band entries are 16 bytes (kBandEntryBytes).
+constexpr size_t kBandEntryBytes = 16;
 int launch_join_tc(const SortedSet &A, const SortedSet &B, bool self, uint64_t na_eff, uint64_t nb_eff,
                    const TcParams &p, const IndexResult &idx, unsigned long long *d_count, uint2 *band,
                    uint64_t band_cap, unsigned long long *d_band_total, uint32_t *d_err, int num_sms,
                    cudaStream_t st, std::string *err);
 void launch_recheck(const SortedSet &A, const SortedSet &B, double T, const uint2 *band,
                     const unsigned long long *d_band_total, uint64_t band_cap, unsigned long long *d_count,
-                    cudaStream_t st);
+                    unsigned int *d_max_err_bits, cudaStream_t st);
+// Test hook: when non-null, the tensor-core kernel writes its dist^2 estimate
+// of every pair to dbg[ia * nb + jb] (EGO ranks). Not thread-safe.
+void set_tc_debug_output(float *dbg);
 // Error-bound constant of a tensor-core form for dimension d.
 void tc_band_constants(int form, uint32_t d, double maxabs, double *c_rel, double *c_abs);
 

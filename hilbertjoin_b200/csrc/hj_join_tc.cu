@@ -1,24 +1,708 @@
-// hj_join_tc.cu -- tensor-core forms (placeholder until the tcgen05 kernel lands).
+// hj_join_tc.cu -- tensor-core forms (HJ_FORM_TC_TF32, HJ_FORM_TC_BF16X3).
+//
+// Replaces the same block-pair kernel as hj_join_fp64.cu (the reference's
+// EGO_LOOP_TRAN[_NOSELF], hilbertjoin/egojoin.h:311-392, :482-553), but with
+// the norm expansion the reference itself uses,
+//     |a - b|^2 = |a|^2 + |b|^2 - 2 a.b      (egojoin.h:182-195, :329-381),
+// and the a.b tile on the 5th-generation tensor cores:
+//
+//   * one persistent CTA per SM, 6 warps, warp-specialised:
+//       warp 0   TMA producer: the A tile (128 EGO ranks x K) once per work
+//                item into one of two A buffers, then the B tiles (256 ranks)
+//                one 128-byte K atom (32 KB) at a time into a ring of stages;
+//       warp 1   MMA issuer (one thread): tcgen05.mma, M=128, N=256, operands
+//                from shared memory (128-byte swizzled, K-major), accumulator
+//                in tensor memory, two accumulators in flight (512 columns);
+//       warps 2-9 epilogue: tcgen05.ld of the accumulator rows (TMEM lane
+//                quadrant = warp % 4, two warps per quadrant on 128 columns
+//                each), dist^2 estimate, classification, count;
+//   * TF32: operands rounded to TF32 on the device (round to nearest), one
+//     MMA per K step; BF16X3: a = a_hi + a_lo in BF16, a.b =
+//     a_hi.b_hi + a_lo.b_hi + a_hi.b_lo (three MMAs per K step);
+//   * exact count: with s = |a|^2 + |b|^2 - 2 v (v the tensor-core dot product),
+//     every error of v, of the FP32 norms and of the FP32 epilogue is bounded
+//     by c_rel * (|a|^2 + |b|^2) + c_abs (tc_band_constants). A pair with
+//     s + bound <= eps^2 is certainly inside, one with s - bound > eps^2 is
+//     certainly outside, and every other pair (the band) is queued and
+//     re-evaluated by k_recheck with the FP64 pair test. So the count equals
+//     the plain FP64 form's, bit for bit.
+//   * fast path: per row and 32-column half the epilogue takes the minimum of
+//     |b|^2 - 2 v; only if that can still reach eps^2 + bound (rare: neighbours
+//     are a small fraction of the candidates) does the warp classify the half,
+//     branch-free against per-tile bounds, and queue the band pairs.
+//
+// Every mbarrier wait is bounded in time (hj_common.cuh); on a timeout the
+// kernel raises kErrTimeout, drains its outstanding copies and MMAs, frees its
+// tensor memory and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <mutex>
+#include <string>
+
+#include "../../include/hj.h"
 #include "hj_common.cuh"
 #include "hj_internal.h"
-#include "../../include/hj.h"
 
 namespace hj {
 
+constexpr int kEpiWarps = 8;  // two per TMEM lane quadrant, each on half of the columns
+constexpr int kTcThreads = 64 + 32 * kEpiWarps;
+constexpr uint32_t kAtomBytes = 128;                  // bytes of K per row per swizzle atom
+constexpr uint32_t kAStageBytes = kTcTileA * kAtomBytes;  // 16 KB per A atom
+constexpr uint32_t kBStageBytes = kTcTileB * kAtomBytes;  // 32 KB per B atom
+constexpr uint32_t kTmemCols = 512;
+
+struct BandEntry {
+    uint32_t ia, jb;  // EGO ranks in A and B
+    float s_hat;      // tensor-core estimate of dist^2
+    uint32_t pad;
+};
+
+struct TcArgs {
+    uint32_t ka;        // K atoms per operand (TF32: kpad/32; BF16: kpad16/64)
+    uint32_t a_bufs;    // 1 or 2 A buffers
+    uint32_t nst;       // B ring stages
+    const WorkItem *items;
+    uint64_t n_items;
+    const float *norm_a, *norm_b;   // FP32 |x|^2 per EGO rank (padding: kPadNorm)
+    const float *tmax_b;            // per 256-rank B tile: max |x|^2
+    const float *gmin_b;            // per 32-rank B group: min |x|^2
+    uint64_t na, nb;                // ranks counted
+    int self;
+    double T, c_rel, c_abs;
+    float T_lo, T_hi;      // eps^2 rounded down / up to FP32
+    float c_rel_f, c_abs_f;  // rounded up to FP32
+    unsigned long long *count;
+    BandEntry *band;
+    uint64_t band_cap;
+    unsigned long long *band_total;
+    uint32_t *err;
+    float *dbg;                     // optional: s_hat for every pair, input order [na][nb] (tests)
+    const uint32_t *perm_a, *perm_b;  // EGO rank -> input index (for dbg)
+};
+
+// ---------------------------------------------------------------- PTX helpers
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t *dst_smem, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+template <int FORM>
+__device__ __forceinline__ void mma_issue(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    if constexpr (FORM == HJ_FORM_TC_TF32) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+            : "memory");
+    }
+}
+
+// 32 consecutive accumulator columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// 64 consecutive accumulator columns of this thread's TMEM lane (two x32
+// loads, one wait).
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
+    uint32_t r[64];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+            "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+            "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+            : "=r"(r[32 * h + 0]), "=r"(r[32 * h + 1]), "=r"(r[32 * h + 2]), "=r"(r[32 * h + 3]),
+              "=r"(r[32 * h + 4]), "=r"(r[32 * h + 5]), "=r"(r[32 * h + 6]), "=r"(r[32 * h + 7]),
+              "=r"(r[32 * h + 8]), "=r"(r[32 * h + 9]), "=r"(r[32 * h + 10]), "=r"(r[32 * h + 11]),
+              "=r"(r[32 * h + 12]), "=r"(r[32 * h + 13]), "=r"(r[32 * h + 14]), "=r"(r[32 * h + 15]),
+              "=r"(r[32 * h + 16]), "=r"(r[32 * h + 17]), "=r"(r[32 * h + 18]), "=r"(r[32 * h + 19]),
+              "=r"(r[32 * h + 20]), "=r"(r[32 * h + 21]), "=r"(r[32 * h + 22]), "=r"(r[32 * h + 23]),
+              "=r"(r[32 * h + 24]), "=r"(r[32 * h + 25]), "=r"(r[32 * h + 26]), "=r"(r[32 * h + 27]),
+              "=r"(r[32 * h + 28]), "=r"(r[32 * h + 29]), "=r"(r[32 * h + 30]), "=r"(r[32 * h + 31])
+            : "r"(taddr + 32 * h));
+    }
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// 128 consecutive accumulator columns of this thread's TMEM lane (four x32
+// loads, one wait).
+__device__ __forceinline__ void tmem_ld128(uint32_t taddr, float (&v)[128]) {
+    uint32_t r[128];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+            "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+            "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+            : "=r"(r[32 * h + 0]), "=r"(r[32 * h + 1]), "=r"(r[32 * h + 2]), "=r"(r[32 * h + 3]),
+              "=r"(r[32 * h + 4]), "=r"(r[32 * h + 5]), "=r"(r[32 * h + 6]), "=r"(r[32 * h + 7]),
+              "=r"(r[32 * h + 8]), "=r"(r[32 * h + 9]), "=r"(r[32 * h + 10]), "=r"(r[32 * h + 11]),
+              "=r"(r[32 * h + 12]), "=r"(r[32 * h + 13]), "=r"(r[32 * h + 14]), "=r"(r[32 * h + 15]),
+              "=r"(r[32 * h + 16]), "=r"(r[32 * h + 17]), "=r"(r[32 * h + 18]), "=r"(r[32 * h + 19]),
+              "=r"(r[32 * h + 20]), "=r"(r[32 * h + 21]), "=r"(r[32 * h + 22]), "=r"(r[32 * h + 23]),
+              "=r"(r[32 * h + 24]), "=r"(r[32 * h + 25]), "=r"(r[32 * h + 26]), "=r"(r[32 * h + 27]),
+              "=r"(r[32 * h + 28]), "=r"(r[32 * h + 29]), "=r"(r[32 * h + 30]), "=r"(r[32 * h + 31])
+            : "r"(taddr + 32 * h));
+    }
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 128; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared-memory matrix descriptor: K-major operand in 128-byte swizzle atoms
+// (8 rows x 128 B, atoms stacked along M/N every 1024 B).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// Instruction descriptor: D = F32, A/B K-major, M = 128, N = 256.
+template <int FORM>
+__device__ __forceinline__ constexpr uint32_t instr_desc() {
+    constexpr uint32_t ab = FORM == HJ_FORM_TC_TF32 ? 2u : 1u;  // TF32 : BF16
+    return (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(kTcTileB >> 3) << 17) | ((uint32_t)(kTcTileA >> 4) << 24);
+}
+
+__device__ __forceinline__ void drain(uint64_t *bar, uint32_t parity) {
+    uint64_t t0 = globaltimer_ns();
+    while (!mbar_try_wait(bar, parity)) {
+        if (globaltimer_ns() - t0 > kWaitLimitNs) break;
+    }
+}
+
+// ---------------------------------------------------------------- the kernel
+
+template <int FORM>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_join_tc(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_a2,
+              const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ CUtensorMap tm_b2, TcArgs p) {
+    // A atoms per buffer: TF32 ka; BF16 2*ka (hi atoms, then lo atoms). B atoms
+    // per tile, in ring order: TF32 q = 0..ka-1; BF16 (hi q, lo q) for each q.
+    constexpr bool kBf = FORM == HJ_FORM_TC_BF16X3;
+    const uint32_t a_atoms = kBf ? 2 * p.ka : p.ka;
+    const uint32_t b_atoms = a_atoms;
+    const uint32_t a_buf_bytes = a_atoms * kAStageBytes;
+
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar_afull[2], bar_aempty[2], bar_accfull[2], bar_accempty[2], bar_drain;
+    __shared__ __align__(8) uint64_t bar_bfull[8], bar_bempty[8];
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ __align__(16) float epi_nb[kEpiWarps][128];
+    __shared__ unsigned long long cta_count;
+
+    const uint32_t smem_base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+    const uint32_t a_base = smem_base;
+    const uint32_t b_base = smem_base + p.a_bufs * a_buf_bytes;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    volatile uint32_t *err = p.err;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&bar_afull[i], 1);
+            mbar_init(&bar_aempty[i], 1);
+            mbar_init(&bar_accfull[i], 1);
+            mbar_init(&bar_accempty[i], kEpiWarps);
+        }
+        for (uint32_t i = 0; i < p.nst; ++i) {
+            mbar_init(&bar_bfull[i], 1);
+            mbar_init(&bar_bempty[i], 1);
+        }
+        mbar_init(&bar_drain, 1);
+        cta_count = 0;
+        fence_barrier_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(&tmem_base_sh, kTmemCols);
+        if (lane == 0) {
+            prefetch_tmap(&tm_a);
+            prefetch_tmap(&tm_b);
+            if (kBf) {
+                prefetch_tmap(&tm_a2);
+                prefetch_tmap(&tm_b2);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_sh;
+
+    if (warp == 0) {
+        // ------------------------------------------------ TMA producer
+        if (lane == 0) {
+            uint32_t a_cnt = 0, b_cnt = 0;
+            for (uint64_t it = blockIdx.x; it < p.n_items; it += gridDim.x) {
+                const WorkItem w = p.items[it];
+                const uint32_t abuf = a_cnt % p.a_bufs, au = a_cnt / p.a_bufs;
+                if (au >= 1) mbar_wait(&bar_aempty[abuf], (au - 1) & 1u, err);
+                mbar_arrive_expect_tx(&bar_afull[abuf], a_buf_bytes);
+                const uint32_t adst = a_base + abuf * a_buf_bytes;
+                for (uint32_t q = 0; q < a_atoms; ++q) {
+                    const bool lo = kBf && q >= p.ka;
+                    const uint32_t kq = kBf ? (lo ? q - p.ka : q) : q;
+                    tma_load_2d(smem_raw + (adst + q * kAStageBytes - smem_u32(smem_raw)), lo ? &tm_a2 : &tm_a,
+                                (int32_t)(kq * (kBf ? 64 : 32)), (int32_t)(w.a * kTcTileA), &bar_afull[abuf]);
+                }
+                ++a_cnt;
+                for (uint32_t bt = w.b0; bt < w.b1; ++bt) {
+                    for (uint32_t q = 0; q < b_atoms; ++q) {
+                        const uint32_t s = b_cnt % p.nst, u = b_cnt / p.nst;
+                        if (u >= 1) mbar_wait(&bar_bempty[s], (u - 1) & 1u, err);
+                        mbar_arrive_expect_tx(&bar_bfull[s], kBStageBytes);
+                        const bool lo = kBf && (q & 1u);
+                        const uint32_t kq = kBf ? (q >> 1) : q;
+                        tma_load_2d(smem_raw + (b_base + s * kBStageBytes - smem_u32(smem_raw)), lo ? &tm_b2 : &tm_b,
+                                    (int32_t)(kq * (kBf ? 64 : 32)), (int32_t)(bt * kTcTileB), &bar_bfull[s]);
+                        ++b_cnt;
+                    }
+                }
+            }
+            // in the normal path every load was consumed; after an error, drain
+            if (*err) {
+                for (uint32_t s = 0; s < p.nst && s < b_cnt; ++s) {
+                    const uint32_t j = b_cnt - 1 - s;
+                    drain(&bar_bfull[j % p.nst], (j / p.nst) & 1u);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            constexpr uint32_t idesc = instr_desc<FORM>();
+            uint32_t a_cnt = 0, b_cnt = 0, t_cnt = 0;
+            bool issued_any = false;
+            for (uint64_t it = blockIdx.x; it < p.n_items; it += gridDim.x) {
+                const WorkItem w = p.items[it];
+                const uint32_t abuf = a_cnt % p.a_bufs, au = a_cnt / p.a_bufs;
+                mbar_wait(&bar_afull[abuf], au & 1u, err);
+                tc_fence_after();
+                const uint32_t abase = a_base + abuf * a_buf_bytes;
+                for (uint32_t bt = w.b0; bt < w.b1; ++bt) {
+                    const uint32_t acc = t_cnt & 1u, tu = t_cnt >> 1;
+                    if (tu >= 1) mbar_wait(&bar_accempty[acc], (tu - 1) & 1u, err);
+                    tc_fence_after();
+                    const uint32_t dcol = tmem + acc * kTcTileB;
+                    uint32_t accumulate = 0;
+                    for (uint32_t q = 0; q < b_atoms; ++q) {
+                        const uint32_t s = b_cnt % p.nst;
+                        mbar_wait(&bar_bfull[s], (b_cnt / p.nst) & 1u, err);
+                        tc_fence_after();
+                        const uint32_t bsm = b_base + s * kBStageBytes;
+                        if constexpr (!kBf) {
+                            const uint32_t asm_ = abase + q * kAStageBytes;
+#pragma unroll
+                            for (uint32_t kk = 0; kk < 4; ++kk) {
+                                mma_issue<FORM>(dcol, sw128_desc(asm_ + kk * 32), sw128_desc(bsm + kk * 32), idesc,
+                                                accumulate);
+                                accumulate = 1;
+                            }
+                        } else {
+                            const uint32_t kq = q >> 1;
+                            const uint32_t a_hi = abase + kq * kAStageBytes;
+                            const uint32_t a_lo = abase + (p.ka + kq) * kAStageBytes;
+                            if ((q & 1u) == 0) {  // B_hi atom: A_hi.B_hi + A_lo.B_hi
+#pragma unroll
+                                for (uint32_t kk = 0; kk < 4; ++kk) {
+                                    mma_issue<FORM>(dcol, sw128_desc(a_hi + kk * 32), sw128_desc(bsm + kk * 32),
+                                                    idesc, accumulate);
+                                    accumulate = 1;
+                                    mma_issue<FORM>(dcol, sw128_desc(a_lo + kk * 32), sw128_desc(bsm + kk * 32),
+                                                    idesc, 1);
+                                }
+                            } else {  // B_lo atom: A_hi.B_lo
+#pragma unroll
+                                for (uint32_t kk = 0; kk < 4; ++kk)
+                                    mma_issue<FORM>(dcol, sw128_desc(a_hi + kk * 32), sw128_desc(bsm + kk * 32),
+                                                    idesc, 1);
+                            }
+                        }
+                        mma_commit(&bar_bempty[s]);  // stage free once these MMAs have read it
+                        ++b_cnt;
+                        issued_any = true;
+                    }
+                    mma_commit(&bar_accfull[acc]);
+                    ++t_cnt;
+                }
+                mma_commit(&bar_aempty[abuf]);
+                ++a_cnt;
+            }
+            // all MMAs complete before the tensor memory is released
+            if (issued_any) {
+                mma_commit(&bar_drain);
+                drain(&bar_drain, 0);
+            }
+        }
+    } else {
+        // ------------------------------------------------ epilogue
+        const uint32_t quad = warp & 3u;
+        const uint32_t half = (warp - 2) >> 2;  // columns [128 half, 128 half + 128)
+        const uint32_t lane_base = (quad * 32u) << 16;
+        float *snb = epi_nb[warp - 2];
+        unsigned long long cnt = 0;
+        uint32_t t_cnt = 0;
+        const double T = p.T;
+        // All classification is in FP32 with eps^2 rounded outward (T_lo, T_hi)
+        // and the bound rounded up; the FP32 rounding of the epilogue itself is
+        // part of c_rel. A pair is inside if s + tau <= T_lo, outside if
+        // s - tau > T_hi, and in the band otherwise.
+        const float T_lo = p.T_lo, T_hi = p.T_hi, crel = p.c_rel_f, cabs = p.c_abs_f;
+        for (uint64_t it = blockIdx.x; it < p.n_items; it += gridDim.x) {
+            const WorkItem w = p.items[it];
+            const uint64_t gi = (uint64_t)w.a * kTcTileA + quad * 32 + lane;
+            const bool row_ok = gi < p.na;
+            const float na = row_ok ? p.norm_a[gi] : kPadNorm;
+            for (uint32_t bt = w.b0; bt < w.b1; ++bt) {
+                const uint32_t acc = t_cnt & 1u;
+                const uint64_t gj0 = (uint64_t)bt * kTcTileB + half * 128;
+                // issued before the wait: the norms of this warp's 128 columns
+                const float4 nbv = __ldg(reinterpret_cast<const float4 *>(p.norm_b + gj0) + lane);
+                const float tmaxb = __ldg(p.tmax_b + bt);
+                const float4 gmin = __ldg(reinterpret_cast<const float4 *>(p.gmin_b + gj0 / 32));
+                // With tau_max = c_rel (|a|^2 + max_tile |b|^2) + c_abs >= tau of every
+                // pair in the tile, and t_j = |b_j|^2 - 2 v_j, s_j = |a|^2 + t_j:
+                //   t_j <= thr_in  => s_j + tau <= eps^2  (certainly inside),
+                //   t_j >  thr_out => s_j - tau >  eps^2  (certainly outside),
+                // anything between is a band pair. Both thresholds carry margins
+                // for their own FP32 rounding (rounded inward / outward).
+                const float tau_max = fmaf(crel, na + tmaxb, cabs) * 1.001f;
+                const float marg = 8.0f * 5.9604645e-8f * (fabsf(T_hi) + fabsf(na) + tmaxb + tau_max);
+                float thr_out = (T_hi + tau_max) - na + marg;
+                float thr_in = (T_lo - tau_max) - na - marg;
+                if (!row_ok) thr_out = thr_in = -3.0e38f;
+                // columns that may be counted at all: gj < nb, and gj > gi for a self-join
+                int jlo = 0, jhi = 128;
+                {
+                    const int64_t lim = (int64_t)p.nb - (int64_t)gj0;
+                    jhi = lim < 128 ? (lim < 0 ? 0 : (int)lim) : 128;
+                    if (p.self) {
+                        const int64_t first = (int64_t)gi + 1 - (int64_t)gj0;
+                        jlo = first > 0 ? (first > 128 ? 128 : (int)first) : 0;
+                    }
+                }
+                mbar_wait(&bar_accfull[acc], (t_cnt >> 1) & 1u, err);
+                tc_fence_after();
+                reinterpret_cast<float4 *>(snb)[lane] = nbv;
+                __syncwarp();
+#pragma unroll 1
+                for (uint32_t c = 0; c < 2; ++c) {
+                    float v[64];
+                    tmem_ld64(tmem + lane_base + acc * kTcTileB + half * 128 + c * 64, v);
+                    // max_j v_j per 32-column group: with the group's minimum norm,
+                    // min_j (|b_j|^2 - 2 v_j) >= gmin - 2 max_j v_j
+                    float mx[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) mx[q] = -3.0e38f;
+#pragma unroll
+                    for (int j = 0; j < 64; ++j) mx[(j & 3) + (j >= 32 ? 4 : 0)] = fmaxf(mx[(j & 3) + (j >= 32 ? 4 : 0)], v[j]);
+                    const float g0 = c ? gmin.z : gmin.x, g1 = c ? gmin.w : gmin.y;
+                    const float mlo = fmaf(-2.0f, fmaxf(fmaxf(mx[0], mx[1]), fmaxf(mx[2], mx[3])), g0);
+                    const float mhi = fmaf(-2.0f, fmaxf(fmaxf(mx[4], mx[5]), fmaxf(mx[6], mx[7])), g1);
+#pragma unroll
+                    for (int h2 = 0; h2 < 2; ++h2) {
+                        // Rare: a 32-column half of some row of the warp may hold a pair
+                        // that is not certainly outside. Branch-free count of the certain
+                        // ones; band pairs are queued.
+                        const bool need = (h2 ? mhi : mlo) <= thr_out || (p.dbg != nullptr && row_ok);
+                        if (!__any_sync(0xffffffffu, need)) continue;
+                        const int cb = (int)(c * 64 + h2 * 32);
+                        uint32_t band_bits = 0;
+                        unsigned int in_cnt = 0;
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const float t = fmaf(-2.0f, v[h2 * 32 + j], snb[cb + j]);
+                            const bool ok = (unsigned)(cb + j - jlo) < (unsigned)(jhi - jlo);
+                            in_cnt += (ok && t <= thr_in) ? 1u : 0u;
+                            band_bits |= (ok && t > thr_in && t <= thr_out) ? (1u << j) : 0u;
+                            if (p.dbg != nullptr && row_ok && gj0 + cb + j < p.nb)
+                                p.dbg[(uint64_t)p.perm_a[gi] * p.nb + p.perm_b[gj0 + cb + j]] = na + t;
+                        }
+                        cnt += in_cnt;
+                        while (band_bits) {  // very rare
+                            const int j = __ffs(band_bits) - 1;
+                            band_bits &= band_bits - 1;
+                            float vj = v[h2 * 32];
+#pragma unroll
+                            for (int k = 1; k < 32; ++k) vj = (k == j) ? v[h2 * 32 + k] : vj;
+                            const float sh = na + fmaf(-2.0f, vj, snb[cb + j]);
+                            const unsigned long long k = atomicAdd(p.band_total, 1ull);
+                            if (k < p.band_cap) {
+                                BandEntry e;
+                                e.ia = (uint32_t)gi;
+                                e.jb = (uint32_t)(gj0 + cb + j);
+                                e.s_hat = sh;
+                                e.pad = 0;
+                                p.band[k] = e;
+                            }
+                        }
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bar_accempty[acc]);
+                ++t_cnt;
+            }
+        }
+        cnt = warp_sum_u64(cnt);
+        if (lane == 0 && cnt) atomicAdd(&cta_count, cnt);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) tmem_dealloc(tmem, kTmemCols);
+    if (threadIdx.x == 0 && cta_count) atomicAdd(p.count, cta_count);
+}
+
+// ---------------------------------------------------------------- recheck
+
+// FP64 pair test (the oracle's) on every band pair; also the largest
+// |s_hat - dist2| seen, as FP32 bits in max_err_bits.
+template <typename TIn>
+__global__ void k_recheck(const TIn *__restrict__ ra, const TIn *__restrict__ rb, uint32_t d, double T,
+                          const BandEntry *__restrict__ band, const unsigned long long *band_total, uint64_t cap,
+                          unsigned long long *count, unsigned int *max_err_bits) {
+    const uint64_t n = min((unsigned long long)cap, *band_total);
+    unsigned long long c = 0;
+    float emax = 0.f;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const BandEntry e = band[i];
+        const TIn *a = ra + (uint64_t)e.ia * d;
+        const TIn *b = rb + (uint64_t)e.jb * d;
+        double acc = 0.0;
+        for (uint32_t k = 0; k < d; ++k) {
+            const double df = __dsub_rn((double)a[k], (double)b[k]);
+            acc = __fma_rn(df, df, acc);
+        }
+        c += acc <= T ? 1ull : 0ull;
+        emax = fmaxf(emax, (float)fabs((double)e.s_hat - acc));
+    }
+    c = warp_sum_u64(c);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) emax = fmaxf(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+    if ((threadIdx.x & 31u) == 0) {
+        if (c) atomicAdd(count, c);
+        atomicMax(max_err_bits, __float_as_uint(emax));
+    }
+}
+
+// ---------------------------------------------------------------- host side
+
+// Error bound of the tensor-core estimate s = |a|^2 + |b|^2 - 2 v against the
+// FP64 pair test, |s - dist2| <= c_rel (|a|^2 + |b|^2) + c_abs, built from:
+//   operand rounding (TF32: 2 * 2^-11 relative per product; BF16 split:
+//   a = a_hi + a_lo + r with |r| <= 2^-16 |a|, dropped a_lo b_lo and r terms
+//   <= 3.1 * 2^-16 |a_k b_k|), FP32 rounding of FP64 inputs (2 * 2^-24),
+//   tensor-core FP32 accumulation budgeted at 2^-22 of the running sum per
+//   product term (K terms TF32, 3K BF16), |a.b| <= sum |a_k b_k| <=
+//   (|a|^2 + |b|^2) / 2 (Cauchy-Schwarz, AM-GM) -- the dot error enters s
+//   twice; FP32 norms (2^-24 each) and the FP32 epilogue (three roundings of
+//   values up to 2 (|a|^2 + |b|^2), 6 * 2^-24, budgeted 10 * 2^-24); the FP64
+//   direct difference's own rounding (d * 2^-50).
+// A margin factor 1.25 covers the bookkeeping in between. c_abs covers
+// subnormal operands (TF32/BF16 keep the FP32 exponent range; values below
+// 2^-100 times the largest coordinate are the only ones that can lose
+// relative accuracy) and is negligible for data of ordinary scale.
 void tc_band_constants(int form, uint32_t d, double maxabs, double *c_rel, double *c_abs) {
-    (void)form; (void)d; (void)maxabs;
-    *c_rel = 0;
-    *c_abs = 0;
+    const double u24 = std::ldexp(1.0, -24), acc = std::ldexp(1.0, -22);
+    const double kpad = form == HJ_FORM_TC_TF32 ? (double)((d + 31) / 32 * 32) : (double)((d + 63) / 64 * 64);
+    double dot;
+    if (form == HJ_FORM_TC_TF32) {
+        const double u = std::ldexp(1.0, -11);
+        dot = 2 * u + u * u + 2 * u24 + kpad * acc;
+    } else {
+        dot = 3.1 * std::ldexp(1.0, -16) + 2 * u24 + 3 * kpad * acc;
+    }
+    *c_rel = 1.25 * (dot + 12 * u24 + (double)d * std::ldexp(1.0, -50));
+    *c_abs = 1e-30 + 4.0 * (double)d * std::ldexp(std::fmax(maxabs, 1e-30), -100) * std::fmax(maxabs, 1.0);
 }
 
-int launch_join_tc(const SortedSet &, const SortedSet &, bool, uint64_t, uint64_t, const TcParams &,
-                   const IndexResult &, unsigned long long *, uint2 *, uint64_t, unsigned long long *, uint32_t *,
-                   int, cudaStream_t, std::string *err) {
-    *err = "tensor-core form not built";
-    return 1;
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn(std::string *err) {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+        else
+            cudaGetLastError();
+    });
+    if (!fn) *err = "cuTensorMapEncodeTiled unavailable";
+    return fn;
 }
 
-void launch_recheck(const SortedSet &, const SortedSet &, double, const uint2 *, const unsigned long long *,
-                    uint64_t, unsigned long long *, cudaStream_t) {}
+// 2D map over a row-major [rows][kp] matrix, box = one 128-byte K atom x box_rows.
+static bool make_map(CUtensorMap *m, const void *base, bool bf16, uint64_t rows, uint32_t kp, uint32_t box_rows,
+                     std::string *err) {
+    EncodeTiledFn fn = encode_fn(err);
+    if (!fn) return false;
+    const uint32_t esz = bf16 ? 2 : 4;
+    cuuint64_t gdim[2] = {kp, rows};
+    cuuint64_t gstride[1] = {(cuuint64_t)kp * esz};
+    cuuint32_t box[2] = {kAtomBytes / esz, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(m, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                    const_cast<void *>(base), gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        *err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
+        return false;
+    }
+    return true;
+}
+
+struct TcLayout {
+    uint32_t ka, a_bufs, nst;
+    size_t smem;
+};
+
+static TcLayout tc_layout(int form, uint32_t d) {
+    TcLayout L;
+    L.ka = form == HJ_FORM_TC_TF32 ? (d + 31) / 32 : (d + 63) / 64;
+    const uint32_t a_atoms = form == HJ_FORM_TC_TF32 ? L.ka : 2 * L.ka;
+    const size_t a_bytes = (size_t)a_atoms * kAStageBytes;
+    const size_t budget = 220 * 1024;
+    L.a_bufs = 2 * a_bytes + 3 * kBStageBytes <= budget ? 2 : 1;
+    size_t left = budget - L.a_bufs * a_bytes;
+    L.nst = (uint32_t)(left / kBStageBytes);
+    if (L.nst > 8) L.nst = 8;
+    L.smem = L.a_bufs * a_bytes + (size_t)L.nst * kBStageBytes + 1024;
+    return L;
+}
+
+static float *g_dbg_out = nullptr;  // set by tests through hj_debug_tc_estimates
+
+int launch_join_tc(const SortedSet &A, const SortedSet &B, bool self, uint64_t na_eff, uint64_t nb_eff,
+                   const TcParams &tp, const IndexResult &idx, unsigned long long *d_count, uint2 *band,
+                   uint64_t band_cap, unsigned long long *d_band_total, uint32_t *d_err, int num_sms, cudaStream_t st,
+                   std::string *err) {
+    if (idx.n_items == 0) return 0;
+    const bool bf = tp.form == HJ_FORM_TC_BF16X3;
+    const TcLayout L = tc_layout(tp.form, A.d);
+    if (L.nst < 2) {
+        *err = "dimension too large for the tensor-core kernel";
+        return 1;
+    }
+    CUtensorMap ma, ma2, mb, mb2;
+    if (!bf) {
+        if (!make_map(&ma, A.tf32, false, A.npad_tc, A.kpad_tf32, kTcTileA, err)) return 1;
+        if (!make_map(&mb, B.tf32, false, B.npad_tc, B.kpad_tf32, kTcTileB, err)) return 1;
+        ma2 = ma;
+        mb2 = mb;
+    } else {
+        if (!make_map(&ma, A.bf_hi, true, A.npad_tc, A.kpad_bf16, kTcTileA, err)) return 1;
+        if (!make_map(&ma2, A.bf_lo, true, A.npad_tc, A.kpad_bf16, kTcTileA, err)) return 1;
+        if (!make_map(&mb, B.bf_hi, true, B.npad_tc, B.kpad_bf16, kTcTileB, err)) return 1;
+        if (!make_map(&mb2, B.bf_lo, true, B.npad_tc, B.kpad_bf16, kTcTileB, err)) return 1;
+    }
+    TcArgs a;
+    a.ka = L.ka;
+    a.a_bufs = L.a_bufs;
+    a.nst = L.nst;
+    a.items = idx.items;
+    a.n_items = idx.n_items;
+    a.norm_a = A.norms;
+    a.norm_b = B.norms;
+    a.tmax_b = B.tile_maxnorm_b;
+    a.gmin_b = B.group_minnorm;
+    a.na = na_eff;
+    a.nb = nb_eff;
+    a.self = self ? 1 : 0;
+    a.T = tp.T;
+    a.c_rel = tp.c_rel;
+    a.c_abs = tp.c_abs;
+    {
+        float t = (float)tp.T;  // outward rounding of eps^2 and upward rounding of the bound
+        a.T_lo = (double)t <= tp.T ? t : std::nextafter(t, -INFINITY);
+        a.T_hi = (double)t >= tp.T ? t : std::nextafter(t, INFINITY);
+        float cr = (float)tp.c_rel, ca = (float)tp.c_abs;
+        a.c_rel_f = (double)cr >= tp.c_rel ? cr : std::nextafter(cr, INFINITY);
+        a.c_abs_f = (double)ca >= tp.c_abs ? ca : std::nextafter(ca, INFINITY);
+    }
+    a.count = d_count;
+    a.band = reinterpret_cast<BandEntry *>(band);
+    a.band_cap = band_cap;
+    a.band_total = d_band_total;
+    a.err = d_err;
+    a.dbg = g_dbg_out;
+    a.perm_a = A.perm;
+    a.perm_b = B.perm;
+    uint64_t grid = (uint64_t)num_sms;
+    if (grid > idx.n_items) grid = idx.n_items;
+    if (!bf) {
+        cudaFuncSetAttribute(k_join_tc<HJ_FORM_TC_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
+        k_join_tc<HJ_FORM_TC_TF32><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
+    } else {
+        cudaFuncSetAttribute(k_join_tc<HJ_FORM_TC_BF16X3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
+        k_join_tc<HJ_FORM_TC_BF16X3><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        *err = std::string("tensor-core kernel launch: ") + cudaGetErrorString(e);
+        return 1;
+    }
+    return 0;
+}
+
+void launch_recheck(const SortedSet &A, const SortedSet &B, double T, const uint2 *band,
+                    const unsigned long long *d_band_total, uint64_t band_cap, unsigned long long *d_count,
+                    unsigned int *d_max_err_bits, cudaStream_t st) {
+    const BandEntry *b = reinterpret_cast<const BandEntry *>(band);
+    if (A.dtype_bytes == 8)
+        k_recheck<double><<<1184, 256, 0, st>>>(static_cast<const double *>(A.rows),
+                                                static_cast<const double *>(B.rows), A.d, T, b, d_band_total, band_cap,
+                                                d_count, d_max_err_bits);
+    else
+        k_recheck<float><<<1184, 256, 0, st>>>(static_cast<const float *>(A.rows), static_cast<const float *>(B.rows),
+                                               A.d, T, b, d_band_total, band_cap, d_count, d_max_err_bits);
+}
+
+void set_tc_debug_output(float *dbg) { g_dbg_out = dbg; }
 
 }  // namespace hj

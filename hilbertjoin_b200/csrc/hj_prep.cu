@@ -31,6 +31,8 @@ __global__ void k_dim_stats_init(DimStats *s, uint32_t d, unsigned long long *ma
     for (uint32_t t = threadIdx.x + blockIdx.x * blockDim.x; t < d; t += blockDim.x * gridDim.x) {
         s[t].cmin = LLONG_MAX;
         s[t].cmax = LLONG_MIN;
+        s[t].xmin = ~0ull;
+        s[t].xmax = 0ull;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *maxabs = 0ull;
@@ -43,11 +45,14 @@ constexpr double kCellLimit = 4.611686018427388e18;
 
 __global__ void k_dim_stats(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, DimStats *s,
                             unsigned long long *maxabs_bits, uint32_t *bad) {
-    extern __shared__ long long sh[];  // [2][d]
+    extern __shared__ long long sh[];  // [4][d]
     long long *smin = sh, *smax = sh + d;
+    unsigned long long *sxmin = reinterpret_cast<unsigned long long *>(sh + 2 * d), *sxmax = sxmin + d;
     for (uint32_t t = threadIdx.x; t < d; t += blockDim.x) {
         smin[t] = LLONG_MAX;
         smax[t] = LLONG_MIN;
+        sxmin[t] = ~0ull;
+        sxmax[t] = 0ull;
     }
     __syncthreads();
     const uint64_t total = n * d;
@@ -70,12 +75,17 @@ __global__ void k_dim_stats(const void *x, int dtype_bytes, uint64_t n, uint32_t
         long long ci = (long long)c;
         atomicMin(&smin[t], ci);
         atomicMax(&smax[t], ci);
+        const unsigned long long ov = ordered_from_double(v);
+        atomicMin(&sxmin[t], ov);
+        atomicMax(&sxmax[t], ov);
     }
     __syncthreads();
     for (uint32_t t = threadIdx.x; t < d; t += blockDim.x) {
         if (smin[t] != LLONG_MAX) {
             atomicMin(&s[t].cmin, smin[t]);
             atomicMax(&s[t].cmax, smax[t]);
+            atomicMin(&s[t].xmin, sxmin[t]);
+            atomicMax(&s[t].xmax, sxmax[t]);
         }
     }
     // non-negative doubles order like their bit patterns
@@ -93,7 +103,7 @@ void launch_dim_stats(const void *x, int dtype_bytes, uint64_t n, uint32_t d, do
     uint64_t total = n * d;
     int blocks = (int)std::min<uint64_t>(hj_ceil_div(total, 256 * 8), 148 * 8);
     if (blocks < 1) blocks = 1;
-    k_dim_stats<<<blocks, 256, 2 * d * sizeof(long long), st>>>(x, dtype_bytes, n, d, eps, dstats, d_maxabs_bits,
+    k_dim_stats<<<blocks, 256, 4 * d * sizeof(long long), st>>>(x, dtype_bytes, n, d, eps, dstats, d_maxabs_bits,
                                                                  d_bad);
 }
 
@@ -119,6 +129,25 @@ __global__ void k_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t
     }
     keys_wm[(uint64_t)cur_word * n + i] = acc;
     for (uint32_t z = cur_word + 1; z < W; ++z) keys_wm[(uint64_t)z * n + i] = 0u;
+}
+
+__global__ void k_norm_key(const void *x, int dtype_bytes, uint64_t n, uint32_t d,
+                           const double *__restrict__ center, double scale, uint32_t *key_out) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+    for (uint32_t k = 0; k < d; ++k) {
+        double v = coord(x, dtype_bytes, i * d + k) - center[k];
+        s = fma(v, v, s);
+    }
+    double q = floor(s * scale);
+    key_out[i] = q < 65535.0 ? (uint32_t)q : 65535u;
+}
+
+void launch_norm_key(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const double *center, double scale,
+                     uint32_t *key_out, cudaStream_t st) {
+    if (n == 0) return;
+    k_norm_key<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(x, dtype_bytes, n, d, center, scale, key_out);
 }
 
 void launch_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, const GridDev &g,
@@ -305,16 +334,18 @@ __device__ __forceinline__ float to_tf32_rn(float v) {
 }
 
 // Tensor-core layouts, one thread per (row, k) element of the padded matrix:
-// TF32 rows [npad][kp32], BF16 hi/lo rows [npad][kp16].
+// TF32 rows [npad][kp32], BF16 hi/lo rows [npad][kp16]. The operands are the
+// coordinates minus `center` (per dim): distances are shift invariant, and the
+// smaller norms narrow the error band of the norm expansion.
 __global__ void k_gather_tc(const void *x, int dtype_bytes, uint64_t n, uint32_t d,
-                            const uint32_t *__restrict__ perm, uint64_t npad, uint32_t kp, float *tf32,
-                            uint16_t *bf_hi, uint16_t *bf_lo) {
+                            const uint32_t *__restrict__ perm, const double *__restrict__ center, uint64_t npad,
+                            uint32_t kp, float *tf32, uint16_t *bf_hi, uint16_t *bf_lo) {
     uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= npad * kp) return;
     uint64_t r = e / kp;
     uint32_t k = (uint32_t)(e % kp);
     float v = 0.0f;
-    if (r < n && k < d) v = (float)coord(x, dtype_bytes, (uint64_t)perm[r] * d + k);
+    if (r < n && k < d) v = (float)(coord(x, dtype_bytes, (uint64_t)perm[r] * d + k) - center[k]);
     if (tf32) tf32[e] = to_tf32_rn(v);
     if (bf_hi) {
         __nv_bfloat16 h = __float2bfloat16_rn(v);
@@ -325,10 +356,10 @@ __global__ void k_gather_tc(const void *x, int dtype_bytes, uint64_t n, uint32_t
     }
 }
 
-// |x|^2 per sorted row in FP64 (input precision widened exactly), stored as
-// FP32; padding rows get kPadNorm so that they never pass a threshold.
+// |x - center|^2 per sorted row in FP64 (input precision widened exactly),
+// stored as FP32; padding rows get kPadNorm so that they never pass a threshold.
 __global__ void k_norms(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const uint32_t *__restrict__ perm,
-                        uint64_t npad, float *norms) {
+                        const double *__restrict__ center, uint64_t npad, float *norms) {
     uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= npad) return;
     if (r >= n) {
@@ -338,17 +369,30 @@ __global__ void k_norms(const void *x, int dtype_bytes, uint64_t n, uint32_t d, 
     uint64_t src = perm[r];
     double s = 0.0;
     for (uint32_t k = 0; k < d; ++k) {
-        double v = coord(x, dtype_bytes, src * d + k);
+        double v = coord(x, dtype_bytes, src * d + k) - center[k];
         s = fma(v, v, s);
     }
     norms[r] = (float)s;
 }
 
+// Per-tile maximum norm over real rows (padding rows excluded).
 __global__ void k_tile_max(const float *__restrict__ v, uint64_t npad, int tile, float *out) {
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t * tile >= npad) return;
-    float m = -3.4e38f;
-    for (int i = 0; i < tile; ++i) m = fmaxf(m, v[t * tile + i]);
+    float m = 0.0f;
+    for (int i = 0; i < tile; ++i) {
+        float x = v[t * tile + i];
+        if (x < 1e29f) m = fmaxf(m, x);
+    }
+    out[t] = m;
+}
+
+// Per-group minimum norm (padding rows hold kPadNorm and never lower it).
+__global__ void k_group_min(const float *__restrict__ v, uint64_t npad, int group, float *out) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t * group >= npad) return;
+    float m = 3.0e38f;
+    for (int i = 0; i < group; ++i) m = fminf(m, v[t * group + i]);
     out[t] = m;
 }
 
@@ -371,24 +415,28 @@ void launch_gather(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const
     }
     if (flags & kGatherTf32) {
         uint64_t total = o.npad_tc * o.kpad_tf32;
-        k_gather_tc<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.npad_tc,
-                                                                      o.kpad_tf32, o.tf32, nullptr, nullptr);
+        k_gather_tc<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.center,
+                                                                      o.npad_tc, o.kpad_tf32, o.tf32, nullptr,
+                                                                      nullptr);
         ++L;
     }
     if (flags & kGatherBf16) {
         uint64_t total = o.npad_tc * o.kpad_bf16;
-        k_gather_tc<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.npad_tc,
-                                                                      o.kpad_bf16, nullptr, o.bf_hi, o.bf_lo);
+        k_gather_tc<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.center,
+                                                                      o.npad_tc, o.kpad_bf16, nullptr, o.bf_hi,
+                                                                      o.bf_lo);
         ++L;
     }
     if (flags & kGatherNorms) {
-        k_norms<<<(unsigned)hj_ceil_div(o.npad_tc, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.npad_tc,
-                                                                      o.norms);
+        k_norms<<<(unsigned)hj_ceil_div(o.npad_tc, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.center,
+                                                                      o.npad_tc, o.norms);
         k_tile_max<<<(unsigned)hj_ceil_div(o.npad_tc / kTcTileA, 256), 256, 0, st>>>(o.norms, o.npad_tc, kTcTileA,
                                                                                     o.tile_maxnorm_a);
         k_tile_max<<<(unsigned)hj_ceil_div(o.npad_tc / kTcTileB, 256), 256, 0, st>>>(o.norms, o.npad_tc, kTcTileB,
                                                                                     o.tile_maxnorm_b);
-        L += 3;
+        k_group_min<<<(unsigned)hj_ceil_div(o.npad_tc / 32, 256), 256, 0, st>>>(o.norms, o.npad_tc, 32,
+                                                                              o.group_minnorm);
+        L += 4;
     }
     if (launches) *launches += L;
 }

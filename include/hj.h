@@ -91,6 +91,7 @@ typedef struct {
     double sort_ms;         /* cell keys + stable LSD radix sort + gather (the reference's SORTTIME) */
     double index_ms;        /* stripe bounds + block-pair work list (the reference's INDEXTIME) */
     double join_ms;         /* distance kernel(s) */
+    double kernel_ms;       /* the main distance kernel alone (CUDA events around its launch) */
     double recheck_ms;      /* FP64 re-evaluation of band pairs (tensor-core forms) */
     double total_ms;        /* whole call, host wall clock */
     double loadpercent;     /* candidate pairs / all pairs * 100 (the reference's LOADPERCENT
@@ -101,6 +102,9 @@ typedef struct {
     uint64_t band_pairs;    /* pairs sent to the FP64 recheck */
     double band_fraction;   /* band_pairs / candidate_pairs */
     double band_halfwidth_rel; /* tensor-core bound: |dist2 - est| <= c * (|a|^2 + |b|^2) + abs; this is c */
+    double max_abs_err_band;   /* largest |est - dist2| over the band pairs (tensor-core forms) */
+    uint64_t fp64_items;    /* tensor-core forms: work items routed to the FP64 kernel because
+                               their error band would exceed eps^2 / 2 */
     int32_t form_used;      /* hj_form actually run */
     int32_t stripes;        /* stripe count (3^s+1)/2 for self-joins, 3^s for two-set joins */
     int32_t kernel_launches;/* kernels this call launched */
@@ -161,6 +165,13 @@ HJ_API void hj_test_ego_loop3_macro(size_t n, size_t d, double epsilon, double *
 HJ_API void hj_test_ego_loop3_noself(const size_t nA, const size_t nB, const int d, const double epsilon, double *arrayA,
                               double *arrayB, size_t *countresult, const int activedims, double *sortTime,
                               double *indextime, double *loadpercent);
+
+/* Testing hook: the tensor-core form's dist^2 estimate of every pair (a in
+ * A, b in B), written to out[i * nB + j] in input order (nA * nB floats).
+ * Runs a two-set join with eps so large that all points share one cell.
+ * Not thread-safe; no reference counterpart. */
+HJ_API int hj_debug_tc_estimates(const float *A, uint64_t nA, const float *B, uint64_t nB, uint32_t d, int form,
+                                 float *out);
 
 /* ---------------------------------------------------------------- serving
  * A request loop with device-resident point sets: sets are uploaded once and

@@ -15,7 +15,7 @@ from tests.golden.make_golden import make
 pytestmark = pytest.mark.gpu
 
 GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "golden_counts.json")))["cases"]
-FORMS = ["plain"]
+FORMS = ["plain", "tf32", "bf16x3"]
 
 
 @pytest.fixture(scope="module")
@@ -94,12 +94,14 @@ def test_eps_extremes(hj, form):
     assert hj.join_count(x, x[:300], 100.0, form=form) == n * 300
 
 
-def test_lattice_ties_plain(hj):
-    """Exact ties at eps follow the direct-difference FP64 test (inclusive)."""
+@pytest.mark.parametrize("form", FORMS)
+def test_lattice_ties(hj, form):
+    """Exact ties at eps follow the direct-difference FP64 test (inclusive); for
+    the tensor-core forms every tie lands in the band and is re-evaluated."""
     from hilbertjoin_b200 import workloads as W
     for levels, step in ((3, 0.1), (5, 0.25), (4, 0.3)):
         x = W.lattice(3000, 6, levels, step=step, levels=levels)
-        assert hj.self_join_count(x, step) == oracle.self_count_brute(x, step)
+        assert hj.self_join_count(x, step, form=form) == oracle.self_count_brute(x, step)
 
 
 @pytest.mark.parametrize("active_dims", [0, 1, 2, 3, 4, 5])
@@ -112,13 +114,27 @@ def test_active_dims_change_work_only(hj, active_dims):
     assert st["candidate_pairs"] >= c
 
 
-def test_fp32_input(hj):
+@pytest.mark.parametrize("form", FORMS)
+def test_fp32_input(hj, form):
     rng = np.random.default_rng(3)
     x = rng.random((3000, 16)).astype(np.float32)
     eps = 0.6
-    assert hj.self_join_count(x, eps) == oracle.self_count_brute(x.astype(np.float64), eps)
+    assert hj.self_join_count(x, eps, form=form) == oracle.self_count_brute(x.astype(np.float64), eps)
     b = rng.random((2000, 16)).astype(np.float32)
-    assert hj.join_count(x, b, eps) == oracle.join_count_brute(x.astype(np.float64), b.astype(np.float64), eps)
+    assert hj.join_count(x, b, eps, form=form) == \
+        oracle.join_count_brute(x.astype(np.float64), b.astype(np.float64), eps)
+
+
+@pytest.mark.parametrize("form", ["tf32", "bf16x3"])
+def test_tc_signed_and_scaled_data(hj, form):
+    """Mixed-sign coordinates and large magnitudes exercise the band bound."""
+    rng = np.random.default_rng(8)
+    x = (rng.random((3000, 24)) * 2.0 - 1.0) * 1000.0
+    eps = 1500.0
+    assert hj.self_join_count(x, eps, form=form) == oracle.self_count_brute(x, eps)
+    y = rng.random((2000, 24)) * 1e-3 + 5.0
+    eps = 1.1e-3
+    assert hj.self_join_count(y, eps, form=form) == oracle.self_count_brute(y, eps)
 
 
 def test_torch_device_input(hj):

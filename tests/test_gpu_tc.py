@@ -1,0 +1,88 @@
+"""Tensor-core forms: the dist^2 estimate of every pair stays inside the error
+bound that decides which pairs are re-evaluated in FP64 (the exactness of the
+count rests on it), and the band logic returns the FP64 count."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def hj():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import hilbertjoin_b200
+    return hilbertjoin_b200
+
+
+def exact_dist2(a, b):
+    a = a.astype(np.float64)
+    b = b.astype(np.float64)
+    out = np.empty((a.shape[0], b.shape[0]))
+    for i0 in range(0, a.shape[0], 128):
+        out[i0:i0 + 128] = ((a[i0:i0 + 128, None, :] - b[None, :, :]) ** 2).sum(-1)
+    return out
+
+
+def bound_constants(hj, form, a, b):
+    _, st = hj.join_count(a, b, 1e-6, form=form, return_stats=True)
+    return st["band_halfwidth_rel"]
+
+
+@pytest.mark.parametrize("form", ["tf32", "bf16x3"])
+@pytest.mark.parametrize("d,kind", [(4, "u"), (20, "u"), (32, "u"), (64, "u"), (100, "u"), (128, "u"),
+                                    (64, "signed"), (28, "gmm")])
+def test_estimates_within_bound(hj, form, d, kind):
+    rng = np.random.default_rng(d * 7 + len(kind))
+    if kind == "u":
+        a, b = rng.random((700, d)), rng.random((900, d))
+    elif kind == "signed":
+        a, b = rng.standard_normal((700, d)) * 3.0, rng.standard_normal((900, d)) * 3.0
+    else:
+        from hilbertjoin_b200 import workloads as W
+        a, b = W.gmm(700, d, 1), W.gmm(900, d, 2)
+    a = a.astype(np.float32)
+    b = b.astype(np.float32)
+    est = hj.tc_estimates(a, b, form).astype(np.float64)
+    ex = exact_dist2(a, b)
+    # the engine shifts the tensor-core operands by the midpoint of the
+    # coordinate range of both sets; its bound is in the shifted norms
+    both = np.concatenate([a, b]).astype(np.float64)
+    center = 0.5 * both.min(0) + 0.5 * both.max(0)
+    na = ((a.astype(np.float64) - center) ** 2).sum(1)
+    nb = ((b.astype(np.float64) - center) ** 2).sum(1)
+    c_rel = bound_constants(hj, form, a, b)
+    bound = c_rel * (na[:, None] + nb[None, :])
+    ratio = np.abs(est - ex) / bound
+    assert np.isfinite(est).all()
+    assert ratio.max() < 1.0, (form, d, kind, float(ratio.max()))
+    # the estimate is a real tensor-core result, not a copy of the FP64 value
+    assert np.abs(est - ex).max() > 0
+
+
+@pytest.mark.parametrize("form", ["tf32", "bf16x3"])
+def test_band_pairs_are_rechecked(hj, form):
+    """eps set at the median distance puts many pairs in the band; the count is
+    still the FP64 count and the reported max error respects the bound."""
+    rng = np.random.default_rng(21)
+    x = rng.random((4000, 32)).astype(np.float32)
+    d2 = exact_dist2(x[:500], x[500:1500])
+    eps = float(np.sqrt(np.median(d2)))
+    c, st = hj.self_join_count(x, eps, form=form, return_stats=True)
+    assert c == oracle.self_count_brute(x.astype(np.float64), eps)
+    assert st["band_pairs"] > 0
+    assert st["max_abs_err_band"] <= st["band_halfwidth_rel"] * 2 * 32 * 1.0
+
+
+def test_forms_agree_dense(hj):
+    """The dense single-cell regime of the headline configuration, at a size the
+    oracle still covers: all forms give the FP64 count."""
+    from hilbertjoin_b200 import workloads as W
+    x = W.uniform(20000, 64, 22, dtype=np.float32)
+    eps = W.calibrate_eps(x, 20000, 32)
+    want = oracle.self_count_brute(x.astype(np.float64), eps)
+    for form in ("plain", "tf32", "bf16x3"):
+        assert hj.self_join_count(x, eps, form=form) == want, form
