@@ -140,6 +140,10 @@ void launch_norm_key(const void *x, int dtype_bytes, uint64_t n, uint32_t d, con
 void radix_sort_perm(const uint32_t *keys_wm, uint64_t n, const std::vector<std::pair<uint32_t, uint32_t>> &passes,
                      uint32_t *perm_out, uint32_t *perm_tmp, uint32_t *hist, cudaStream_t st, int *launches);
 size_t radix_hist_entries(uint64_t n);
+// One stable pass of the above (perm_in null = identity), and an iota.
+void radix_sort_pass(const uint32_t *keyw, uint64_t n, uint32_t shift, const uint32_t *perm_in,
+                     uint32_t *perm_out, uint32_t *hist, cudaStream_t st);
+void launch_iota(uint32_t *p, uint64_t n, cudaStream_t st);
 // Exclusive scan of u32 entries in place (one block); total into *total if non-null.
 void launch_scan_u32(uint32_t *a, uint64_t count, unsigned long long *total, cudaStream_t st);
 

@@ -286,6 +286,20 @@ void radix_sort_perm(const uint32_t *keys_wm, uint64_t n, const std::vector<std:
     }
 }
 
+// One radix pass (histogram, scan, stable scatter) and a plain iota, for
+// callers that drive the passes themselves (hj_noalloc.cu).
+void radix_sort_pass(const uint32_t *keyw, uint64_t n, uint32_t shift, const uint32_t *perm_in,
+                     uint32_t *perm_out, uint32_t *hist, cudaStream_t st) {
+    const uint32_t nb = (uint32_t)hj_ceil_div(n, kRsTile);
+    k_rs_hist<<<nb, kRsThreads, 0, st>>>(keyw, perm_in, n, shift, hist, nb);
+    k_scan_u32<<<1, 1024, 0, st>>>(hist, (uint64_t)nb * 256, nullptr);
+    k_rs_scatter<<<nb, kRsThreads, 0, st>>>(keyw, perm_in, n, shift, hist, nb, perm_out);
+}
+
+void launch_iota(uint32_t *p, uint64_t n, cudaStream_t st) {
+    if (n) k_iota<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(p, n);
+}
+
 // ------------------------------------------------------------ gather
 
 // Sorted keys row-major [n][W] (for binary searches) and sorted rows.

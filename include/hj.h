@@ -145,6 +145,24 @@ HJ_API int hj_join_count_f32(const float *A, uint64_t nA, const float *B, uint64
 HJ_API int hj_ego_sort(const double *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts, uint64_t *perm,
                        double *sorted);
 
+/* EGO sort of a device-resident point set that allocates no memory. For
+ * callers that cannot call cudaMalloc while they run: an application whose own
+ * memory pool owns the device, or a latency-critical stream that must not pay
+ * cudaMalloc's implicit synchronisation. All temporaries live in one fixed
+ * 32 MiB array inside libhj.so (a file-scope __device__ array that every GPU
+ * loading the library holds until the process exits); sizes whose temporaries
+ * exceed it (about 4 n (W + 2) bytes, W = 32-bit words of the packed cell key)
+ * are rejected with HJ_ERR_INVALID_ARG. pts: device rows [n][d], dtype_bytes 8
+ * or 4; perm: device uint32 [n] output, the same stable order as hj_ego_sort.
+ * The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress); make it before any stream capture. Calls share the
+ * array and it keeps the last call's contents: calls that overlap on the GPU
+ * race, calls on one stream are ordered. Returns once the work is queued on
+ * `stream` (NULL = default stream), after one small read-back.
+ * This entry point has no counterpart in the reference. */
+HJ_API int hj_ego_sort_device_noalloc(const void *pts, int dtype_bytes, uint64_t n, uint32_t d, double eps,
+                                      uint32_t *perm, void *stream);
+
 /* The same calls on inputs already in device memory (row-major, d per row).
  * `dtype_bytes` is 8 (FP64) or 4 (FP32). The pointers must be device (or
  * managed) memory of the device the call runs on. */
