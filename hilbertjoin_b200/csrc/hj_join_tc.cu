@@ -229,6 +229,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __shared__ __align__(8) uint64_t bar_bfull[8], bar_bempty[8];
     __shared__ uint32_t tmem_base_sh;
     __shared__ __align__(16) float epi_nb[kEpiWarps][128];
+    __shared__ __align__(16) float epi_row[kEpiWarps][32];
     __shared__ unsigned long long cta_count;
 
     const uint32_t smem_base = (smem_u32(smem_raw) + 1023u) & ~1023u;
@@ -379,26 +380,53 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const uint32_t half = (warp - 2) >> 2;  // columns [128 half, 128 half + 128)
         const uint32_t lane_base = (quad * 32u) << 16;
         float *snb = epi_nb[warp - 2];
+        float *srow = epi_row[warp - 2];
         unsigned long long cnt = 0;
         uint32_t t_cnt = 0;
-        const double T = p.T;
         // All classification is in FP32 with eps^2 rounded outward (T_lo, T_hi)
         // and the bound rounded up; the FP32 rounding of the epilogue itself is
         // part of c_rel. A pair is inside if s + tau <= T_lo, outside if
         // s - tau > T_hi, and in the band otherwise.
         const float T_lo = p.T_lo, T_hi = p.T_hi, crel = p.c_rel_f, cabs = p.c_abs_f;
-        for (uint64_t it = blockIdx.x; it < p.n_items; it += gridDim.x) {
-            const WorkItem w = p.items[it];
+        // Flat walk over (item, B tile) with the next tile's norms, group minima
+        // and tile maximum (and the next item) loaded one step ahead, so that
+        // their memory latency overlaps the current tile.
+        const uint64_t stride = gridDim.x;
+        uint64_t it = blockIdx.x;
+        WorkItem w = it < p.n_items ? p.items[it] : WorkItem{0, 0, 0, 0};
+        WorkItem wn = it + stride < p.n_items ? p.items[it + stride] : WorkItem{0, 0, 0, 0};
+        uint32_t bt = w.b0;
+        float4 pf_nbv = make_float4(0, 0, 0, 0), pf_gmin = make_float4(0, 0, 0, 0);
+        float pf_tmax = 0.f, pf_na = kPadNorm;
+        auto prefetch = [&](const WorkItem &ww, uint32_t b) {
+            const uint64_t g = (uint64_t)b * kTcTileB + half * 128;
+            pf_nbv = __ldg(reinterpret_cast<const float4 *>(p.norm_b + g) + lane);
+            pf_gmin = __ldg(reinterpret_cast<const float4 *>(p.gmin_b + g / 32));
+            pf_tmax = __ldg(p.tmax_b + b);
+            const uint64_t r = (uint64_t)ww.a * kTcTileA + quad * 32 + lane;
+            pf_na = r < p.na ? __ldg(p.norm_a + r) : kPadNorm;
+        };
+        if (it < p.n_items) prefetch(w, bt);
+        while (it < p.n_items) {
             const uint64_t gi = (uint64_t)w.a * kTcTileA + quad * 32 + lane;
             const bool row_ok = gi < p.na;
-            const float na = row_ok ? p.norm_a[gi] : kPadNorm;
-            for (uint32_t bt = w.b0; bt < w.b1; ++bt) {
+            const float na = pf_na;
+            const float4 nbv = pf_nbv, gmin = pf_gmin;
+            const float tmaxb = pf_tmax;
+            const uint32_t cur_bt = bt;
+            // advance, and prefetch the next tile
+            if (bt + 1 < w.b1) {
+                ++bt;
+            } else {
+                it += stride;
+                w = wn;
+                bt = w.b0;
+                wn = it + stride < p.n_items ? p.items[it + stride] : WorkItem{0, 0, 0, 0};
+            }
+            if (it < p.n_items) prefetch(w, bt);
+            {
                 const uint32_t acc = t_cnt & 1u;
-                const uint64_t gj0 = (uint64_t)bt * kTcTileB + half * 128;
-                // issued before the wait: the norms of this warp's 128 columns
-                const float4 nbv = __ldg(reinterpret_cast<const float4 *>(p.norm_b + gj0) + lane);
-                const float tmaxb = __ldg(p.tmax_b + bt);
-                const float4 gmin = __ldg(reinterpret_cast<const float4 *>(p.gmin_b + gj0 / 32));
+                const uint64_t gj0 = (uint64_t)cur_bt * kTcTileB + half * 128;
                 // With tau_max = c_rel (|a|^2 + max_tile |b|^2) + c_abs >= tau of every
                 // pair in the tile, and t_j = |b_j|^2 - 2 v_j, s_j = |a|^2 + t_j:
                 //   t_j <= thr_in  => s_j + tau <= eps^2  (certainly inside),
@@ -440,40 +468,50 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const float mhi = fmaf(-2.0f, fmaxf(fmaxf(mx[4], mx[5]), fmaxf(mx[6], mx[7])), g1);
 #pragma unroll
                     for (int h2 = 0; h2 < 2; ++h2) {
-                        // Rare: a 32-column half of some row of the warp may hold a pair
-                        // that is not certainly outside. Branch-free count of the certain
-                        // ones; band pairs are queued.
+                        // Rare: a 32-column half of some rows of the warp may hold a
+                        // pair that is not certainly outside. For each such row the
+                        // owning lane publishes its 32 values through shared memory
+                        // and the whole warp classifies the 32 columns at once (lane
+                        // = column), branch-free; band pairs are queued.
                         const bool need = (h2 ? mhi : mlo) <= thr_out || (p.dbg != nullptr && row_ok);
-                        if (!__any_sync(0xffffffffu, need)) continue;
+                        uint32_t rows = __ballot_sync(0xffffffffu, need);
                         const int cb = (int)(c * 64 + h2 * 32);
-                        uint32_t band_bits = 0;
-                        unsigned int in_cnt = 0;
+                        const float nbl = snb[cb + lane];
+                        while (rows) {
+                            const int L = __ffs(rows) - 1;
+                            rows &= rows - 1;
+                            if (lane == (uint32_t)L) {
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const float t = fmaf(-2.0f, v[h2 * 32 + j], snb[cb + j]);
-                            const bool ok = (unsigned)(cb + j - jlo) < (unsigned)(jhi - jlo);
-                            in_cnt += (ok && t <= thr_in) ? 1u : 0u;
-                            band_bits |= (ok && t > thr_in && t <= thr_out) ? (1u << j) : 0u;
-                            if (p.dbg != nullptr && row_ok && gj0 + cb + j < p.nb)
-                                p.dbg[(uint64_t)p.perm_a[gi] * p.nb + p.perm_b[gj0 + cb + j]] = na + t;
-                        }
-                        cnt += in_cnt;
-                        while (band_bits) {  // very rare
-                            const int j = __ffs(band_bits) - 1;
-                            band_bits &= band_bits - 1;
-                            float vj = v[h2 * 32];
-#pragma unroll
-                            for (int k = 1; k < 32; ++k) vj = (k == j) ? v[h2 * 32 + k] : vj;
-                            const float sh = na + fmaf(-2.0f, vj, snb[cb + j]);
-                            const unsigned long long k = atomicAdd(p.band_total, 1ull);
-                            if (k < p.band_cap) {
-                                BandEntry e;
-                                e.ia = (uint32_t)gi;
-                                e.jb = (uint32_t)(gj0 + cb + j);
-                                e.s_hat = sh;
-                                e.pad = 0;
-                                p.band[k] = e;
+                                for (int q = 0; q < 8; ++q)
+                                    reinterpret_cast<float4 *>(srow)[q] =
+                                        make_float4(v[h2 * 32 + 4 * q], v[h2 * 32 + 4 * q + 1], v[h2 * 32 + 4 * q + 2],
+                                                    v[h2 * 32 + 4 * q + 3]);
                             }
+                            __syncwarp();
+                            const float naL = __shfl_sync(0xffffffffu, na, L);
+                            const float tinL = __shfl_sync(0xffffffffu, thr_in, L);
+                            const float toutL = __shfl_sync(0xffffffffu, thr_out, L);
+                            const int jloL = __shfl_sync(0xffffffffu, jlo, L);
+                            const int jhiL = __shfl_sync(0xffffffffu, jhi, L);
+                            const uint64_t giL = gi - (uint64_t)lane + (uint64_t)L;
+                            const float t = fmaf(-2.0f, srow[lane], nbl);
+                            const int col = cb + (int)lane;
+                            const bool ok = (unsigned)(col - jloL) < (unsigned)(jhiL - jloL) && giL < p.na;
+                            cnt += (ok && t <= tinL) ? 1ull : 0ull;
+                            if (p.dbg != nullptr && giL < p.na && gj0 + col < p.nb)
+                                p.dbg[(uint64_t)p.perm_a[giL] * p.nb + p.perm_b[gj0 + col]] = naL + t;
+                            if (ok && t > tinL && t <= toutL) {  // band pair: very rare
+                                const unsigned long long k = atomicAdd(p.band_total, 1ull);
+                                if (k < p.band_cap) {
+                                    BandEntry e;
+                                    e.ia = (uint32_t)giL;
+                                    e.jb = (uint32_t)(gj0 + col);
+                                    e.s_hat = naL + t;
+                                    e.pad = 0;
+                                    p.band[k] = e;
+                                }
+                            }
+                            __syncwarp();
                         }
                     }
                 }
