@@ -50,13 +50,17 @@ UNIT = "pair-dist evals/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default="tf32", choices=["tf32", "bf16x3", "plain"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison step")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--n", type=int, default=N_POINTS, help=argparse.SUPPRESS)
+    ap.add_argument("--workload", default="selfjoin", choices=["selfjoin", "serving"],
+                    help="serving: the join-serving stream (not the headline line)")
+    ap.add_argument("--requests", type=int, default=2000)
+    ap.add_argument("--baseline-requests", type=int, default=200)
     return ap.parse_args()
 
 
@@ -112,10 +116,19 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
+    def mark(self):
+        """Start of the timed region: earlier samples are dropped."""
+        try:
+            self.out.flush()
+            self.skip = len(open(self.out.name).read().strip().splitlines())
+        except OSError:
+            self.skip = 0
+
     def summary(self):
         try:
             self.out.flush()
             rows = [r.split(",") for r in open(self.out.name).read().strip().splitlines() if r.strip()]
+            rows = rows[getattr(self, "skip", 0):]
         except OSError:
             rows = []
         finally:
@@ -191,8 +204,25 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_serving(args):
+    """The serving stream: throughput and p50/p99 latency of the tensor-core
+    server (continuous batching across streams) next to the plain FP64 path
+    serving one request at a time."""
+    import torch
+    torch.cuda.set_device(0)
+    from hilbertjoin_b200 import serving
+    r = serving.run_benchmark(n_requests=args.requests, form=args.form if args.form != "plain" else "tf32",
+                              baseline_requests=args.baseline_requests)
+    line = {"metric": "join-serving requests/s (p50/p99 latency)", "value": r["saturated"]["requests_per_s"],
+            "unit": "requests/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": r["workload"], "form": r["form"]}, "serving": r}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "serving":
+        return run_serving(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -225,15 +255,16 @@ def main():
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    # warm-up
-    for _ in range(args.warmup):
-        c0, st0 = step_dev(args.form)
-    # timed region: device-resident input
-    counts, kernel_ms, launches = [], [], []
     props = torch.cuda.get_device_properties(dev)
     gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(dev.index)
+    counts, kernel_ms, launches = [], [], []
     with ClockSampler(gpu_id) as clk:
+        # warm-up (the sampler starts up meanwhile; its samples are kept only
+        # from the timed region on)
+        for _ in range(args.warmup):
+            c0, st0 = step_dev(args.form)
         barrier()
+        clk.mark()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):

@@ -39,7 +39,8 @@ class HJError(RuntimeError):
 
 class Opts(ctypes.Structure):
     _fields_ = [("form", ctypes.c_int32), ("active_dims", ctypes.c_int32), ("ref_compat", ctypes.c_int32),
-                ("device", ctypes.c_int32), ("stream", ctypes.c_void_p), ("reserved", ctypes.c_uint64 * 4)]
+                ("device", ctypes.c_int32), ("stream", ctypes.c_void_p), ("shard_index", ctypes.c_int32),
+                ("shard_count", ctypes.c_int32), ("reserved", ctypes.c_uint64 * 3)]
 
 
 class Stats(ctypes.Structure):
@@ -121,7 +122,7 @@ def _check(status: int) -> None:
         raise HJError(status, lib().hj_last_error().decode())
 
 
-def _opts(form, active_dims, ref_compat, device, stream) -> Opts:
+def _opts(form, active_dims, ref_compat, device, stream, shard=None) -> Opts:
     o = Opts()
     lib().hj_opts_init(ctypes.byref(o))
     o.form = FORMS[form] if isinstance(form, str) else int(form)
@@ -129,6 +130,8 @@ def _opts(form, active_dims, ref_compat, device, stream) -> Opts:
     o.ref_compat = int(bool(ref_compat))
     o.device = -1 if device is None else int(device)
     o.stream = stream
+    if shard is not None:
+        o.shard_index, o.shard_count = int(shard[0]), int(shard[1])
     return o
 
 
@@ -154,7 +157,7 @@ def _torch_stream(x, stream):
 
 
 def self_join_count(points, eps: float, form="plain", active_dims=None, ref_compat=False, device=None,
-                    stream=None, return_stats=False):
+                    stream=None, return_stats=False, shard=None):
     """Number of unordered pairs {a, b}, a != b, of `points` with |a-b| <= eps.
 
     `points`: (n, d) float32/float64 numpy array (copied to the device inside
@@ -166,13 +169,13 @@ def self_join_count(points, eps: float, form="plain", active_dims=None, ref_comp
             raise ValueError("points must be a 2-D float32/float64 tensor")
         x = points.contiguous()
         opts = _opts(form, active_dims, ref_compat, x.device.index if device is None else device,
-                     _torch_stream(x, stream))
+                     _torch_stream(x, stream), shard)
         _check(lib().hj_self_join_count_device(ctypes.c_void_p(x.data_ptr()), x.element_size(), x.shape[0],
                                                x.shape[1], float(eps), ctypes.byref(opts), ctypes.byref(c),
                                                ctypes.byref(o)))
     else:
         x = _host_array(points)
-        opts = _opts(form, active_dims, ref_compat, device, stream)
+        opts = _opts(form, active_dims, ref_compat, device, stream, shard)
         fn = lib().hj_self_join_count if x.dtype == np.float64 else lib().hj_self_join_count_f32
         _check(fn(x.ctypes.data_as(ctypes.c_void_p), x.shape[0], x.shape[1], float(eps), ctypes.byref(opts),
                   ctypes.byref(c), ctypes.byref(o)))
@@ -180,7 +183,7 @@ def self_join_count(points, eps: float, form="plain", active_dims=None, ref_comp
 
 
 def join_count(a, b, eps: float, form="plain", active_dims=None, ref_compat=False, device=None, stream=None,
-               return_stats=False):
+               return_stats=False, shard=None):
     """Number of ordered pairs (p in a, q in b) with |p-q| <= eps."""
     o = Stats()
     c = ctypes.c_uint64(0)
@@ -189,7 +192,7 @@ def join_count(a, b, eps: float, form="plain", active_dims=None, ref_compat=Fals
         if xa.dtype != xb.dtype or xa.shape[1] != xb.shape[1]:
             raise ValueError("a and b must have the same dtype and dimension")
         opts = _opts(form, active_dims, ref_compat, xa.device.index if device is None else device,
-                     _torch_stream(xa, stream))
+                     _torch_stream(xa, stream), shard)
         _check(lib().hj_join_count_device(ctypes.c_void_p(xa.data_ptr()), xa.shape[0], ctypes.c_void_p(xb.data_ptr()),
                                           xb.shape[0], xa.element_size(), xa.shape[1], float(eps),
                                           ctypes.byref(opts), ctypes.byref(c), ctypes.byref(o)))
@@ -199,7 +202,7 @@ def join_count(a, b, eps: float, form="plain", active_dims=None, ref_compat=Fals
             xb = xb.astype(xa.dtype)
         if xa.shape[1] != xb.shape[1]:
             raise ValueError("a and b must have the same dimension")
-        opts = _opts(form, active_dims, ref_compat, device, stream)
+        opts = _opts(form, active_dims, ref_compat, device, stream, shard)
         fn = lib().hj_join_count if xa.dtype == np.float64 else lib().hj_join_count_f32
         _check(fn(xa.ctypes.data_as(ctypes.c_void_p), xa.shape[0], xb.ctypes.data_as(ctypes.c_void_p), xb.shape[0],
                   xa.shape[1], float(eps), ctypes.byref(opts), ctypes.byref(c), ctypes.byref(o)))

@@ -404,6 +404,16 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
     if (r == 2) return fail(HJ_ERR_OOM, err);
     if (r == 3) return fail(HJ_ERR_CUDA, err);
     if (r) return fail(HJ_ERR_INVALID_ARG, err);
+    if (opts && opts->shard_count > 1) {
+        if (opts->shard_index < 0 || opts->shard_index >= opts->shard_count)
+            return fail(HJ_ERR_INVALID_ARG, "shard_index out of range");
+        IndexResult sh;
+        int sr = shard_items(idx, opts->shard_index, opts->shard_count, slot_alloc_cb, &actx, st, &sh);
+        if (sr == 2) return fail(HJ_ERR_OOM, "out of device memory (shard)");
+        if (sr) return check_cuda("shard selection");
+        launches += 3;
+        idx = sh;
+    }
     cudaEventRecord(c->ev[3], st);
 
     // 4. distance kernels. d_small: [2] count of the tensor-core kernel and the

@@ -303,7 +303,52 @@ __global__ void k_permute_items(const WorkItem *__restrict__ in, const uint32_t 
 
 // Scratch slots requested through the caller's allocator.
 enum { kSlotRuns = 40, kSlotNruns, kSlotCounts, kSlotItemsTmp, kSlotItems, kSlotItemKeys, kSlotItemPerm,
-       kSlotItemPermTmp, kSlotItemHist, kSlotIdxStats, kSlotSplitFlags, kSlotSplitTc, kSlotSplitFp, kSlotSplitStats };
+       kSlotItemPermTmp, kSlotItemHist, kSlotIdxStats, kSlotSplitFlags, kSlotSplitTc, kSlotSplitFp, kSlotSplitStats,
+       kSlotShardLoad, kSlotShardCut };
+
+__global__ void k_item_loads(const WorkItem *__restrict__ items, uint64_t n, uint32_t *load) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) load[i] = items[i].b1 - items[i].b0;
+}
+
+// cut[0], cut[1]: first items whose exclusive load prefix reaches lo and hi.
+__global__ void k_shard_cut(const uint32_t *__restrict__ prefix, uint64_t n, unsigned long long lo,
+                            unsigned long long hi, unsigned long long *cut) {
+    for (int c = 0; c < 2; ++c) {
+        const unsigned long long target = c ? hi : lo;
+        uint64_t a = 0, b = n;
+        while (a < b) {
+            uint64_t m = (a + b) >> 1;
+            if ((unsigned long long)prefix[m] < target) a = m + 1; else b = m;
+        }
+        cut[c] = a;
+    }
+}
+
+int shard_items(const IndexResult &in, int k, int K, void *(*alloc)(void *ctx, int slot, size_t bytes), void *actx,
+                cudaStream_t st, IndexResult *out) {
+    *out = in;
+    if (K <= 1 || in.n_items == 0) return 0;
+    const uint64_t n = in.n_items;
+    uint32_t *load = (uint32_t *)alloc(actx, kSlotShardLoad, (n + 1) * sizeof(uint32_t));
+    unsigned long long *cut = (unsigned long long *)alloc(actx, kSlotShardCut, 4 * sizeof(unsigned long long));
+    if (!load || !cut) return 2;
+    k_item_loads<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(in.items, n, load);
+    launch_scan_u32(load, n, cut + 2, st);
+    unsigned long long total = 0;
+    cudaMemcpyAsync(&total, cut + 2, 8, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return 3;
+    const unsigned long long lo = total * (unsigned long long)k / (unsigned long long)K;
+    const unsigned long long hi = total * (unsigned long long)(k + 1) / (unsigned long long)K;
+    k_shard_cut<<<1, 1, 0, st>>>(load, n, lo, hi, cut);
+    unsigned long long hc[2];
+    cudaMemcpyAsync(hc, cut, 16, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return 3;
+    const uint64_t a = hc[0], b = k + 1 == K ? n : hc[1];
+    out->items = in.items + a;
+    out->n_items = b > a ? b - a : 0;
+    return 0;
+}
 
 __global__ void k_item_precision_flags(const WorkItem *__restrict__ items, uint64_t n, const float *__restrict__ tmax_a,
                                        const float *__restrict__ tmax_b, double c_rel, double c_abs, double limit,
@@ -413,7 +458,7 @@ int build_index(const SortedSet &A, const SortedSet &B, const Grid &grid, const 
     ba.nruns = nruns;
     ba.cand = stats;
     size_t smem = (size_t)kBoundsWarps * (2 * grid.W + 2 * kMaxCombos) * sizeof(uint32_t);
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_tile_bounds, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (smem > 48 * 1024) ensure_max_dynamic_smem((const void *)k_tile_bounds, (int)smem);
     k_tile_bounds<<<(unsigned)hj_ceil_div(n_tiles, kBoundsWarps), kBoundsWarps * 32, smem, st>>>(ba, n_tiles);
     k_item_counts<<<(unsigned)hj_ceil_div(n_tiles, 256), 256, 0, st>>>(runs, nruns, n_tiles, chunk, counts,
                                                                      stats + 1);

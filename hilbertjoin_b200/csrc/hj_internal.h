@@ -108,12 +108,24 @@ int split_items_by_precision(const IndexResult &tc_in, const SortedSet &A, const
                              double c_abs, double limit, void *(*alloc)(void *ctx, int slot, size_t bytes),
                              void *actx, cudaStream_t st, IndexResult *tc_out, IndexResult *fp_out);
 
+// Restricts a work list to shard k of K: the contiguous item range whose
+// cumulative tile-pair load lies in [k L / K, (k+1) L / K) (L = total load).
+// Synchronises once on `st`.
+int shard_items(const IndexResult &in, int k, int K, void *(*alloc)(void *ctx, int slot, size_t bytes), void *actx,
+                cudaStream_t st, IndexResult *out);
+
 struct IndexResult {
     WorkItem *items = nullptr;  // device, Hilbert ordered
     uint64_t n_items = 0;
     uint64_t tile_pairs = 0;
     uint64_t candidate_pairs = 0;
 };
+
+// Raises a kernel's dynamic shared memory limit to `bytes` on the current
+// device, once, and never lowers it: the attribute is global to the function,
+// so per-call values would race between host threads launching the same
+// kernel with different sizes.
+void ensure_max_dynamic_smem(const void *func, int bytes);
 
 // ---- launch wrappers (all asynchronous on `st` unless noted) ----------------
 

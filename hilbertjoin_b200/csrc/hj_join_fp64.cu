@@ -208,11 +208,8 @@ void launch_join_fp64(const SortedSet &A, const SortedSet &B, bool self, uint64_
     a.count = d_count;
     a.err = d_err;
     const size_t smem = (size_t)3 * A.d * kPlainTile * sizeof(double);
-    static thread_local int configured_smem = 0;
-    if ((int)smem > configured_smem) {
-        cudaFuncSetAttribute(k_join_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        configured_smem = (int)smem;
-    }
+    // the largest this kernel ever needs (d <= 128), set once
+    ensure_max_dynamic_smem((const void *)k_join_fp64, 3 * 128 * kPlainTile * (int)sizeof(double));
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_join_fp64, kPlainThreads, smem);
     if (per_sm < 1) per_sm = 1;

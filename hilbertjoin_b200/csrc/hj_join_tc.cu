@@ -650,7 +650,7 @@ static TcLayout tc_layout(int form, uint32_t d) {
     size_t left = budget - L.a_bufs * a_bytes;
     L.nst = (uint32_t)(left / kBStageBytes);
     if (L.nst > 8) L.nst = 8;
-    L.smem = L.a_bufs * a_bytes + (size_t)L.nst * kBStageBytes + 1024;
+    L.smem = L.a_bufs * a_bytes + (size_t)L.nst * kBStageBytes + 1024;  // <= 221 KB
     return L;
 }
 
@@ -714,10 +714,10 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, bool self, uint64_t n
     uint64_t grid = (uint64_t)num_sms;
     if (grid > idx.n_items) grid = idx.n_items;
     if (!bf) {
-        cudaFuncSetAttribute(k_join_tc<HJ_FORM_TC_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
+        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_TF32>, 221 * 1024);
         k_join_tc<HJ_FORM_TC_TF32><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
     } else {
-        cudaFuncSetAttribute(k_join_tc<HJ_FORM_TC_BF16X3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
+        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_BF16X3>, 221 * 1024);
         k_join_tc<HJ_FORM_TC_BF16X3><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
     }
     cudaError_t e = cudaGetLastError();

@@ -11,6 +11,9 @@
 // indices, and every data layout is written once, by the gather.
 #include <cuda_bf16.h>
 
+#include <map>
+#include <mutex>
+
 #include "hj_common.cuh"
 #include "hj_internal.h"
 
@@ -249,6 +252,19 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint32_t *__res
         __syncthreads();
         if (valid) perm_out[s_wcnt[warp][dig] + rank] = src;
         __syncthreads();
+    }
+}
+
+void ensure_max_dynamic_smem(const void *func, int bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, int> done;  // (function, device) -> bytes set
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    int &cur = done[{func, dev}];
+    if (bytes > cur) {
+        cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cur = bytes;
     }
 }
 

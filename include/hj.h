@@ -81,7 +81,11 @@ typedef struct {
                               points of each set, as the reference's block loops do */
     int32_t device;        /* CUDA device ordinal; -1 = current */
     void *stream;          /* cudaStream_t to run on; NULL = the calling thread's own stream */
-    uint64_t reserved[4];
+    int32_t shard_index;   /* with shard_count > 1: count only shard `shard_index` of the join's */
+    int32_t shard_count;   /* work list (contiguous, equal-load ranges of the Hilbert-ordered block
+                              pairs, the reference's equal-load split egojoin.h:214-222). The counts
+                              of shards 0..shard_count-1 sum to the full count. */
+    uint64_t reserved[3];
 } hj_opts;
 
 /* Per-call statistics (all optional). Times are device times of each stage

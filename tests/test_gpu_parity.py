@@ -205,3 +205,18 @@ def test_medium_sparse_config_shape(hj):
     c, st = hj.self_join_count(x, 0.2, return_stats=True)
     assert c == 0
     assert st["loadpercent"] < 60.0
+
+
+@pytest.mark.parametrize("form", ["plain", "tf32"])
+@pytest.mark.parametrize("K", [2, 3, 4])
+def test_shards_sum_to_full_count(hj, form, K):
+    """The device shard selection (equal-load ranges of the work list) partitions the work."""
+    from hilbertjoin_b200 import workloads as W
+    x = W.gmm(20000, 16, 5)
+    eps = 0.08
+    full = hj.self_join_count(x, eps, form=form)
+    parts = [hj.self_join_count(x, eps, form=form, shard=(k, K)) for k in range(K)]
+    assert sum(parts) == full
+    a, b = W.uniform(6000, 8, 1), W.uniform(5000, 8, 2)
+    fj = hj.join_count(a, b, 0.3, form=form)
+    assert sum(hj.join_count(a, b, 0.3, form=form, shard=(k, K)) for k in range(K)) == fj
