@@ -263,8 +263,18 @@ void ensure_max_dynamic_smem(const void *func, int bytes) {
     std::lock_guard<std::mutex> lk(mu);
     int &cur = done[{func, dev}];
     if (bytes > cur) {
-        cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        cur = bytes;
+        // never above what fits next to the kernel's static shared memory
+        int optin = 0;
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, func) == cudaSuccess && optin > 0) {
+            const int room = optin - (int)fa.sharedSizeBytes;
+            if (bytes > room) bytes = room;
+        }
+        cudaGetLastError();
+        if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess)
+            cur = bytes;
+        cudaGetLastError();
     }
 }
 
