@@ -26,6 +26,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -336,14 +337,15 @@ def main():
     roof["kernel_ms"] = kms
     roof["algorithmic_flops_per_launch"] = flops
     roof["traffic"] = None
-    tpath = os.path.join(ROOT, "profiles", f"traffic_{roof['kernel']}_{args.form}.json")
-    if os.path.exists(tpath):
-        try:
-            tj = json.load(open(tpath))
-            roof["traffic"] = tj.get("bytes_per_launch_full_size")
-            roof["traffic_source"] = tj.get("source")
-        except (OSError, ValueError):
-            pass
+    # one-pass ncu capture of dram__bytes_read.sum + dram__bytes_write.sum on this exact
+    # workload, summarised under profiles/ (the line "bytes_per_launch_full_size: N")
+    tname = f"{roof['kernel']}_{args.form}_selfjoin_1Mx64_dram_traffic.md"
+    tpath = os.path.join(ROOT, "profiles", tname)
+    if args.n == N_POINTS and os.path.exists(tpath):
+        m = re.search(r"^bytes_per_launch_full_size:\s*(\d+)", open(tpath).read(), re.M)
+        if m:
+            roof["traffic"] = int(m.group(1))
+            roof["traffic_source"] = f"profiles/{tname}"
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:

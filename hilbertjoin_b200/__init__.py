@@ -28,7 +28,8 @@ FORM_NAMES = {0: "plain_fp64", 1: "tc_tf32", 2: "tc_bf16x3", 3: "auto"}
 OK = 0
 STATUS = {0: "ok", 1: "invalid argument", 2: "out of device memory", 3: "CUDA error", 4: "device wait timed out",
           5: "band queue overflow", 6: "no usable device", 7: "unsupported input for this form",
-          8: "rejected by admission", 9: "not found"}
+          8: "rejected by admission", 9: "not found", 10: "output buffer too small"}
+ERR_CAPACITY = 10
 
 
 class HJError(RuntimeError):
@@ -40,7 +41,8 @@ class HJError(RuntimeError):
 class Opts(ctypes.Structure):
     _fields_ = [("form", ctypes.c_int32), ("active_dims", ctypes.c_int32), ("ref_compat", ctypes.c_int32),
                 ("device", ctypes.c_int32), ("stream", ctypes.c_void_p), ("shard_index", ctypes.c_int32),
-                ("shard_count", ctypes.c_int32), ("reserved", ctypes.c_uint64 * 3)]
+                ("shard_count", ctypes.c_int32), ("reorder_dims", ctypes.c_int32), ("reserved_i", ctypes.c_int32),
+                ("reserved", ctypes.c_uint64 * 2)]
 
 
 class Stats(ctypes.Structure):
@@ -52,7 +54,7 @@ class Stats(ctypes.Structure):
                 ("band_fraction", ctypes.c_double), ("band_halfwidth_rel", ctypes.c_double),
                 ("max_abs_err_band", ctypes.c_double), ("fp64_items", ctypes.c_uint64),
                 ("form_used", ctypes.c_int32), ("stripes", ctypes.c_int32), ("kernel_launches", ctypes.c_int32),
-                ("reserved_i", ctypes.c_int32), ("reserved", ctypes.c_uint64 * 4)]
+                ("reserved_i", ctypes.c_int32), ("reorder_ms", ctypes.c_double), ("reserved", ctypes.c_uint64 * 3)]
 
     def to_dict(self) -> dict:
         d = {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("reserved")}
@@ -94,6 +96,11 @@ def lib() -> ctypes.CDLL:
         "hj_self_join_count_f32": (I, [P, U64, U32, D, pO, pU64, pS]),
         "hj_join_count": (I, [P, U64, P, U64, U32, D, pO, pU64, pS]),
         "hj_join_count_f32": (I, [P, U64, P, U64, U32, D, pO, pU64, pS]),
+        "hj_self_join_pairs": (I, [P, U64, U32, D, pO, P, U64, pU64, pS]),
+        "hj_self_join_pairs_f32": (I, [P, U64, U32, D, pO, P, U64, pU64, pS]),
+        "hj_join_pairs": (I, [P, U64, P, U64, U32, D, pO, P, U64, pU64, pS]),
+        "hj_join_pairs_f32": (I, [P, U64, P, U64, U32, D, pO, P, U64, pU64, pS]),
+        "hj_dim_order": (I, [P, U64, U32, D, pO, P, P]),
         "hj_self_join_count_device": (I, [P, I, U64, U32, D, pO, pU64, pS]),
         "hj_join_count_device": (I, [P, U64, P, U64, I, U32, D, pO, pU64, pS]),
         "hj_debug_tc_estimates": (I, [P, U64, P, U64, U32, I, P]),
@@ -122,7 +129,7 @@ def _check(status: int) -> None:
         raise HJError(status, lib().hj_last_error().decode())
 
 
-def _opts(form, active_dims, ref_compat, device, stream, shard=None) -> Opts:
+def _opts(form, active_dims, ref_compat, device, stream, shard=None, reorder_dims=False) -> Opts:
     o = Opts()
     lib().hj_opts_init(ctypes.byref(o))
     o.form = FORMS[form] if isinstance(form, str) else int(form)
@@ -132,6 +139,7 @@ def _opts(form, active_dims, ref_compat, device, stream, shard=None) -> Opts:
     o.stream = stream
     if shard is not None:
         o.shard_index, o.shard_count = int(shard[0]), int(shard[1])
+    o.reorder_dims = int(bool(reorder_dims))
     return o
 
 
@@ -157,7 +165,7 @@ def _torch_stream(x, stream):
 
 
 def self_join_count(points, eps: float, form="plain", active_dims=None, ref_compat=False, device=None,
-                    stream=None, return_stats=False, shard=None):
+                    stream=None, return_stats=False, shard=None, reorder_dims=False):
     """Number of unordered pairs {a, b}, a != b, of `points` with |a-b| <= eps.
 
     `points`: (n, d) float32/float64 numpy array (copied to the device inside
@@ -169,13 +177,13 @@ def self_join_count(points, eps: float, form="plain", active_dims=None, ref_comp
             raise ValueError("points must be a 2-D float32/float64 tensor")
         x = points.contiguous()
         opts = _opts(form, active_dims, ref_compat, x.device.index if device is None else device,
-                     _torch_stream(x, stream), shard)
+                     _torch_stream(x, stream), shard, reorder_dims)
         _check(lib().hj_self_join_count_device(ctypes.c_void_p(x.data_ptr()), x.element_size(), x.shape[0],
                                                x.shape[1], float(eps), ctypes.byref(opts), ctypes.byref(c),
                                                ctypes.byref(o)))
     else:
         x = _host_array(points)
-        opts = _opts(form, active_dims, ref_compat, device, stream, shard)
+        opts = _opts(form, active_dims, ref_compat, device, stream, shard, reorder_dims)
         fn = lib().hj_self_join_count if x.dtype == np.float64 else lib().hj_self_join_count_f32
         _check(fn(x.ctypes.data_as(ctypes.c_void_p), x.shape[0], x.shape[1], float(eps), ctypes.byref(opts),
                   ctypes.byref(c), ctypes.byref(o)))
@@ -183,7 +191,7 @@ def self_join_count(points, eps: float, form="plain", active_dims=None, ref_comp
 
 
 def join_count(a, b, eps: float, form="plain", active_dims=None, ref_compat=False, device=None, stream=None,
-               return_stats=False, shard=None):
+               return_stats=False, shard=None, reorder_dims=False):
     """Number of ordered pairs (p in a, q in b) with |p-q| <= eps."""
     o = Stats()
     c = ctypes.c_uint64(0)
@@ -192,7 +200,7 @@ def join_count(a, b, eps: float, form="plain", active_dims=None, ref_compat=Fals
         if xa.dtype != xb.dtype or xa.shape[1] != xb.shape[1]:
             raise ValueError("a and b must have the same dtype and dimension")
         opts = _opts(form, active_dims, ref_compat, xa.device.index if device is None else device,
-                     _torch_stream(xa, stream), shard)
+                     _torch_stream(xa, stream), shard, reorder_dims)
         _check(lib().hj_join_count_device(ctypes.c_void_p(xa.data_ptr()), xa.shape[0], ctypes.c_void_p(xb.data_ptr()),
                                           xb.shape[0], xa.element_size(), xa.shape[1], float(eps),
                                           ctypes.byref(opts), ctypes.byref(c), ctypes.byref(o)))
@@ -202,11 +210,78 @@ def join_count(a, b, eps: float, form="plain", active_dims=None, ref_compat=Fals
             xb = xb.astype(xa.dtype)
         if xa.shape[1] != xb.shape[1]:
             raise ValueError("a and b must have the same dimension")
-        opts = _opts(form, active_dims, ref_compat, device, stream, shard)
+        opts = _opts(form, active_dims, ref_compat, device, stream, shard, reorder_dims)
         fn = lib().hj_join_count if xa.dtype == np.float64 else lib().hj_join_count_f32
         _check(fn(xa.ctypes.data_as(ctypes.c_void_p), xa.shape[0], xb.ctypes.data_as(ctypes.c_void_p), xb.shape[0],
                   xa.shape[1], float(eps), ctypes.byref(opts), ctypes.byref(c), ctypes.byref(o)))
     return (int(c.value), o.to_dict()) if return_stats else int(c.value)
+
+
+def _pairs(call, n_hint: int, capacity, return_stats: bool):
+    """Runs a pair entry point, growing the output to the exact total when the
+    first buffer is too small (the library writes nothing in that case)."""
+    o = Stats()
+    cnt = ctypes.c_uint64(0)
+    cap = int(capacity) if capacity is not None else max(1 << 16, 4 * n_hint)
+    for _ in range(2):
+        out = np.empty((max(cap, 1), 2), dtype=np.uint64)
+        st = call(out.ctypes.data_as(ctypes.c_void_p), cap, ctypes.byref(cnt), ctypes.byref(o))
+        if st == ERR_CAPACITY and capacity is None:
+            cap = int(cnt.value)
+            continue
+        _check(st)
+        res = out[:int(cnt.value)]
+        return (res, o.to_dict()) if return_stats else res
+    _check(st)
+
+
+def self_join_pairs(points, eps: float, active_dims=None, ref_compat=False, device=None, capacity=None,
+                    return_stats=False, shard=None, reorder_dims=False):
+    """The unordered pairs {i, j}, i < j, of `points` (input indices) with
+    |p_i - p_j| <= eps, as a (k, 2) uint64 array sorted by (i, j). Exactly the
+    pairs self_join_count counts (plain FP64 form). `capacity`: the most pairs
+    the caller accepts (HJError with status 10 beyond it); None = as many as
+    there are."""
+    x = _host_array(points)
+    opts = _opts("plain", active_dims, ref_compat, device, None, shard, reorder_dims)
+    fn = lib().hj_self_join_pairs if x.dtype == np.float64 else lib().hj_self_join_pairs_f32
+
+    def call(buf, cap, cnt, st):
+        return fn(x.ctypes.data_as(ctypes.c_void_p), x.shape[0], x.shape[1], float(eps), ctypes.byref(opts), buf,
+                  cap, cnt, st)
+    return _pairs(call, x.shape[0], capacity, return_stats)
+
+
+def join_pairs(a, b, eps: float, active_dims=None, ref_compat=False, device=None, capacity=None,
+               return_stats=False, shard=None, reorder_dims=False):
+    """The ordered pairs (i in a, j in b) with |a_i - b_j| <= eps, (k, 2) uint64
+    sorted by (i, j)."""
+    xa, xb = _host_array(a), _host_array(b)
+    if xa.dtype != xb.dtype:
+        xb = xb.astype(xa.dtype)
+    if xa.shape[1] != xb.shape[1]:
+        raise ValueError("a and b must have the same dimension")
+    opts = _opts("plain", active_dims, ref_compat, device, None, shard, reorder_dims)
+    fn = lib().hj_join_pairs if xa.dtype == np.float64 else lib().hj_join_pairs_f32
+
+    def call(buf, cap, cnt, st):
+        return fn(xa.ctypes.data_as(ctypes.c_void_p), xa.shape[0], xb.ctypes.data_as(ctypes.c_void_p), xb.shape[0],
+                  xa.shape[1], float(eps), ctypes.byref(opts), buf, cap, cnt, st)
+    return _pairs(call, xa.shape[0], capacity, return_stats)
+
+
+def dim_order(points, eps: float, device=None, return_costs=False):
+    """reorder_dim (int32, d): the key position of every dim when the dims are
+    ranked by ascending sampled cost (the reference's outputStatistics
+    convention), and optionally the d costs (uint64)."""
+    x = np.ascontiguousarray(np.asarray(points, dtype=np.float64))
+    rd = np.zeros(x.shape[1], dtype=np.int32)
+    costs = np.zeros(x.shape[1], dtype=np.uint64)
+    opts = _opts("plain", None, False, device, None)
+    _check(lib().hj_dim_order(x.ctypes.data_as(ctypes.c_void_p), x.shape[0], x.shape[1], float(eps),
+                              ctypes.byref(opts), rd.ctypes.data_as(ctypes.c_void_p),
+                              costs.ctypes.data_as(ctypes.c_void_p)))
+    return (rd, costs) if return_costs else rd
 
 
 def ego_sort(points, eps: float, device=None):

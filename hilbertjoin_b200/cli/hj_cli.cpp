@@ -11,10 +11,13 @@
 //           the reference does, which hard-codes 2)
 //   -t T, -k K, -a A   accepted and ignored, as in the reference
 // Extensions: -F plain|tf32|bf16x3|auto (distance form, default plain),
-//             -r (count like the reference: first 8*floor(n/8) EGO-sorted points).
+//             -r (count like the reference: first 8*floor(n/8) EGO-sorted points),
+//             -R 0|1 (dimension reordering off/on; on by default for the join,
+//             which the reference's join driver always reorders,
+//             mainJoin.cpp:97-100, off for the self-join, which never does).
 // Output: the reference's one-line format (main.cpp:122, mainJoin.cpp:139).
 // THREADS reports the GPU's SM count, KBLOCK the early-exit granularity (8
-// dims), REORDERTIME is 0 (no dimension reordering), WH is 0.
+// dims), REORDERTIME the dimension cost and ordering step, WH is 0.
 //
 // Without -f/-g the sets are uniform [0,1) from the MCG31m1 recurrence
 // x <- 1132489760 x mod (2^31 - 1), seeded 15 * seed with seed 1 for A and 2
@@ -103,10 +106,12 @@ static bool read_points(const std::string &path, size_t n, size_t d, std::vector
 
 static void usage(const char *prog) {
 #ifdef HJ_CLI_JOIN
-    fprintf(stderr, "Usage: %s -n N -m M -e EPS -d D [-f fileA] [-g fileB] [-F plain|tf32|bf16x3|auto] [-r]\n", prog);
+    fprintf(stderr, "Usage: %s -n N -m M -e EPS -d D [-f fileA] [-g fileB] [-F plain|tf32|bf16x3|auto] [-r] [-R 0|1]\n",
+            prog);
     fprintf(stderr, "Example: %s -n 200000 -m 200000 -e 0.2 -d 20\n", prog);
 #else
-    fprintf(stderr, "Usage: %s -n N -e EPS -d D [-f file] [-s activedims] [-F plain|tf32|bf16x3|auto] [-r]\n", prog);
+    fprintf(stderr, "Usage: %s -n N -e EPS -d D [-f file] [-s activedims] [-F plain|tf32|bf16x3|auto] [-r] [-R 0|1]\n",
+            prog);
     fprintf(stderr, "Example: %s -n 200000 -e 0.2 -d 64\n", prog);
 #endif
 }
@@ -118,12 +123,17 @@ int main(int argc, char **argv) {
     int actdim = 3;
     int form = HJ_FORM_PLAIN_FP64;
     bool refc = false;
+#ifdef HJ_CLI_JOIN
+    int reorder = 1;
+#else
+    int reorder = 0;
+#endif
     if (argc < 5) {
         usage(argv[0]);
         return 1;
     }
     int c;
-    while ((c = getopt(argc, argv, "n:m:e:d:t:f:g:k:a:s:F:r")) != -1) {
+    while ((c = getopt(argc, argv, "n:m:e:d:t:f:g:k:a:s:F:rR:")) != -1) {
         switch (c) {
             case 'n': n = strtoull(optarg, 0, 10); break;
             case 'm': m = strtoull(optarg, 0, 10); break;
@@ -133,6 +143,7 @@ int main(int argc, char **argv) {
             case 'g': fb = optarg; break;
             case 's': actdim = atoi(optarg); break;
             case 'r': refc = true; break;
+            case 'R': reorder = atoi(optarg) != 0; break;
             case 'F':
                 if (!strcmp(optarg, "plain")) form = HJ_FORM_PLAIN_FP64;
                 else if (!strcmp(optarg, "tf32")) form = HJ_FORM_TC_TF32;
@@ -168,6 +179,7 @@ int main(int argc, char **argv) {
     hj_opts_init(&o);
     o.form = form;
     o.ref_compat = refc ? 1 : 0;
+    o.reorder_dims = reorder;
     hj_stats st;
     uint64_t count = 0;
     auto t0 = std::chrono::steady_clock::now();
@@ -186,16 +198,16 @@ int main(int argc, char **argv) {
         return 2;
     }
     int sms = hj_device_sm_count(-1);
-    double sort_s = st.sort_ms / 1e3, index_s = st.index_ms / 1e3;
+    double sort_s = st.sort_ms / 1e3, index_s = st.index_ms / 1e3, reorder_s = st.reorder_ms / 1e3;
     double jppp = count == 0 ? 0.0 : (double)count / (double)n;
     const int kblock = 8;
     int stripes = st.stripes;
 #ifdef HJ_CLI_JOIN
     printf("%zu;%zu;%zu;%f;%d;%2.14f;%d;%d;%f;%f;%f;%f;%f;%ld;%f;%f\n", n, m, d, jppp, sms, eps, stripes, kblock,
-           total, total - sort_s, sort_s, index_s, 0.0, (long)count, st.loadpercent, 0.0);
+           total, total - sort_s - reorder_s, sort_s, index_s, reorder_s, (long)count, st.loadpercent, 0.0);
 #else
     printf("%zu;%zu;%f;%d;%2.14f;%d;%d;%f;%f;%f;%f;%f;%zu;%f;%f\n", n, d, jppp, sms, eps, stripes, kblock, total,
-           total - sort_s, sort_s, index_s, 0.0, (size_t)count, st.loadpercent, 0.0);
+           total - sort_s - reorder_s, sort_s, index_s, reorder_s, (size_t)count, st.loadpercent, 0.0);
 #endif
     return 0;
 }

@@ -132,6 +132,8 @@ enum {
     kSlotRowsA, kSlotRowsB, kSlotKeysA, kSlotKeysB, kSlotTilesA, kSlotTilesB,
     kSlotTf32A, kSlotTf32B, kSlotHiA, kSlotLoA, kSlotHiB, kSlotLoB, kSlotNormA, kSlotNormB,
     kSlotTmaxAA, kSlotTmaxAB, kSlotTmaxBA, kSlotTmaxBB, kSlotBand, kSlotCenter, kSlotGminA, kSlotGminB,
+    kSlotItemCnt, kSlotPairKeys, kSlotPairPerm, kSlotPairTmp, kSlotPairHist, kSlotPairOut, kSlotDimCost,
+    kSlotGridOrd,
 };
 
 static int bitwidth(unsigned long long v) {
@@ -140,9 +142,14 @@ static int bitwidth(unsigned long long v) {
     return b;
 }
 
-// Plans the packed key layout from the per-dim cell ranges.
-static int plan_grid(const std::vector<DimStats> &ds, uint32_t d, double eps, double maxabs, Grid *g) {
+// Plans the packed key layout from the per-dim cell ranges. `ord` (empty =
+// identity) lists the dims from the most significant key field down.
+static int plan_grid(const std::vector<DimStats> &ds, uint32_t d, double eps, double maxabs,
+                     const std::vector<uint32_t> &ord, Grid *g) {
     g->d = d;
+    g->ord = ord;
+    if (g->ord.empty())
+        for (uint32_t t = 0; t < d; ++t) g->ord.push_back(t);
     g->eps = eps;
     g->maxabs = maxabs;
     g->eps_wide = eps + std::ldexp(eps + maxabs, -40);
@@ -152,7 +159,8 @@ static int plan_grid(const std::vector<DimStats> &ds, uint32_t d, double eps, do
     g->shift.resize(d);
     g->range.resize(d);
     uint32_t w = 0, left = 32;
-    for (uint32_t t = 0; t < d; ++t) {
+    for (uint32_t pos = 0; pos < d; ++pos) {
+        const uint32_t t = g->ord[pos];
         long long lo = ds[t].cmin, hi = ds[t].cmax;
         if (lo > hi) lo = hi = 0;  // empty set
         long long range = hi - lo;
@@ -297,17 +305,48 @@ static int ensure_plain_tiles(Ctx *c, cudaStream_t st, SortedSet *s, bool is_b, 
     return check_cuda("plain layout");
 }
 
-static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *count, hj_stats *stats,
-                    cudaEvent_t ev_h2d_start) {
-    cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
-    int form = opts ? opts->form : HJ_FORM_PLAIN_FP64;
+// Key order by ascending dimension cost (ties by dim index) from set A's
+// sample; see hj_dim_order. Synchronises once on `st`.
+static int dim_order_by_cost(Ctx *c, cudaStream_t st, const void *x, int dtype_bytes, uint64_t n, uint32_t d,
+                             double eps, const DimStats *ds, std::vector<uint32_t> *ord,
+                             std::vector<unsigned long long> *costs) {
+    unsigned long long *dcost = (unsigned long long *)slot_alloc_impl(c, st, kSlotDimCost, d * 8);
+    if (!dcost) return fail(HJ_ERR_OOM, "out of device memory");
+    launch_dim_cost(x, dtype_bytes, n, d, eps, ds, dcost, st);
+    costs->assign(d, 0);
+    cudaMemcpyAsync(costs->data(), dcost, d * 8, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("dimension cost");
+    if (int r = check_cuda("dimension cost")) return r;
+    ord->resize(d);
+    for (uint32_t t = 0; t < d; ++t) (*ord)[t] = t;
+    std::stable_sort(ord->begin(), ord->end(),
+                     [&](uint32_t a, uint32_t b) { return (*costs)[a] < (*costs)[b]; });
+    return HJ_OK;
+}
+
+// Everything before the distance kernels: cell statistics, key layout, EGO
+// sort and layouts of both sets, stripe index and work list (and the shard).
+struct Prepared {
+    int form = HJ_FORM_PLAIN_FP64;
+    int active_dims = 0;
+    double maxabs = 0;
+    Grid g;
+    GridDev gd;
+    SortedSet A, B;
+    IndexResult idx;
+    uint64_t na_eff = 0, nb_eff = 0;
+    int launches = 0;
+    double reorder_ms = 0;
+};
+
+static int prepare_join(Ctx *c, cudaStream_t st, const JoinIn &in, const hj_opts *opts, int form_override,
+                        Prepared *P) {
+    int form = form_override >= 0 ? form_override : (opts ? opts->form : HJ_FORM_PLAIN_FP64);
     int active_dims = opts ? opts->active_dims : -1;
     const bool ref_compat = opts && opts->ref_compat;
     if (active_dims < 0) active_dims = in.self ? 3 : 2;
     if (active_dims > kMaxActiveDims) active_dims = kMaxActiveDims;
     int launches = 0;
-    auto t_wall0 = std::chrono::steady_clock::now();
-    cudaEventRecord(c->ev[1], st);  // after H2D
 
     const uint32_t d = in.d;
     // 1. per-dim cell ranges (union of both sets), read back to plan the keys
@@ -339,9 +378,22 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
     if (form_is_tc(form) && d > 256) return fail(HJ_ERR_UNSUPPORTED, "tensor-core forms support d <= 256");
     if (form_is_tc(form) && !(maxabs < 1e18)) return fail(HJ_ERR_UNSUPPORTED, "tensor-core forms need |x| < 1e18");
     if (form == HJ_FORM_PLAIN_FP64 && d > 128) return fail(HJ_ERR_UNSUPPORTED, "plain FP64 form supports d <= 128");
-    Grid g;
-    if (int r = plan_grid(hds, d, in.eps, maxabs, &g)) return r;
-    GridDev gd;
+    std::vector<uint32_t> ord;
+    if (opts && opts->reorder_dims && d > 1) {
+        auto t0 = std::chrono::steady_clock::now();
+        std::vector<unsigned long long> costs;
+        if (int r = dim_order_by_cost(c, st, in.a, in.dtype_bytes, in.na, d, in.eps, ds, &ord, &costs)) return r;
+        ++launches;
+        P->reorder_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    Grid &g = P->g;
+    if (int r = plan_grid(hds, d, in.eps, maxabs, ord, &g)) return r;
+    GridDev &gd = P->gd;
+    if (!ord.empty()) {
+        gd.ord = (uint32_t *)slot_alloc_impl(c, st, kSlotGridOrd, d * 4);
+        if (!gd.ord) return fail(HJ_ERR_OOM, "out of device memory");
+        cudaMemcpyAsync(gd.ord, g.ord.data(), d * 4, cudaMemcpyHostToDevice, st);
+    }
     gd.off = (long long *)slot_alloc_impl(c, st, kSlotGridOff, d * 8);
     gd.bits = (uint32_t *)slot_alloc_impl(c, st, kSlotGridBits, d * 4);
     gd.word = (uint32_t *)slot_alloc_impl(c, st, kSlotGridWord, d * 4);
@@ -375,7 +427,7 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
     }
 
     // 2. EGO sort + layouts
-    SortedSet A, B;
+    SortedSet &A = P->A, &B = P->B;
     if (int r = prepare_set(c, st, in.a, in.na, in.dtype_bytes, g, gd, center, norm_scale, form, false, &A,
                             &launches))
         return r;
@@ -396,7 +448,7 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
     const bool tc = form_is_tc(form);
     const int tile_a = tc ? kTcTileA : kPlainTile, tile_b = tc ? kTcTileB : kPlainTile;
     const uint32_t chunk = tc ? 32 : 16;
-    IndexResult idx;
+    IndexResult &idx = P->idx;
     AllocCtx actx{c, st};
     std::string err;
     int r = build_index(A, B, g, gd, in.self, na_eff, nb_eff, tile_a, tile_b, active_dims, chunk, slot_alloc_cb,
@@ -415,6 +467,32 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
         idx = sh;
     }
     cudaEventRecord(c->ev[3], st);
+    P->form = form;
+    P->active_dims = active_dims;
+    P->maxabs = maxabs;
+    P->na_eff = na_eff;
+    P->nb_eff = nb_eff;
+    P->launches = launches;
+    return HJ_OK;
+}
+
+static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *count, hj_stats *stats,
+                    cudaEvent_t ev_h2d_start) {
+    cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
+    auto t_wall0 = std::chrono::steady_clock::now();
+    cudaEventRecord(c->ev[1], st);  // after H2D
+    Prepared P;
+    if (int r = prepare_join(c, st, in, opts, -1, &P)) return r;
+    int form = P.form;
+    const int active_dims = P.active_dims;
+    const double maxabs = P.maxabs;
+    const uint32_t d = in.d;
+    SortedSet &A = P.A, &B = P.B;
+    IndexResult &idx = P.idx;
+    const uint64_t na_eff = P.na_eff, nb_eff = P.nb_eff;
+    int launches = P.launches;
+    const bool tc = form_is_tc(form);
+    AllocCtx actx{c, st};
 
     // 4. distance kernels. d_small: [2] count of the tensor-core kernel and the
     // recheck, [3] error word, [4] band pairs, [5] max band error bits,
@@ -535,9 +613,111 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
         }
         stats->form_used = form;
         stats->fp64_items = fp_items;
+        stats->reorder_ms = P.reorder_ms;
         int s = active_dims;
         int p3 = 1;
         for (int i = 0; i < s; ++i) p3 *= 3;
+        stats->stripes = in.self ? (p3 + 1) / 2 : p3;
+        stats->kernel_launches = launches;
+    }
+    return HJ_OK;
+}
+
+// ------------------------------------------------------------ pair output
+
+__global__ void k_pairs_gather(const uint32_t *__restrict__ pi, const uint32_t *__restrict__ pj,
+                               const uint32_t *__restrict__ perm, uint64_t n, unsigned long long *__restrict__ out) {
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const uint32_t s = perm[r];
+    out[2 * r] = pi[s];
+    out[2 * r + 1] = pj[s];
+}
+
+// Pair materialisation: the join on the plain FP64 kernel run twice, once
+// counting the pairs of every work item, once writing them at the exclusive
+// scan of those counts, then a stable radix sort by (i, j) so that the output
+// is the same on every run. Nothing is written to `pairs` unless all of them
+// fit; *n_pairs is always the exact total.
+static int run_pairs(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *pairs, uint64_t capacity,
+                     uint64_t *n_pairs, hj_stats *stats, cudaEvent_t ev_h2d_start) {
+    cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
+    auto t_wall0 = std::chrono::steady_clock::now();
+    cudaEventRecord(c->ev[1], st);
+    Prepared P;
+    if (int r = prepare_join(c, st, in, opts, HJ_FORM_PLAIN_FP64, &P)) return r;
+    SortedSet &A = P.A, &B = P.B;
+    IndexResult &idx = P.idx;
+    int launches = P.launches;
+    const double T = in.eps * in.eps;
+    uint32_t *d_err = reinterpret_cast<uint32_t *>(c->d_small + 3);
+    cudaMemsetAsync(c->d_small + 2, 0, 5 * sizeof(unsigned long long), st);
+    const uint64_t n_items = idx.n_items;
+    uint32_t *item_cnt = (uint32_t *)slot_alloc_impl(c, st, kSlotItemCnt, (n_items + 1) * 4);
+    if (!item_cnt) return fail(HJ_ERR_OOM, "out of device memory");
+    cudaMemsetAsync(item_cnt, 0, (n_items + 1) * 4, st);
+    cudaEventRecord(c->ev[6], st);
+    launch_pairs_fp64(A, B, in.self, P.na_eff, P.nb_eff, T, idx, item_cnt, nullptr, nullptr, d_err, c->num_sms, st);
+    launch_scan_u32(item_cnt, n_items, c->d_small + 2, st);
+    launches += 2;
+    cudaMemcpyAsync(c->h_small + 2, c->d_small + 2, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("pair count");
+    if (int rr = check_cuda("pair count")) return rr;
+    if ((uint32_t)c->h_small[3] & kErrTimeout) return fail(HJ_ERR_TIMEOUT, "a bounded device-side wait timed out");
+    if ((uint32_t)c->h_small[3]) return fail(HJ_ERR_CUDA, "device error word set");
+    const uint64_t total = c->h_small[2];
+    *n_pairs = total;
+    if (total > capacity)
+        return fail(HJ_ERR_CAPACITY, "the pairs do not fit into the caller's buffer; *n_pairs holds their number");
+    if (total >= (1ull << 32)) return fail(HJ_ERR_UNSUPPORTED, "more than 2^32 - 1 pairs");
+    if (total) {
+        // keys word-major: word 0 = i (most significant), word 1 = j
+        uint32_t *keys = (uint32_t *)slot_alloc_impl(c, st, kSlotPairKeys, total * 8);
+        uint32_t *perm = (uint32_t *)slot_alloc_impl(c, st, kSlotPairPerm, total * 4);
+        uint32_t *ptmp = (uint32_t *)slot_alloc_impl(c, st, kSlotPairTmp, total * 4);
+        uint32_t *hist = (uint32_t *)slot_alloc_impl(c, st, kSlotPairHist, radix_hist_entries(total) * 4);
+        unsigned long long *out = (unsigned long long *)slot_alloc_impl(c, st, kSlotPairOut, total * 16);
+        if (!keys || !perm || !ptmp || !hist || !out) return fail(HJ_ERR_OOM, "out of device memory (pairs)");
+        launch_pairs_fp64(A, B, in.self, P.na_eff, P.nb_eff, T, idx, item_cnt, keys, keys + total, d_err,
+                          c->num_sms, st);
+        ++launches;
+        std::vector<std::pair<uint32_t, uint32_t>> passes;
+        const int bj = bitwidth(in.nb ? in.nb - 1 : 0), bi = bitwidth(in.na ? in.na - 1 : 0);
+        for (int b = 0; b < bj; b += 8) passes.push_back({1u, (uint32_t)b});
+        for (int b = 0; b < bi; b += 8) passes.push_back({0u, (uint32_t)b});
+        radix_sort_perm(keys, total, passes, perm, ptmp, hist, st, &launches);
+        k_pairs_gather<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(keys, keys + total, perm, total, out);
+        ++launches;
+        cudaEventRecord(c->ev[4], st);
+        cudaMemcpyAsync(pairs, out, total * 16, cudaMemcpyDeviceToHost, st);
+    } else {
+        cudaEventRecord(c->ev[4], st);
+    }
+    cudaMemcpyAsync(c->h_small + 3, c->d_small + 3, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("pair output");
+    if (int rr = check_cuda("pair output")) return rr;
+    if ((uint32_t)c->h_small[3] & kErrTimeout) return fail(HJ_ERR_TIMEOUT, "a bounded device-side wait timed out");
+    if ((uint32_t)c->h_small[3]) return fail(HJ_ERR_CUDA, "device error word set");
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        if (ev_h2d_start) stats->h2d_ms = ev_ms(ev_h2d_start, c->ev[1]);
+        stats->sort_ms = ev_ms(c->ev[1], c->ev[2]);
+        stats->index_ms = ev_ms(c->ev[2], c->ev[3]);
+        stats->join_ms = ev_ms(c->ev[3], c->ev[4]);
+        stats->kernel_ms = ev_ms(c->ev[6], c->ev[4]);
+        stats->total_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_wall0).count() +
+            stats->h2d_ms;
+        const double all = in.self ? (double)P.na_eff * (double)(P.na_eff > 0 ? P.na_eff - 1 : 0) / 2.0
+                                   : (double)P.na_eff * (double)P.nb_eff;
+        stats->candidate_pairs = idx.candidate_pairs;
+        stats->tile_pairs = idx.tile_pairs;
+        stats->work_items = idx.n_items;
+        stats->loadpercent = all > 0 ? 100.0 * (double)idx.candidate_pairs / all : 0.0;
+        stats->form_used = HJ_FORM_PLAIN_FP64;
+        stats->reorder_ms = P.reorder_ms;
+        int p3 = 1;
+        for (int i = 0; i < P.active_dims; ++i) p3 *= 3;
         stats->stripes = in.self ? (p3 + 1) / 2 : p3;
         stats->kernel_launches = launches;
     }
@@ -592,6 +772,33 @@ static int join_device(const void *a, uint64_t na, const void *b, uint64_t nb, i
     return run_join(c, in, opts, count, stats, nullptr);
 }
 
+static int pairs_host(const void *a, uint64_t na, const void *b, uint64_t nb, int dtype_bytes, uint32_t d,
+                      double eps, bool self, const hj_opts *opts, uint64_t *pairs, uint64_t capacity,
+                      uint64_t *n_pairs, hj_stats *stats) {
+    tl_error.clear();
+    if (!n_pairs || (capacity && !pairs) || (na && !a) || (!self && nb && !b))
+        return fail(HJ_ERR_INVALID_ARG, "null pointer");
+    if (int r = validate(na, nb, d, eps)) return r;
+    if (d > 128) return fail(HJ_ERR_UNSUPPORTED, "pair output supports d <= 128 (plain FP64 form)");
+    Ctx *c;
+    if (int r = get_ctx(opts ? opts->device : -1, &c)) return r;
+    cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
+    *n_pairs = 0;
+    if (na == 0 || (!self && nb == 0)) {
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        return HJ_OK;
+    }
+    cudaEventRecord(c->ev[0], st);
+    void *da = slot_alloc_impl(c, st, kSlotInA, na * d * dtype_bytes);
+    void *db = self ? da : slot_alloc_impl(c, st, kSlotInB, nb * d * dtype_bytes);
+    if (!da || !db) return fail(HJ_ERR_OOM, "out of device memory");
+    cudaMemcpyAsync(da, a, na * d * dtype_bytes, cudaMemcpyHostToDevice, st);
+    if (!self) cudaMemcpyAsync(db, b, nb * d * dtype_bytes, cudaMemcpyHostToDevice, st);
+    if (int r = check_cuda("host to device copy")) return r;
+    JoinIn in{da, db, na, self ? na : nb, dtype_bytes, d, eps, self};
+    return run_pairs(c, in, opts, pairs, capacity, n_pairs, stats, c->ev[0]);
+}
+
 // Device EGO sort of one host set; perm (and sorted rows) copied back.
 static int ego_sort_host(const double *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts, uint64_t *perm,
                          double *sorted) {
@@ -618,7 +825,7 @@ static int ego_sort_host(const double *pts, uint64_t n, uint32_t d, double eps, 
     double maxabs;
     std::memcpy(&maxabs, &c->h_small[0], 8);
     Grid g;
-    if (int r = plan_grid(hds, d, eps, maxabs, &g)) return r;
+    if (int r = plan_grid(hds, d, eps, maxabs, {}, &g)) return r;
     GridDev gd;
     gd.off = (long long *)slot_alloc_impl(c, st, kSlotGridOff, d * 8);
     gd.bits = (uint32_t *)slot_alloc_impl(c, st, kSlotGridBits, d * 4);
@@ -649,6 +856,40 @@ static int ego_sort_host(const double *pts, uint64_t n, uint32_t d, double eps, 
     if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("EGO sort");
     if (int r = check_cuda("EGO sort")) return r;
     for (uint64_t i = 0; i < n; ++i) perm[i] = hp[i];
+    return HJ_OK;
+}
+
+static int dim_order_host(const double *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts,
+                          int32_t *reorder_dim, uint64_t *costs_out) {
+    tl_error.clear();
+    if (!reorder_dim || (n && !pts)) return fail(HJ_ERR_INVALID_ARG, "null pointer");
+    if (int r = validate(n, n, d, eps)) return r;
+    Ctx *c;
+    if (int r = get_ctx(opts ? opts->device : -1, &c)) return r;
+    if (n == 0) {
+        for (uint32_t t = 0; t < d; ++t) reorder_dim[t] = (int32_t)t;
+        if (costs_out)
+            for (uint32_t t = 0; t < d; ++t) costs_out[t] = 0;
+        return HJ_OK;
+    }
+    cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;
+    void *dx = slot_alloc_impl(c, st, kSlotInA, n * d * 8);
+    DimStats *ds = (DimStats *)slot_alloc_impl(c, st, kSlotDimStats, d * sizeof(DimStats));
+    if (!dx || !ds) return fail(HJ_ERR_OOM, "out of device memory");
+    cudaMemcpyAsync(dx, pts, n * d * 8, cudaMemcpyHostToDevice, st);
+    unsigned long long *d_maxabs = c->d_small + 0;
+    uint32_t *d_bad = reinterpret_cast<uint32_t *>(c->d_small + 1);
+    launch_dim_stats_init(ds, d, d_maxabs, d_bad, st);
+    launch_dim_stats(dx, 8, n, d, eps, ds, d_maxabs, d_bad, st);
+    cudaMemcpyAsync(c->h_small, c->d_small, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("cell statistics");
+    if ((uint32_t)c->h_small[1]) return fail(HJ_ERR_INVALID_ARG, "non-finite coordinate or cell out of range");
+    std::vector<uint32_t> ord;
+    std::vector<unsigned long long> costs;
+    if (int r = dim_order_by_cost(c, st, dx, 8, n, d, eps, ds, &ord, &costs)) return r;
+    for (uint32_t pos = 0; pos < d; ++pos) reorder_dim[ord[pos]] = (int32_t)pos;
+    if (costs_out)
+        for (uint32_t t = 0; t < d; ++t) costs_out[t] = costs[t];
     return HJ_OK;
 }
 
@@ -687,6 +928,7 @@ const char *hj_status_str(int s) {
         case HJ_ERR_UNSUPPORTED: return "unsupported input for this form";
         case HJ_ERR_BUSY: return "rejected by admission";
         case HJ_ERR_NOT_FOUND: return "not found";
+        case HJ_ERR_CAPACITY: return "output buffer too small";
         default: return "unknown status";
     }
 }
@@ -726,6 +968,31 @@ int hj_join_count(const double *A, uint64_t nA, const double *B, uint64_t nB, ui
 int hj_join_count_f32(const float *A, uint64_t nA, const float *B, uint64_t nB, uint32_t d, double eps,
                       const hj_opts *opts, uint64_t *count, hj_stats *stats) {
     return join_host(A, nA, B, nB, 4, d, eps, false, opts, count, stats);
+}
+
+int hj_self_join_pairs(const double *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts, uint64_t *pairs,
+                       uint64_t capacity, uint64_t *n_pairs, hj_stats *stats) {
+    return pairs_host(pts, n, pts, n, 8, d, eps, true, opts, pairs, capacity, n_pairs, stats);
+}
+
+int hj_self_join_pairs_f32(const float *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts,
+                           uint64_t *pairs, uint64_t capacity, uint64_t *n_pairs, hj_stats *stats) {
+    return pairs_host(pts, n, pts, n, 4, d, eps, true, opts, pairs, capacity, n_pairs, stats);
+}
+
+int hj_join_pairs(const double *A, uint64_t nA, const double *B, uint64_t nB, uint32_t d, double eps,
+                  const hj_opts *opts, uint64_t *pairs, uint64_t capacity, uint64_t *n_pairs, hj_stats *stats) {
+    return pairs_host(A, nA, B, nB, 8, d, eps, false, opts, pairs, capacity, n_pairs, stats);
+}
+
+int hj_join_pairs_f32(const float *A, uint64_t nA, const float *B, uint64_t nB, uint32_t d, double eps,
+                      const hj_opts *opts, uint64_t *pairs, uint64_t capacity, uint64_t *n_pairs, hj_stats *stats) {
+    return pairs_host(A, nA, B, nB, 4, d, eps, false, opts, pairs, capacity, n_pairs, stats);
+}
+
+int hj_dim_order(const double *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts, int32_t *reorder_dim,
+                 uint64_t *costs) {
+    return dim_order_host(pts, n, d, eps, opts, reorder_dim, costs);
 }
 
 int hj_ego_sort(const double *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts, uint64_t *perm,

@@ -64,20 +64,22 @@ __device__ __forceinline__ uint32_t digit_of(const BoundsArgs &a, double cell, u
 __device__ __forceinline__ double cell_lo(const BoundsArgs &a, double x) { return floor((x - a.epsw) / a.eps); }
 __device__ __forceinline__ double cell_hi(const BoundsArgs &a, double x) { return floor((x + a.epsw) / a.eps); }
 
-// -1, 0, 1: lexicographic comparison of the lo-vectors of rows p and q.
+// -1, 0, 1: lexicographic comparison (in key order) of the lo-vectors of rows p and q.
 __device__ int cmp_lo(const BoundsArgs &a, uint64_t p, uint64_t q) {
-    for (uint32_t t = 0; t < a.d; ++t) {
+    for (uint32_t pos = 0; pos < a.d; ++pos) {
+        const uint32_t t = grid_dim_at(a.g, pos);
         double cp = cell_lo(a, crd(a, p, t)), cq = cell_lo(a, crd(a, q, t));
         if (cp != cq) return cp < cq ? -1 : 1;
     }
     return 0;
 }
-// Same for the upper vectors (lo cells in dims < k, hi cells from dim k on).
+// Same for the upper vectors (lo cells at key positions < k, hi cells from k on).
 __device__ int cmp_up(const BoundsArgs &a, uint64_t p, uint64_t q, int k) {
-    for (uint32_t t = 0; t < a.d; ++t) {
+    for (uint32_t pos = 0; pos < a.d; ++pos) {
+        const uint32_t t = grid_dim_at(a.g, pos);
         double xp = crd(a, p, t), xq = crd(a, q, t);
-        double cp = (int)t < k ? cell_lo(a, xp) : cell_hi(a, xp);
-        double cq = (int)t < k ? cell_lo(a, xq) : cell_hi(a, xq);
+        double cp = (int)pos < k ? cell_lo(a, xp) : cell_hi(a, xp);
+        double cq = (int)pos < k ? cell_lo(a, xq) : cell_hi(a, xq);
         if (cp != cq) return cp < cq ? -1 : 1;
     }
     return 0;
@@ -131,7 +133,7 @@ __global__ void __launch_bounds__(kBoundsWarps * 32) k_tile_bounds(BoundsArgs a,
     for (uint64_t p = p0 + lane; p < p1; p += 32) {
         int ke = 0;
         while (ke < kt) {
-            double x = crd(a, p, ke);
+            double x = crd(a, p, grid_dim_at(a.g, ke));
             if (cell_hi(a, x) - cell_lo(a, x) > 2.0) break;
             ++ke;
         }
@@ -160,10 +162,11 @@ __global__ void __launch_bounds__(kBoundsWarps * 32) k_tile_bounds(BoundsArgs a,
         qhi[w] = 0;
     }
     __syncwarp();
-    for (uint32_t t = lane; t < a.d; t += 32) {
+    for (uint32_t pos = lane; pos < a.d; pos += 32) {
+        const uint32_t t = grid_dim_at(a.g, pos);
         double xl = crd(a, pmin, t), xu = crd(a, pmax, t);
         uint32_t dl = digit_of(a, cell_lo(a, xl), t);
-        uint32_t du = digit_of(a, (int)t < kt ? cell_lo(a, xu) : cell_hi(a, xu), t);
+        uint32_t du = digit_of(a, (int)pos < kt ? cell_lo(a, xu) : cell_hi(a, xu), t);
         atomicOr(&qlo[a.g.word[t]], dl << a.g.shift[t]);
         atomicOr(&qhi[a.g.word[t]], du << a.g.shift[t]);
     }
@@ -171,7 +174,7 @@ __global__ void __launch_bounds__(kBoundsWarps * 32) k_tile_bounds(BoundsArgs a,
     // 4. one pair of searches per combination of the first kt dims
     int ncomb = 1;
     for (int t = 0; t < kt; ++t) ncomb *= 3;
-    const int np = kt > 0 ? (int)a.g.word[kt - 1] + 1 : 0;  // words holding active dims
+    const int np = kt > 0 ? (int)a.g.word[grid_dim_at(a.g, kt - 1)] + 1 : 0;  // words holding active dims
     for (int c = lane; c < ncomb; c += 32) {
         uint32_t pl[kMaxActiveDims], ph[kMaxActiveDims];
         for (int w = 0; w < np; ++w) {
@@ -179,7 +182,8 @@ __global__ void __launch_bounds__(kBoundsWarps * 32) k_tile_bounds(BoundsArgs a,
             ph[w] = qhi[w];
         }
         int rem = c;
-        for (int t = kt - 1; t >= 0; --t) {
+        for (int pos = kt - 1; pos >= 0; --pos) {
+            const uint32_t t = grid_dim_at(a.g, (uint32_t)pos);
             uint32_t delta = (uint32_t)(rem % 3);
             rem /= 3;
             uint32_t w = a.g.word[t], sh = a.g.shift[t];

@@ -57,13 +57,26 @@ struct Grid {
     std::vector<long long> range;      // max cell - min cell per dim
     // radix passes: (word, low bit) of each 8-bit digit window that can vary
     std::vector<std::pair<uint32_t, uint32_t>> passes;
+    // key position -> dim: fields are packed, and stripes take their active
+    // dims, in this order (identity unless the dims are reordered)
+    std::vector<uint32_t> ord;
 };
 
-// Device copy of the grid's per-dim packing tables.
+// Device copy of the grid's per-dim packing tables (indexed by dim) and of the
+// position order (nullptr = identity).
 struct GridDev {
     long long *off = nullptr;
     uint32_t *bits = nullptr, *word = nullptr, *shift = nullptr;
+    uint32_t *ord = nullptr;
 };
+__host__ __device__ inline uint32_t grid_dim_at(const GridDev &g, uint32_t pos) { return g.ord ? g.ord[pos] : pos; }
+
+// Dimension cost for reordering: per dim, the number of unordered pairs of a
+// fixed sample (min(n, kCostSample) points at floor(s n / S)) whose cells are
+// equal or adjacent. One block per dim; cost[d] zeroed by the kernel.
+constexpr uint32_t kCostSample = 8192;
+void launch_dim_cost(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, const DimStats *ds,
+                     unsigned long long *cost, cudaStream_t st);
 
 // A point set after EGO sorting, in every layout the kernels need. Rows are
 // in EGO rank order; `perm[r]` is the input index of rank r.
@@ -179,6 +192,15 @@ int build_index(const SortedSet &A, const SortedSet &B, const Grid &grid, const 
 void launch_join_fp64(const SortedSet &A, const SortedSet &B, bool self, uint64_t na_eff, uint64_t nb_eff,
                       double T, const IndexResult &idx, unsigned long long *d_count, uint32_t *d_err,
                       int num_sms, cudaStream_t st);
+
+// Pair materialisation on the FP64 kernel. out_i == nullptr: adds each item's
+// pair count into item_cnt[item] (zeroed by the caller). Otherwise item_cnt
+// holds each item's first output slot (exclusive scan of the counts) and the
+// kernel writes the pairs of input indices there (self joins as i < j), in no
+// particular order within an item.
+void launch_pairs_fp64(const SortedSet &A, const SortedSet &B, bool self, uint64_t na_eff, uint64_t nb_eff,
+                       double T, const IndexResult &idx, uint32_t *item_cnt, uint32_t *out_i, uint32_t *out_j,
+                       uint32_t *d_err, int num_sms, cudaStream_t st);
 
 // Tensor-core kernel + FP64 recheck of the band. Adds into *d_count; band pair
 // count into *d_band_total (may exceed `band_cap`: then the caller regrows).

@@ -17,6 +17,14 @@
 // 512 pairs all exceed eps^2 after some dims stops early (checked every 8
 // dims) without changing any decision. Counts are reduced by warp shuffles and
 // one 64-bit atomic per warp.
+//
+// The same kernel materialises the pairs (hj_self_join_pairs / hj_join_pairs)
+// in two more modes: kModeItemCounts adds each warp's count of an item into
+// item_cnt[item] (one 32-bit atomic per warp and item), and after an exclusive
+// scan of those counts kModeEmit writes every qualifying pair as (input index
+// of the A point, input index of the B point) at item_cnt[item] (now the
+// item's cursor), reserving each warp's block of slots per B tile with one
+// atomic and placing the lanes by a warp prefix sum.
 #include "hj_common.cuh"
 #include "hj_internal.h"
 
@@ -32,7 +40,13 @@ struct PlainArgs {
     int self;
     unsigned long long *count;
     uint32_t *err;
+    // pair modes
+    uint32_t *item_cnt;                 // per item: count (kModeItemCounts) / cursor (kModeEmit)
+    const uint32_t *perm_a, *perm_b;    // EGO rank -> input index
+    uint32_t *out_i, *out_j;            // emitted pairs
 };
+
+enum PlainMode { kModeCount = 0, kModeItemCounts = 1, kModeEmit = 2 };
 
 constexpr int kPlainThreads = 256;
 constexpr int kPlainWarps = kPlainThreads / 32;
@@ -46,6 +60,7 @@ __device__ __forceinline__ void drain_wait(uint64_t *bar, uint32_t parity) {
     }
 }
 
+template <int MODE>
 __global__ void __launch_bounds__(kPlainThreads, 2) k_join_fp64(PlainArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar_a, bar_full[2], bar_empty[2];
@@ -170,32 +185,81 @@ __global__ void __launch_bounds__(kPlainThreads, 2) k_join_fp64(PlainArgs a) {
                 }
             }
             const uint64_t jb0 = (uint64_t)bt * kPlainTile + tx * 4;
+            uint32_t hits = 0;  // bit 4i+j: pair (i, j) of this thread's block qualifies
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const uint64_t pi = ia0 + i, pj = jb0 + j;
                     const bool valid = pi < a.na && pj < a.nb && (!a.self || pj > pi);
-                    cnt += (valid && acc[i][j] <= T) ? 1ull : 0ull;
+                    hits |= (valid && acc[i][j] <= T) ? 1u << (4 * i + j) : 0u;
                 }
             __syncwarp();
             if (lane == 0) mbar_arrive(&bar_empty[s]);
             ++consumed;
+            const uint32_t nh = __popc(hits);
+            if (MODE != kModeEmit) {
+                cnt += nh;
+            } else if (__any_sync(0xffffffffu, nh != 0)) {
+                uint32_t incl = nh;  // inclusive warp prefix sum of the hit counts
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= (uint32_t)o) incl += v;
+                }
+                const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(a.item_cnt + it, total);
+                base = __shfl_sync(0xffffffffu, base, 0) + incl - nh;
+                while (hits) {
+                    const int b = __ffs(hits) - 1;
+                    hits &= hits - 1;
+                    const uint32_t ri = (uint32_t)(ia0 + (b >> 2)), rj = (uint32_t)(jb0 + (b & 3));
+                    uint32_t gi = a.perm_a[ri], gj = a.perm_b[rj];
+                    if (a.self && gi > gj) {
+                        const uint32_t t = gi;
+                        gi = gj;
+                        gj = t;
+                    }
+                    a.out_i[base] = gi;
+                    a.out_j[base] = gj;
+                    ++base;
+                }
+            }
+        }
+        if (MODE == kModeItemCounts) {
+            const unsigned long long wc = warp_sum_u64(cnt);
+            if (lane == 0 && wc) atomicAdd(a.item_cnt + it, (uint32_t)wc);
+            cnt = 0;
         }
     }
-    cnt = warp_sum_u64(cnt);
-    if (lane == 0 && cnt) atomicAdd(a.count, cnt);
+    if (MODE == kModeCount) {
+        cnt = warp_sum_u64(cnt);
+        if (lane == 0 && cnt) atomicAdd(a.count, cnt);
+    }
     // Every issued copy has been consumed unless a wait gave up; then drain.
     if (tid == 0 && *err != 0) {
         for (uint32_t j = consumed; j < issued; ++j) drain_wait(&bar_full[j & 1u], (j >> 1) & 1u);
     }
 }
 
-void launch_join_fp64(const SortedSet &A, const SortedSet &B, bool self, uint64_t na_eff, uint64_t nb_eff,
-                      double T, const IndexResult &idx, unsigned long long *d_count, uint32_t *d_err, int num_sms,
-                      cudaStream_t st) {
-    if (idx.n_items == 0) return;
+template <int MODE>
+static void launch_plain(const PlainArgs &a, uint64_t n_items, int num_sms, cudaStream_t st) {
+    const size_t smem = (size_t)3 * a.d * kPlainTile * sizeof(double);
+    // the largest this kernel ever needs (d <= 128), set once
+    ensure_max_dynamic_smem((const void *)k_join_fp64<MODE>, 3 * 128 * kPlainTile * (int)sizeof(double));
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_join_fp64<MODE>, kPlainThreads, smem);
+    if (per_sm < 1) per_sm = 1;
+    uint64_t grid = (uint64_t)per_sm * num_sms;
+    if (grid > n_items) grid = n_items;
+    k_join_fp64<MODE><<<(unsigned)grid, kPlainThreads, smem, st>>>(a);
+}
+
+static PlainArgs plain_args(const SortedSet &A, const SortedSet &B, bool self, uint64_t na_eff, uint64_t nb_eff,
+                            double T, const IndexResult &idx, uint32_t *d_err) {
     PlainArgs a;
+    memset(&a, 0, sizeof(a));
     a.A = A.tiles64;
     a.B = B.tiles64;
     a.d = A.d;
@@ -205,17 +269,33 @@ void launch_join_fp64(const SortedSet &A, const SortedSet &B, bool self, uint64_
     a.na = na_eff;
     a.nb = nb_eff;
     a.self = self ? 1 : 0;
-    a.count = d_count;
     a.err = d_err;
-    const size_t smem = (size_t)3 * A.d * kPlainTile * sizeof(double);
-    // the largest this kernel ever needs (d <= 128), set once
-    ensure_max_dynamic_smem((const void *)k_join_fp64, 3 * 128 * kPlainTile * (int)sizeof(double));
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_join_fp64, kPlainThreads, smem);
-    if (per_sm < 1) per_sm = 1;
-    uint64_t grid = (uint64_t)per_sm * num_sms;
-    if (grid > idx.n_items) grid = idx.n_items;
-    k_join_fp64<<<(unsigned)grid, kPlainThreads, smem, st>>>(a);
+    return a;
+}
+
+void launch_join_fp64(const SortedSet &A, const SortedSet &B, bool self, uint64_t na_eff, uint64_t nb_eff,
+                      double T, const IndexResult &idx, unsigned long long *d_count, uint32_t *d_err, int num_sms,
+                      cudaStream_t st) {
+    if (idx.n_items == 0) return;
+    PlainArgs a = plain_args(A, B, self, na_eff, nb_eff, T, idx, d_err);
+    a.count = d_count;
+    launch_plain<kModeCount>(a, idx.n_items, num_sms, st);
+}
+
+void launch_pairs_fp64(const SortedSet &A, const SortedSet &B, bool self, uint64_t na_eff, uint64_t nb_eff,
+                       double T, const IndexResult &idx, uint32_t *item_cnt, uint32_t *out_i, uint32_t *out_j,
+                       uint32_t *d_err, int num_sms, cudaStream_t st) {
+    if (idx.n_items == 0) return;
+    PlainArgs a = plain_args(A, B, self, na_eff, nb_eff, T, idx, d_err);
+    a.item_cnt = item_cnt;
+    a.perm_a = A.perm;
+    a.perm_b = B.perm;
+    a.out_i = out_i;
+    a.out_j = out_j;
+    if (out_i)
+        launch_plain<kModeEmit>(a, idx.n_items, num_sms, st);
+    else
+        launch_plain<kModeItemCounts>(a, idx.n_items, num_sms, st);
 }
 
 }  // namespace hj

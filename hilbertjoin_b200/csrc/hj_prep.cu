@@ -118,7 +118,8 @@ __global__ void k_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t cur_word = 0, acc = 0;
-    for (uint32_t t = 0; t < d; ++t) {
+    for (uint32_t pos = 0; pos < d; ++pos) {  // fields in key order: words never decrease
+        const uint32_t t = grid_dim_at(g, pos);
         uint32_t w = g.word[t];
         if (w != cur_word) {
             keys_wm[(uint64_t)cur_word * n + i] = acc;
@@ -151,6 +152,71 @@ void launch_norm_key(const void *x, int dtype_bytes, uint64_t n, uint32_t d, con
                      uint32_t *key_out, cudaStream_t st) {
     if (n == 0) return;
     k_norm_key<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(x, dtype_bytes, n, d, center, scale, key_out);
+}
+
+// Dimension cost (the selectivity estimate of the reference's
+// outputStatistics, hilbertjoin/egojoin.cpp:523-592): the sample's cell
+// indices of one dim are sorted in shared memory (bitonic), and every sample
+// position s counts the positions q > s with cell[q] <= cell[s] + 1 by a
+// binary search -- together the pairs in equal cells, sum h(h-1)/2, plus the
+// pairs in adjacent cells, sum h[c-1] h[c].
+__global__ void __launch_bounds__(1024) k_dim_cost(const void *x, int dtype_bytes, uint64_t n, uint32_t d,
+                                                   double eps, const DimStats *__restrict__ ds,
+                                                   unsigned long long *cost) {
+    __shared__ uint32_t v[kCostSample];
+    __shared__ unsigned long long total;
+    const uint32_t t = blockIdx.x, tid = threadIdx.x;
+    const uint32_t S = (uint32_t)(n < kCostSample ? n : kCostSample);
+    const long long cmin = ds[t].cmin;
+    if (tid == 0) total = 0;
+    for (uint32_t s = tid; s < kCostSample; s += blockDim.x) {
+        uint32_t c = 0xffffffffu;  // padding sorts last
+        if (s < S) {
+            const uint64_t i = (uint64_t)s * n / S;
+            long long q = (long long)floor(coord(x, dtype_bytes, i * d + t) / eps) - cmin;
+            q = q < 0 ? 0 : (q > 0x7fffffffll ? 0x7fffffffll : q);
+            c = (uint32_t)q;
+        }
+        v[s] = c;
+    }
+    __syncthreads();
+    for (uint32_t k = 2; k <= kCostSample; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = tid; i < kCostSample; i += blockDim.x) {
+                const uint32_t p = i ^ j;
+                if (p > i) {
+                    const uint32_t a = v[i], b = v[p];
+                    if ((a > b) == ((i & k) == 0)) {
+                        v[i] = b;
+                        v[p] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    unsigned long long mine = 0;
+    for (uint32_t s = tid; s < S; s += blockDim.x) {
+        const uint32_t lim = v[s] + 1;  // cells are below 2^31: no wrap
+        uint32_t lo = s + 1, hi = S;    // first q in (s, S) with v[q] > lim
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (v[mid] <= lim)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        mine += lo - s - 1;
+    }
+    mine = warp_sum_u64(mine);
+    if ((tid & 31u) == 0 && mine) atomicAdd(&total, mine);
+    __syncthreads();
+    if (tid == 0) cost[t] = total;
+}
+
+void launch_dim_cost(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, const DimStats *ds,
+                     unsigned long long *cost, cudaStream_t st) {
+    k_dim_cost<<<d, 1024, 0, st>>>(x, dtype_bytes, n, d, eps, ds, cost);
 }
 
 void launch_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, const GridDev &g,

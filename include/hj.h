@@ -49,7 +49,8 @@ typedef enum {
     HJ_ERR_NO_DEVICE = 6,     /* no usable sm_100 device */
     HJ_ERR_UNSUPPORTED = 7,   /* the requested form cannot run this input (see hj_opts.form) */
     HJ_ERR_BUSY = 8,          /* serving: request rejected by admission (memory budget) */
-    HJ_ERR_NOT_FOUND = 9      /* serving: unknown handle or request id */
+    HJ_ERR_NOT_FOUND = 9,     /* serving: unknown handle or request id */
+    HJ_ERR_CAPACITY = 10      /* pair output: more pairs than the caller's capacity (*n_pairs = the total) */
 } hj_status;
 
 /* How pair distances are evaluated. Every form returns the exact count of the
@@ -85,7 +86,14 @@ typedef struct {
     int32_t shard_count;   /* work list (contiguous, equal-load ranges of the Hilbert-ordered block
                               pairs, the reference's equal-load split egojoin.h:214-222). The counts
                               of shards 0..shard_count-1 sum to the full count. */
-    uint64_t reserved[3];
+    int32_t reorder_dims;  /* nonzero: order the dims of the cell key (EGO order, stripes)
+                              by ascending cost, most selective first, as hj_dim_order
+                              computes it from set A (the reference's join driver does this
+                              before every join, mainJoin.cpp:97-100). Distances are still
+                              summed in the caller's dim order, so the count is unchanged;
+                              only the work (candidate pairs) changes. */
+    int32_t reserved_i;
+    uint64_t reserved[2];
 } hj_opts;
 
 /* Per-call statistics (all optional). Times are device times of each stage
@@ -113,7 +121,8 @@ typedef struct {
     int32_t stripes;        /* stripe count (3^s+1)/2 for self-joins, 3^s for two-set joins */
     int32_t kernel_launches;/* kernels this call launched */
     int32_t reserved_i;
-    uint64_t reserved[4];
+    double reorder_ms;      /* dimension cost sampling and ordering (opts.reorder_dims) */
+    uint64_t reserved[3];
 } hj_stats;
 
 HJ_API void hj_opts_init(hj_opts *o);
@@ -139,6 +148,29 @@ HJ_API int hj_join_count(const double *A, uint64_t nA, const double *B, uint64_t
                   const hj_opts *opts, uint64_t *count, hj_stats *stats);
 HJ_API int hj_join_count_f32(const float *A, uint64_t nA, const float *B, uint64_t nB, uint32_t d, double eps,
                       const hj_opts *opts, uint64_t *count, hj_stats *stats);
+
+/* The qualifying pairs themselves. pairs[2k], pairs[2k+1] are the input
+ * indices (i, j) of pair k -- the layout of the reference's
+ * struct join_pair { size_t p1, p2; } (hilbertjoin/egojoin.h:32-35), whose
+ * queue output (hilbertjoin/test_ego_loop3_queue.cpp:19-37) the reference
+ * compiles out under COUNT_ONLY. Self joins list each unordered pair once with
+ * i < j; two-set joins list (index in A, index in B). Sorted by (i, j).
+ * The reference pushes indices into its EGO-sorted array; these are indices
+ * into the caller's unsorted input. Always computed by the plain FP64 form
+ * (d <= 128; opts->form is ignored), so the pairs are exactly the ones the
+ * count functions count. If more than `capacity` pairs qualify nothing is
+ * written, *n_pairs is set to the number and HJ_ERR_CAPACITY is returned
+ * (capacity 0 with pairs NULL asks for the number alone). */
+HJ_API int hj_self_join_pairs(const double *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts,
+                              uint64_t *pairs, uint64_t capacity, uint64_t *n_pairs, hj_stats *stats);
+HJ_API int hj_self_join_pairs_f32(const float *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts,
+                                  uint64_t *pairs, uint64_t capacity, uint64_t *n_pairs, hj_stats *stats);
+HJ_API int hj_join_pairs(const double *A, uint64_t nA, const double *B, uint64_t nB, uint32_t d, double eps,
+                         const hj_opts *opts, uint64_t *pairs, uint64_t capacity, uint64_t *n_pairs,
+                         hj_stats *stats);
+HJ_API int hj_join_pairs_f32(const float *A, uint64_t nA, const float *B, uint64_t nB, uint32_t d, double eps,
+                             const hj_opts *opts, uint64_t *pairs, uint64_t capacity, uint64_t *n_pairs,
+                             hj_stats *stats);
 
 /* Epsilon-grid order of a point set computed on the device: perm[r] is the
  * input index of the point at rank r, ranks ordered lexicographically by the
@@ -166,6 +198,20 @@ HJ_API int hj_ego_sort(const double *pts, uint64_t n, uint32_t d, double eps, co
  * This entry point has no counterpart in the reference. */
 HJ_API int hj_ego_sort_device_noalloc(const void *pts, int dtype_bytes, uint64_t n, uint32_t d, double eps,
                                       uint32_t *perm, void *stream);
+
+/* Dimension order for the cell key, computed on the device. Per dim j the
+ * cost is the number of unordered pairs of sampled points whose cells in dim j
+ * are equal or adjacent -- sum h(h-1)/2 + sum h[c-1] h[c] over the sample's
+ * cell histogram, the Super-EGO selectivity estimate the reference computes
+ * in outputStatistics (hilbertjoin/egojoin.cpp:523-592). Dims are ranked by
+ * ascending cost, ties by dim index, and reorder_dim[j] receives the new
+ * position of dim j (the reference's convention, egojoin.cpp:587-589). Unlike
+ * the reference, the sample is deterministic -- the min(n, 8192) points
+ * floor(s n / S), s = 0..S-1 -- and every dim is ranked (the reference leaves
+ * dims with cells beyond +-100000 uncosted). costs (optional) receives the d
+ * costs. pts: host FP64 rows. */
+HJ_API int hj_dim_order(const double *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts,
+                        int32_t *reorder_dim, uint64_t *costs);
 
 /* The same calls on inputs already in device memory (row-major, d per row).
  * `dtype_bytes` is 8 (FP64) or 4 (FP32). The pointers must be device (or

@@ -58,6 +58,12 @@ def lib():
         L.hjo_join_count_brute.argtypes = [P, U64, P, U64, U32, D, I]
         L.hjo_self_row_counts.restype = None
         L.hjo_self_row_counts.argtypes = [P, U64, U32, D, P, U64, P, I]
+        L.hjo_self_pairs_brute.restype = U64
+        L.hjo_self_pairs_brute.argtypes = [P, U64, U32, D, P, U64, I]
+        L.hjo_join_pairs_brute.restype = U64
+        L.hjo_join_pairs_brute.argtypes = [P, U64, P, U64, U32, D, P, U64, I]
+        L.hjo_dim_costs.restype = None
+        L.hjo_dim_costs.argtypes = [P, U64, U32, D, P]
         L.hjo_cells.restype = None
         L.hjo_cells.argtypes = [P, U64, U32, D, P]
         L.hjo_ego_order.restype = None
@@ -99,6 +105,50 @@ def self_row_counts(x, eps: float, rows, threads: int = 0) -> np.ndarray:
     out = np.zeros(rows.shape[0], dtype=np.uint64)
     lib().hjo_self_row_counts(_ptr(x), x.shape[0], x.shape[1], eps, _ptr(rows), rows.shape[0], _ptr(out), threads)
     return out
+
+
+def _pairs(call, cap_hint: int) -> np.ndarray:
+    cap = max(int(cap_hint), 1)
+    for _ in range(2):
+        out = np.empty((cap, 2), dtype=np.uint64)
+        total = int(call(out, cap))
+        if total <= cap:
+            return out[:total]
+        cap = total
+    raise RuntimeError("pair list changed size between passes")
+
+
+def self_pairs_brute(x, eps: float, threads: int = 0, cap_hint: int = 1 << 16) -> np.ndarray:
+    """(k, 2) uint64 pairs (i, j), i < j, with dist2 <= eps^2, sorted by (i, j)."""
+    x = _f64(x)
+    return _pairs(lambda out, cap: lib().hjo_self_pairs_brute(_ptr(x), x.shape[0], x.shape[1], eps, _ptr(out), cap,
+                                                              threads), cap_hint)
+
+
+def join_pairs_brute(a, b, eps: float, threads: int = 0, cap_hint: int = 1 << 16) -> np.ndarray:
+    """(k, 2) uint64 ordered pairs (i in a, j in b), sorted by (i, j)."""
+    a, b = _f64(a), _f64(b)
+    return _pairs(lambda out, cap: lib().hjo_join_pairs_brute(_ptr(a), a.shape[0], _ptr(b), b.shape[0], a.shape[1],
+                                                              eps, _ptr(out), cap, threads), cap_hint)
+
+
+def dim_costs(x, eps: float) -> np.ndarray:
+    """Per-dim Super-EGO cost on the deterministic sample (uint64, d)."""
+    x = _f64(x)
+    out = np.zeros(x.shape[1], dtype=np.uint64)
+    lib().hjo_dim_costs(_ptr(x), x.shape[0], x.shape[1], eps, _ptr(out))
+    return out
+
+
+def dim_order(x, eps: float) -> np.ndarray:
+    """reorder_dim: new key position of every dim, ascending cost, ties by index
+    (the reference's convention, hilbertjoin/egojoin.cpp:587-589)."""
+    c = dim_costs(x, eps)
+    ranked = sorted(range(len(c)), key=lambda t: (int(c[t]), t))
+    rd = np.zeros(len(c), dtype=np.int32)
+    for pos, t in enumerate(ranked):
+        rd[t] = pos
+    return rd
 
 
 def cells(x, eps: float) -> np.ndarray:

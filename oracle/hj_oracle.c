@@ -158,6 +158,91 @@ HJO_EXPORT void hjo_self_row_counts(const double *X, uint64_t n, uint32_t d, dou
     }
 }
 
+/* ---------------------------------------------------------------- pair lists */
+
+/* The qualifying pairs themselves, as (i, j) input indices sorted by (i, j):
+ * self joins i < j, two-set joins (index in A, index in B). The reference
+ * would push join_pair{p1, p2} (hilbertjoin/egojoin.h:32-35) per qualifying
+ * pair (hilbertjoin/test_ego_loop3_queue.cpp:19-37); that code is compiled out
+ * of its count build, so this restates the pair list from the same pair test.
+ * Two passes: per-row counts, then each row's pairs at its prefix offset.
+ * Writes out[0 .. 2*total) only if total <= cap; returns total. */
+static uint64_t pairs_brute(const double *A, uint64_t nA, const double *B, uint64_t nB, uint32_t d, double eps,
+                            int self, uint64_t *out, uint64_t cap, int nthreads) {
+    const double T = eps * eps;
+    set_threads(nthreads);
+    uint64_t *rc = (uint64_t *)calloc((size_t)nA + 1, sizeof(uint64_t));
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t ii = 0; ii < (int64_t)nA; ++ii) {
+        uint64_t i = (uint64_t)ii, cnt = 0;
+        for (uint64_t j = self ? i + 1 : 0; j < nB; ++j)
+            if (dist2(A + (size_t)i * d, B + (size_t)j * d, d) <= T) ++cnt;
+        rc[i] = cnt;
+    }
+    uint64_t total = 0;
+    for (uint64_t i = 0; i < nA; ++i) {
+        uint64_t c = rc[i];
+        rc[i] = total;
+        total += c;
+    }
+    if (total <= cap && out) {
+#pragma omp parallel for schedule(dynamic, 16)
+        for (int64_t ii = 0; ii < (int64_t)nA; ++ii) {
+            uint64_t i = (uint64_t)ii, o = rc[i];
+            for (uint64_t j = self ? i + 1 : 0; j < nB; ++j)
+                if (dist2(A + (size_t)i * d, B + (size_t)j * d, d) <= T) {
+                    out[2 * o] = i;
+                    out[2 * o + 1] = j;
+                    ++o;
+                }
+        }
+    }
+    free(rc);
+    return total;
+}
+
+HJO_EXPORT uint64_t hjo_self_pairs_brute(const double *X, uint64_t n, uint32_t d, double eps, uint64_t *out,
+                                         uint64_t cap, int nthreads) {
+    return pairs_brute(X, n, X, n, d, eps, 1, out, cap, nthreads);
+}
+
+HJO_EXPORT uint64_t hjo_join_pairs_brute(const double *A, uint64_t nA, const double *B, uint64_t nB, uint32_t d,
+                                         double eps, uint64_t *out, uint64_t cap, int nthreads) {
+    return pairs_brute(A, nA, B, nB, d, eps, 0, out, cap, nthreads);
+}
+
+/* ---------------------------------------------------------- dimension order */
+
+static int cmp_double(const void *a, const void *b) {
+    double x = *(const double *)a, y = *(const double *)b;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+/* Per-dim cost of the Super-EGO dimension reordering, the estimate of the
+ * reference's outputStatistics (hilbertjoin/egojoin.cpp:523-592): with h the
+ * histogram of the sampled points' cells floor(x/eps) in dim j,
+ * cost_j = sum_c h[c](h[c]-1)/2 + sum_c h[c-1] h[c], i.e. the number of
+ * unordered sample pairs whose cells are equal or adjacent. The reference
+ * samples with drand48 and skips dims with cells beyond +-100000; this
+ * restatement uses the engine's deterministic sample (S = min(n, 8192) points,
+ * point floor(s n / S) for s = 0..S-1) and costs every dim. */
+HJO_EXPORT void hjo_dim_costs(const double *X, uint64_t n, uint32_t d, double eps, uint64_t *costs) {
+    const uint64_t S = n < 8192 ? n : 8192;
+    double *v = (double *)malloc((S ? S : 1) * sizeof(double));
+    for (uint32_t t = 0; t < d; ++t) {
+        for (uint64_t s = 0; s < S; ++s) v[s] = floor(X[(s * n / S) * d + t] / eps);
+        qsort(v, S, sizeof(double), cmp_double);
+        uint64_t cost = 0, q = 0;
+        for (uint64_t s = 0; s < S; ++s) {
+            if (q < s + 1) q = s + 1;
+            while (q < S && v[q] <= v[s] + 1.0) ++q;
+            cost += q - s - 1;
+        }
+        costs[t] = cost;
+    }
+    free(v);
+}
+
 /* ---------------------------------------------------------------- EGO order */
 
 HJO_EXPORT void hjo_cells(const double *X, uint64_t n, uint32_t d, double eps, double *cells) {

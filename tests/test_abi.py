@@ -20,7 +20,8 @@ def test_header_declares_the_boundary():
     names = declared_functions()
     for must in ("hj_self_join_count", "hj_join_count", "hj_self_join_count_f32", "hj_join_count_f32",
                  "hj_test_ego_loop3_macro", "hj_test_ego_loop3_noself", "hj_ego_sort", "hj_server_create",
-                 "hj_submit", "hj_poll", "hj_wait", "hj_set_upload"):
+                 "hj_submit", "hj_poll", "hj_wait", "hj_set_upload", "hj_self_join_pairs", "hj_join_pairs",
+                 "hj_self_join_pairs_f32", "hj_join_pairs_f32"):
         assert must in names
 
 
@@ -46,5 +47,5 @@ def test_no_device_gives_status_not_crash():
 def test_status_strings():
     import hilbertjoin_b200 as hj
     L = hj.lib()
-    for s in range(10):
+    for s in range(11):
         assert L.hj_status_str(s)
