@@ -14,7 +14,7 @@ events on the stream the engine runs on; `e2e` through the public C-ABI call
 with the input in pinned host memory (host->device copy and the count's
 read-back inside the timed region, synchronous calls, host clock).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--form tf32|bf16x3|plain]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--form tf32|fp16|bf16x3|plain]
     python bench.py --impl reference ...     (the reference's AVX-512 CPU path)
 
 With N > 1 (torchrun), every rank runs its own replica of the workload on its
@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="tf32", choices=["tf32", "bf16x3", "plain"])
+    ap.add_argument("--form", default="tf32", choices=["tf32", "fp16", "bf16x3", "plain"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison step")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--n", type=int, default=N_POINTS, help=argparse.SUPPRESS)
@@ -327,6 +327,9 @@ def main():
         if args.form == "tf32":
             peak = sustained / 2.0
             src = f"{peak_src} bf16_tflops_sustained / 2 (TF32 dense = half of BF16)"
+        elif args.form == "fp16":
+            peak = sustained
+            src = f"{peak_src} bf16_tflops_sustained (FP16 dense = BF16 dense)"
         else:
             peak = sustained / 3.0
             src = f"{peak_src} bf16_tflops_sustained / 3 (three BF16 products per algorithmic multiply-add)"
@@ -360,7 +363,7 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": {"tf32": "tf32", "bf16x3": "bf16x3", "plain": "f64"}[args.form],
+            "vs_baseline": None, "dtype": {"tf32": "tf32", "fp16": "fp16", "bf16x3": "bf16x3", "plain": "f64"}[args.form],
             "data": "synthetic (seeded uniform, FP32)",
             "config": {"workload": f"self-join {n} x {DIM}, uniform [0,1) FP32 seed {SEED}, eps for {NEIGHBOURS} "
                                    f"neighbours (dense regime, all pairs evaluated)", "n": n, "d": DIM,

@@ -22,8 +22,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libhj.so")
 
-FORMS = {"plain": 0, "fp64": 0, "tf32": 1, "bf16x3": 2, "auto": 3}
-FORM_NAMES = {0: "plain_fp64", 1: "tc_tf32", 2: "tc_bf16x3", 3: "auto"}
+FORMS = {"plain": 0, "fp64": 0, "tf32": 1, "bf16x3": 2, "auto": 3, "fp16": 4}
+FORM_NAMES = {0: "plain_fp64", 1: "tc_tf32", 2: "tc_bf16x3", 3: "auto", 4: "tc_fp16"}
 
 OK = 0
 STATUS = {0: "ok", 1: "invalid argument", 2: "out of device memory", 3: "CUDA error", 4: "device wait timed out",

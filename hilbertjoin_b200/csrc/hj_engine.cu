@@ -207,7 +207,7 @@ struct JoinIn {
     bool self;
 };
 
-static int form_is_tc(int f) { return f == HJ_FORM_TC_TF32 || f == HJ_FORM_TC_BF16X3; }
+static int form_is_tc(int f) { return f == HJ_FORM_TC_TF32 || f == HJ_FORM_TC_BF16X3 || f == HJ_FORM_TC_FP16; }
 
 static int check_cuda(const char *what) {
     cudaError_t e = cudaGetLastError();
@@ -226,16 +226,17 @@ static float ev_ms(cudaEvent_t a, cudaEvent_t b) {
 
 // Sorts one set and gathers the layouts the chosen form needs.
 static int prepare_set(Ctx *c, cudaStream_t st, const void *x, uint64_t n, int dtype_bytes, const Grid &g,
-                       const GridDev &gd, const double *center, double norm_scale, int form, bool is_b,
-                       SortedSet *out, int *launches) {
+                       const GridDev &gd, const double *center, double norm_scale, double op_scale, int form,
+                       bool is_b, SortedSet *out, int *launches) {
     SortedSet s;
     s.n = n;
     s.d = g.d;
     s.dtype_bytes = dtype_bytes;
     s.src = x;
     s.center = center;
+    s.op_scale = form == HJ_FORM_TC_FP16 ? op_scale : 1.0;
     const uint32_t W = g.W;
-    const bool norm_order = form == HJ_FORM_TC_TF32 || form == HJ_FORM_TC_BF16X3;
+    const bool norm_order = form_is_tc(form);
     uint32_t *keys_wm = (uint32_t *)slot_alloc_impl(c, st, is_b ? kSlotKeysWmB : kSlotKeysWmA,
                                                     n * (W + (norm_order ? 1 : 0)) * 4);
     uint32_t *perm = (uint32_t *)slot_alloc_impl(c, st, is_b ? kSlotPermB : kSlotPermA, n * 4);
@@ -260,6 +261,10 @@ static int prepare_set(Ctx *c, cudaStream_t st, const void *x, uint64_t n, int d
             s.tf32 = (float *)slot_alloc_impl(c, st, is_b ? kSlotTf32B : kSlotTf32A, s.npad_tc * s.kpad_tf32 * 4);
             if (!s.tf32) return fail(HJ_ERR_OOM, "out of device memory");
             flags |= kGatherTf32;
+        } else if (form == HJ_FORM_TC_FP16) {
+            s.bf_hi = (uint16_t *)slot_alloc_impl(c, st, is_b ? kSlotHiB : kSlotHiA, s.npad_tc * s.kpad_bf16 * 2);
+            if (!s.bf_hi) return fail(HJ_ERR_OOM, "out of device memory");
+            flags |= kGatherF16;
         } else {
             s.bf_hi = (uint16_t *)slot_alloc_impl(c, st, is_b ? kSlotHiB : kSlotHiA, s.npad_tc * s.kpad_bf16 * 2);
             s.bf_lo = (uint16_t *)slot_alloc_impl(c, st, is_b ? kSlotLoB : kSlotLoA, s.npad_tc * s.kpad_bf16 * 2);
@@ -337,11 +342,13 @@ struct Prepared {
     uint64_t na_eff = 0, nb_eff = 0;
     int launches = 0;
     double reorder_ms = 0;
+    double op_scale = 1.0;  // FP16 form: operand scale 2^s
 };
 
 static int prepare_join(Ctx *c, cudaStream_t st, const JoinIn &in, const hj_opts *opts, int form_override,
                         Prepared *P) {
     int form = form_override >= 0 ? form_override : (opts ? opts->form : HJ_FORM_PLAIN_FP64);
+    if (form < HJ_FORM_PLAIN_FP64 || form > HJ_FORM_TC_FP16) return fail(HJ_ERR_INVALID_ARG, "unknown form");
     int active_dims = opts ? opts->active_dims : -1;
     const bool ref_compat = opts && opts->ref_compat;
     if (active_dims < 0) active_dims = in.self ? 3 : 2;
@@ -422,19 +429,27 @@ static int prepare_join(Ctx *c, cudaStream_t st, const JoinIn &in, const hj_opts
             nmax += r * r;
         }
         norm_scale = nmax > 0 ? 65535.0 / (nmax * 1.001) : 0.0;
+        // FP16 operand scale: 2^s with the largest centred |coordinate| in [2^14, 2^15)
+        double rmax = 0.0;
+        for (uint32_t t = 0; t < d; ++t) {
+            if (hds[t].cmin > hds[t].cmax) continue;
+            const double lo = double_from_ordered(hds[t].xmin), hi = double_from_ordered(hds[t].xmax);
+            rmax = std::fmax(rmax, std::fmax(hi - hc[t], hc[t] - lo));
+        }
+        P->op_scale = rmax > 0 ? std::ldexp(1.0, 14 - std::ilogb(rmax)) : 1.0;
         cudaMemcpyAsync(center, hc.data(), d * 8, cudaMemcpyHostToDevice, st);
         cudaStreamSynchronize(st);  // hc goes out of scope
     }
 
     // 2. EGO sort + layouts
     SortedSet &A = P->A, &B = P->B;
-    if (int r = prepare_set(c, st, in.a, in.na, in.dtype_bytes, g, gd, center, norm_scale, form, false, &A,
-                            &launches))
+    if (int r = prepare_set(c, st, in.a, in.na, in.dtype_bytes, g, gd, center, norm_scale, P->op_scale, form,
+                            false, &A, &launches))
         return r;
     if (in.self) {
         B = A;
-    } else if (int r = prepare_set(c, st, in.b, in.nb, in.dtype_bytes, g, gd, center, norm_scale, form, true, &B,
-                                   &launches)) {
+    } else if (int r = prepare_set(c, st, in.b, in.nb, in.dtype_bytes, g, gd, center, norm_scale, P->op_scale,
+                                   form, true, &B, &launches)) {
         return r;
     }
     cudaEventRecord(c->ev[2], st);
@@ -512,14 +527,17 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
         cudaEventRecord(c->ev[4], st);
         cudaEventRecord(c->ev[5], st);
     } else {
+        // the FP16 form works in scaled units: norms, eps^2 and the bound times op_scale^2
+        const double s2 = A.op_scale * A.op_scale;
         tc_band_constants(form, d, maxabs, &c_rel, &c_abs);
-        TcParams p{form, T, c_rel, c_abs};
+        const double T_tc = T * s2;
+        TcParams p{form, T_tc, c_rel, c_abs};
         // Items whose error band would exceed half of eps^2 (eps^2 tiny against
         // the squared norms: the cancellation limit of the norm expansion) run
         // on the FP64 kernel instead.
         IndexResult idx_tc, idx_fp;
         for (int attempt = 0;; ++attempt) {
-            const double limit = attempt == 0 ? 0.5 * T : -1.0;  // -1: everything to FP64
+            const double limit = attempt == 0 ? 0.5 * T_tc : -1.0;  // -1: everything to FP64
             int sr = split_items_by_precision(idx, A, B, c_rel, c_abs, limit, slot_alloc_cb, &actx, st, &idx_tc,
                                               &idx_fp);
             if (sr == 2) return fail(HJ_ERR_OOM, "out of device memory (work list split)");
@@ -1004,7 +1022,7 @@ int hj_debug_tc_estimates(const float *A, uint64_t nA, const float *B, uint64_t 
                           float *out) {
     tl_error.clear();
     if (!A || !B || !out || nA == 0 || nB == 0) return fail(HJ_ERR_INVALID_ARG, "null pointer or empty set");
-    if (form != HJ_FORM_TC_TF32 && form != HJ_FORM_TC_BF16X3) return fail(HJ_ERR_INVALID_ARG, "not a tensor-core form");
+    if (!form_is_tc(form)) return fail(HJ_ERR_INVALID_ARG, "not a tensor-core form");
     Ctx *c;
     if (int r = get_ctx(-1, &c)) return r;
     float *dbg = nullptr;

@@ -93,9 +93,10 @@ struct SortedSet {
     uint64_t n_tiles64 = 0;
     // tensor-core layouts: [npad][kpad] with npad a multiple of 256
     float *tf32 = nullptr;       // TF32-rounded values in FP32 containers, kpad = roundup(d, 32)
-    uint16_t *bf_hi = nullptr;   // BF16 split, kpad16 = roundup(d, 64)
+    uint16_t *bf_hi = nullptr;   // BF16 split (or the FP16 operand), kpad16 = roundup(d, 64)
     uint16_t *bf_lo = nullptr;
     const double *center = nullptr;  // per-dim shift of the tensor-core operands (shared by A and B)
+    double op_scale = 1.0;       // FP16 form: power of two applied to operands (norms: its square)
     float *norms = nullptr;      // FP32(|x - center|^2 in FP64); padding rows hold kPadNorm
     float *tile_maxnorm_a = nullptr;  // per 128-row tile
     float *tile_maxnorm_b = nullptr;  // per 256-row tile
@@ -174,7 +175,7 @@ void launch_scan_u32(uint32_t *a, uint64_t count, unsigned long long *total, cud
 
 // Gathers the sorted layouts of a set (flags select the layouts to build).
 enum GatherFlags : uint32_t { kGatherRows = 1, kGatherKeys = 2, kGatherPlain = 4, kGatherTf32 = 8, kGatherBf16 = 16,
-                              kGatherNorms = 32 };
+                              kGatherNorms = 32, kGatherF16 = 64 };
 void launch_gather(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const uint32_t *perm,
                    const uint32_t *keys_wm, uint32_t W, const SortedSet &out, uint32_t flags, cudaStream_t st,
                    int *launches);
@@ -205,8 +206,8 @@ void launch_pairs_fp64(const SortedSet &A, const SortedSet &B, bool self, uint64
 // Tensor-core kernel + FP64 recheck of the band. Adds into *d_count; band pair
 // count into *d_band_total (may exceed `band_cap`: then the caller regrows).
 struct TcParams {
-    int form;             // HJ_FORM_TC_TF32 or HJ_FORM_TC_BF16X3
-    double T;             // eps * eps
+    int form;             // HJ_FORM_TC_TF32, HJ_FORM_TC_BF16X3 or HJ_FORM_TC_FP16
+    double T;             // eps * eps (FP16 form: times op_scale^2, the units of the norms)
     double c_rel;         // band half-width: c_rel * (|a|^2 + |b|^2) + c_abs
     double c_abs;
 };

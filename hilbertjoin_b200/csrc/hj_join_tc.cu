@@ -1,4 +1,4 @@
-// hj_join_tc.cu -- tensor-core forms (HJ_FORM_TC_TF32, HJ_FORM_TC_BF16X3).
+// hj_join_tc.cu -- tensor-core forms (HJ_FORM_TC_TF32, HJ_FORM_TC_BF16X3, HJ_FORM_TC_FP16).
 //
 // Replaces the same block-pair kernel as hj_join_fp64.cu (the reference's
 // EGO_LOOP_TRAN[_NOSELF], hilbertjoin/egojoin.h:311-392, :482-553), but with
@@ -18,7 +18,10 @@
 //                each), dist^2 estimate, classification, count;
 //   * TF32: operands rounded to TF32 on the device (round to nearest), one
 //     MMA per K step; BF16X3: a = a_hi + a_lo in BF16, a.b =
-//     a_hi.b_hi + a_lo.b_hi + a_hi.b_lo (three MMAs per K step);
+//     a_hi.b_hi + a_lo.b_hi + a_hi.b_lo (three MMAs per K step); FP16: the
+//     operands scaled by a power of two into FP16's range and rounded once
+//     (the precision of TF32 at twice its MMA rate), one MMA per K step, the
+//     norms, eps^2 and the bound in the same scaled units;
 //   * exact count: with s = |a|^2 + |b|^2 - 2 v (v the tensor-core dot product),
 //     every error of v, of the FP32 norms and of the FP32 epilogue is bounded
 //     by c_rel * (|a|^2 + |b|^2) + c_abs (tc_band_constants). A pair with
@@ -79,6 +82,7 @@ struct TcArgs {
     uint64_t band_cap;
     unsigned long long *band_total;
     uint32_t *err;
+    float s_unscale;                // 1 / op_scale^2: s_hat back to the caller's units (band, dbg)
     float *dbg;                     // optional: s_hat for every pair, input order [na][nb] (tests)
     const uint32_t *perm_a, *perm_b;  // EGO rank -> input index (for dbg)
 };
@@ -200,7 +204,7 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
 // Instruction descriptor: D = F32, A/B K-major, M = 128, N = 256.
 template <int FORM>
 __device__ __forceinline__ constexpr uint32_t instr_desc() {
-    constexpr uint32_t ab = FORM == HJ_FORM_TC_TF32 ? 2u : 1u;  // TF32 : BF16
+    constexpr uint32_t ab = FORM == HJ_FORM_TC_TF32 ? 2u : (FORM == HJ_FORM_TC_BF16X3 ? 1u : 0u);  // TF32, BF16, F16
     return (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(kTcTileB >> 3) << 17) | ((uint32_t)(kTcTileA >> 4) << 24);
 }
 
@@ -220,6 +224,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // A atoms per buffer: TF32 ka; BF16 2*ka (hi atoms, then lo atoms). B atoms
     // per tile, in ring order: TF32 q = 0..ka-1; BF16 (hi q, lo q) for each q.
     constexpr bool kBf = FORM == HJ_FORM_TC_BF16X3;
+    constexpr int32_t kAtomElems = FORM == HJ_FORM_TC_TF32 ? 32 : 64;  // K elements per 128-byte atom
     const uint32_t a_atoms = kBf ? 2 * p.ka : p.ka;
     const uint32_t b_atoms = a_atoms;
     const uint32_t a_buf_bytes = a_atoms * kAStageBytes;
@@ -283,7 +288,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const bool lo = kBf && q >= p.ka;
                     const uint32_t kq = kBf ? (lo ? q - p.ka : q) : q;
                     tma_load_2d(smem_raw + (adst + q * kAStageBytes - smem_u32(smem_raw)), lo ? &tm_a2 : &tm_a,
-                                (int32_t)(kq * (kBf ? 64 : 32)), (int32_t)(w.a * kTcTileA), &bar_afull[abuf]);
+                                (int32_t)(kq * kAtomElems), (int32_t)(w.a * kTcTileA), &bar_afull[abuf]);
                 }
                 ++a_cnt;
                 for (uint32_t bt = w.b0; bt < w.b1; ++bt) {
@@ -294,7 +299,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         const bool lo = kBf && (q & 1u);
                         const uint32_t kq = kBf ? (q >> 1) : q;
                         tma_load_2d(smem_raw + (b_base + s * kBStageBytes - smem_u32(smem_raw)), lo ? &tm_b2 : &tm_b,
-                                    (int32_t)(kq * (kBf ? 64 : 32)), (int32_t)(bt * kTcTileB), &bar_bfull[s]);
+                                    (int32_t)(kq * kAtomElems), (int32_t)(bt * kTcTileB), &bar_bfull[s]);
                         ++b_cnt;
                     }
                 }
@@ -499,14 +504,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                             const bool ok = (unsigned)(col - jloL) < (unsigned)(jhiL - jloL) && giL < p.na;
                             cnt += (ok && t <= tinL) ? 1ull : 0ull;
                             if (p.dbg != nullptr && giL < p.na && gj0 + col < p.nb)
-                                p.dbg[(uint64_t)p.perm_a[giL] * p.nb + p.perm_b[gj0 + col]] = naL + t;
+                                p.dbg[(uint64_t)p.perm_a[giL] * p.nb + p.perm_b[gj0 + col]] = (naL + t) * p.s_unscale;
                             if (ok && t > tinL && t <= toutL) {  // band pair: very rare
                                 const unsigned long long k = atomicAdd(p.band_total, 1ull);
                                 if (k < p.band_cap) {
                                     BandEntry e;
                                     e.ia = (uint32_t)giL;
                                     e.jb = (uint32_t)(gj0 + col);
-                                    e.s_hat = naL + t;
+                                    e.s_hat = (naL + t) * p.s_unscale;
                                     e.pad = 0;
                                     p.band[k] = e;
                                 }
@@ -580,18 +585,27 @@ __global__ void k_recheck(const TIn *__restrict__ ra, const TIn *__restrict__ rb
 // subnormal operands (TF32/BF16 keep the FP32 exponent range; values below
 // 2^-100 times the largest coordinate are the only ones that can lose
 // relative accuracy) and is negligible for data of ordinary scale.
+//
+// FP16 (in units scaled by op_scale^2, where the largest centred coordinate
+// is below 2^15): operands rounded once from FP64, 2^-11 relative each, so
+// products as TF32's; FP16 subnormals (|v| < 2^-14) carry an absolute error up
+// to 2^-25 instead, at most 2 * 2^-25 * 2^15 per product term, d terms, twice
+// in s: c_abs = 1.25 * d * 2^-8.
 void tc_band_constants(int form, uint32_t d, double maxabs, double *c_rel, double *c_abs) {
     const double u24 = std::ldexp(1.0, -24), acc = std::ldexp(1.0, -22);
     const double kpad = form == HJ_FORM_TC_TF32 ? (double)((d + 31) / 32 * 32) : (double)((d + 63) / 64 * 64);
     double dot;
-    if (form == HJ_FORM_TC_TF32) {
+    if (form == HJ_FORM_TC_TF32 || form == HJ_FORM_TC_FP16) {
         const double u = std::ldexp(1.0, -11);
         dot = 2 * u + u * u + 2 * u24 + kpad * acc;
     } else {
         dot = 3.1 * std::ldexp(1.0, -16) + 2 * u24 + 3 * kpad * acc;
     }
     *c_rel = 1.25 * (dot + 12 * u24 + (double)d * std::ldexp(1.0, -50));
-    *c_abs = 1e-30 + 4.0 * (double)d * std::ldexp(std::fmax(maxabs, 1e-30), -100) * std::fmax(maxabs, 1.0);
+    if (form == HJ_FORM_TC_FP16)
+        *c_abs = 1.25 * (double)d * std::ldexp(1.0, -8);
+    else
+        *c_abs = 1e-30 + 4.0 * (double)d * std::ldexp(std::fmax(maxabs, 1e-30), -100) * std::fmax(maxabs, 1.0);
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -615,16 +629,16 @@ static EncodeTiledFn encode_fn(std::string *err) {
 }
 
 // 2D map over a row-major [rows][kp] matrix, box = one 128-byte K atom x box_rows.
-static bool make_map(CUtensorMap *m, const void *base, bool bf16, uint64_t rows, uint32_t kp, uint32_t box_rows,
-                     std::string *err) {
+static bool make_map(CUtensorMap *m, const void *base, CUtensorMapDataType type, uint64_t rows, uint32_t kp,
+                     uint32_t box_rows, std::string *err) {
     EncodeTiledFn fn = encode_fn(err);
     if (!fn) return false;
-    const uint32_t esz = bf16 ? 2 : 4;
+    const uint32_t esz = type == CU_TENSOR_MAP_DATA_TYPE_FLOAT32 ? 4 : 2;
     cuuint64_t gdim[2] = {kp, rows};
     cuuint64_t gstride[1] = {(cuuint64_t)kp * esz};
     cuuint32_t box[2] = {kAtomBytes / esz, box_rows};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = fn(m, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+    CUresult r = fn(m, type, 2,
                     const_cast<void *>(base), gdim, gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                     CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -643,7 +657,7 @@ struct TcLayout {
 static TcLayout tc_layout(int form, uint32_t d) {
     TcLayout L;
     L.ka = form == HJ_FORM_TC_TF32 ? (d + 31) / 32 : (d + 63) / 64;
-    const uint32_t a_atoms = form == HJ_FORM_TC_TF32 ? L.ka : 2 * L.ka;
+    const uint32_t a_atoms = form == HJ_FORM_TC_BF16X3 ? 2 * L.ka : L.ka;
     const size_t a_bytes = (size_t)a_atoms * kAStageBytes;
     const size_t budget = 216 * 1024;  // + 1 KB alignment + ~5 KB static smem <= 227 KB per block
     L.a_bufs = 2 * a_bytes + 3 * kBStageBytes <= budget ? 2 : 1;
@@ -661,23 +675,28 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, bool self, uint64_t n
                    uint64_t band_cap, unsigned long long *d_band_total, uint32_t *d_err, int num_sms, cudaStream_t st,
                    std::string *err) {
     if (idx.n_items == 0) return 0;
-    const bool bf = tp.form == HJ_FORM_TC_BF16X3;
     const TcLayout L = tc_layout(tp.form, A.d);
     if (L.nst < 2) {
         *err = "dimension too large for the tensor-core kernel";
         return 1;
     }
     CUtensorMap ma, ma2, mb, mb2;
-    if (!bf) {
-        if (!make_map(&ma, A.tf32, false, A.npad_tc, A.kpad_tf32, kTcTileA, err)) return 1;
-        if (!make_map(&mb, B.tf32, false, B.npad_tc, B.kpad_tf32, kTcTileB, err)) return 1;
+    if (tp.form == HJ_FORM_TC_TF32) {
+        if (!make_map(&ma, A.tf32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, A.npad_tc, A.kpad_tf32, kTcTileA, err)) return 1;
+        if (!make_map(&mb, B.tf32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, B.npad_tc, B.kpad_tf32, kTcTileB, err)) return 1;
+        ma2 = ma;
+        mb2 = mb;
+    } else if (tp.form == HJ_FORM_TC_FP16) {
+        if (!make_map(&ma, A.bf_hi, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, A.npad_tc, A.kpad_bf16, kTcTileA, err)) return 1;
+        if (!make_map(&mb, B.bf_hi, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, B.npad_tc, B.kpad_bf16, kTcTileB, err)) return 1;
         ma2 = ma;
         mb2 = mb;
     } else {
-        if (!make_map(&ma, A.bf_hi, true, A.npad_tc, A.kpad_bf16, kTcTileA, err)) return 1;
-        if (!make_map(&ma2, A.bf_lo, true, A.npad_tc, A.kpad_bf16, kTcTileA, err)) return 1;
-        if (!make_map(&mb, B.bf_hi, true, B.npad_tc, B.kpad_bf16, kTcTileB, err)) return 1;
-        if (!make_map(&mb2, B.bf_lo, true, B.npad_tc, B.kpad_bf16, kTcTileB, err)) return 1;
+        const CUtensorMapDataType t = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+        if (!make_map(&ma, A.bf_hi, t, A.npad_tc, A.kpad_bf16, kTcTileA, err)) return 1;
+        if (!make_map(&ma2, A.bf_lo, t, A.npad_tc, A.kpad_bf16, kTcTileA, err)) return 1;
+        if (!make_map(&mb, B.bf_hi, t, B.npad_tc, B.kpad_bf16, kTcTileB, err)) return 1;
+        if (!make_map(&mb2, B.bf_lo, t, B.npad_tc, B.kpad_bf16, kTcTileB, err)) return 1;
     }
     TcArgs a;
     a.ka = L.ka;
@@ -708,14 +727,18 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, bool self, uint64_t n
     a.band_cap = band_cap;
     a.band_total = d_band_total;
     a.err = d_err;
+    a.s_unscale = (float)(1.0 / (A.op_scale * A.op_scale));  // a power of two: exact
     a.dbg = g_dbg_out;
     a.perm_a = A.perm;
     a.perm_b = B.perm;
     uint64_t grid = (uint64_t)num_sms;
     if (grid > idx.n_items) grid = idx.n_items;
-    if (!bf) {
+    if (tp.form == HJ_FORM_TC_TF32) {
         ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_TF32>, 217 * 1024);
         k_join_tc<HJ_FORM_TC_TF32><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
+    } else if (tp.form == HJ_FORM_TC_FP16) {
+        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_FP16>, 217 * 1024);
+        k_join_tc<HJ_FORM_TC_FP16><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
     } else {
         ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_BF16X3>, 217 * 1024);
         k_join_tc<HJ_FORM_TC_BF16X3><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);

@@ -10,6 +10,7 @@
 // order is the lexicographic cell order; the sort then only moves 4-byte
 // indices, and every data layout is written once, by the gather.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <map>
 #include <mutex>
@@ -443,13 +444,22 @@ __device__ __forceinline__ float to_tf32_rn(float v) {
 // TF32 rows [npad][kp32], BF16 hi/lo rows [npad][kp16]. The operands are the
 // coordinates minus `center` (per dim): distances are shift invariant, and the
 // smaller norms narrow the error band of the norm expansion.
+// FP16 (f16 != nullptr): (x - center) * scale rounded once from FP64 to FP16
+// (round to nearest even); scale is a power of two, so the scaling is exact.
 __global__ void k_gather_tc(const void *x, int dtype_bytes, uint64_t n, uint32_t d,
                             const uint32_t *__restrict__ perm, const double *__restrict__ center, uint64_t npad,
-                            uint32_t kp, float *tf32, uint16_t *bf_hi, uint16_t *bf_lo) {
+                            uint32_t kp, float *tf32, uint16_t *bf_hi, uint16_t *bf_lo, uint16_t *f16,
+                            double scale) {
     uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= npad * kp) return;
     uint64_t r = e / kp;
     uint32_t k = (uint32_t)(e % kp);
+    if (f16) {
+        double w = 0.0;
+        if (r < n && k < d) w = (coord(x, dtype_bytes, (uint64_t)perm[r] * d + k) - center[k]) * scale;
+        f16[e] = __half_as_ushort(__double2half(w));
+        return;
+    }
     float v = 0.0f;
     if (r < n && k < d) v = (float)(coord(x, dtype_bytes, (uint64_t)perm[r] * d + k) - center[k]);
     if (tf32) tf32[e] = to_tf32_rn(v);
@@ -465,7 +475,7 @@ __global__ void k_gather_tc(const void *x, int dtype_bytes, uint64_t n, uint32_t
 // |x - center|^2 per sorted row in FP64 (input precision widened exactly),
 // stored as FP32; padding rows get kPadNorm so that they never pass a threshold.
 __global__ void k_norms(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const uint32_t *__restrict__ perm,
-                        const double *__restrict__ center, uint64_t npad, float *norms) {
+                        const double *__restrict__ center, uint64_t npad, double scale2, float *norms) {
     uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= npad) return;
     if (r >= n) {
@@ -478,7 +488,7 @@ __global__ void k_norms(const void *x, int dtype_bytes, uint64_t n, uint32_t d, 
         double v = coord(x, dtype_bytes, src * d + k) - center[k];
         s = fma(v, v, s);
     }
-    norms[r] = (float)s;
+    norms[r] = (float)(s * scale2);
 }
 
 // Per-tile maximum norm over real rows (padding rows excluded).
@@ -523,19 +533,27 @@ void launch_gather(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const
         uint64_t total = o.npad_tc * o.kpad_tf32;
         k_gather_tc<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.center,
                                                                       o.npad_tc, o.kpad_tf32, o.tf32, nullptr,
-                                                                      nullptr);
+                                                                      nullptr, nullptr, 1.0);
         ++L;
     }
     if (flags & kGatherBf16) {
         uint64_t total = o.npad_tc * o.kpad_bf16;
         k_gather_tc<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.center,
                                                                       o.npad_tc, o.kpad_bf16, nullptr, o.bf_hi,
-                                                                      o.bf_lo);
+                                                                      o.bf_lo, nullptr, 1.0);
+        ++L;
+    }
+    if (flags & kGatherF16) {
+        uint64_t total = o.npad_tc * o.kpad_bf16;
+        k_gather_tc<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.center,
+                                                                      o.npad_tc, o.kpad_bf16, nullptr, nullptr,
+                                                                      nullptr, o.bf_hi, o.op_scale);
         ++L;
     }
     if (flags & kGatherNorms) {
         k_norms<<<(unsigned)hj_ceil_div(o.npad_tc, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.center,
-                                                                      o.npad_tc, o.norms);
+                                                                      o.npad_tc, o.op_scale * o.op_scale,
+                                                                      o.norms);
         k_tile_max<<<(unsigned)hj_ceil_div(o.npad_tc / kTcTileA, 256), 256, 0, st>>>(o.norms, o.npad_tc, kTcTileA,
                                                                                     o.tile_maxnorm_a);
         k_tile_max<<<(unsigned)hj_ceil_div(o.npad_tc / kTcTileB, 256), 256, 0, st>>>(o.norms, o.npad_tc, kTcTileB,

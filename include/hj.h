@@ -69,7 +69,13 @@ typedef enum {
     HJ_FORM_TC_BF16X3 = 2,
     /* HJ_FORM_TC_TF32 when the input allows it (d <= 256, coordinates within
      * +-2^60), else HJ_FORM_PLAIN_FP64. */
-    HJ_FORM_AUTO = 3
+    HJ_FORM_AUTO = 3,
+    /* As TF32 with FP16 operands at twice the tensor-core rate: the centred
+     * coordinates are scaled by a power of two 2^s (exact) so that the largest
+     * lands in [2^14, 2^15), then rounded once from FP64 to FP16 (11-bit
+     * significand, the precision of TF32); a.b in FP32 accumulation, band
+     * pairs re-evaluated with the FP64 pair test. */
+    HJ_FORM_TC_FP16 = 4
 } hj_form;
 
 typedef struct {

@@ -91,7 +91,7 @@ def test_pairs_are_deterministic_and_consistent_with_all_forms(hj):
     p1 = hj.self_join_pairs(x, eps)
     p2 = hj.self_join_pairs(x, eps)
     assert np.array_equal(p1, p2)
-    for form in ("plain", "tf32", "bf16x3"):
+    for form in ("plain", "tf32", "bf16x3", "fp16"):
         assert hj.self_join_count(x, eps, form=form) == len(p1)
 
 

@@ -15,7 +15,7 @@ from tests.golden.make_golden import make
 pytestmark = pytest.mark.gpu
 
 GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "golden_counts.json")))["cases"]
-FORMS = ["plain", "tf32", "bf16x3"]
+FORMS = ["plain", "tf32", "bf16x3", "fp16"]
 
 
 @pytest.fixture(scope="module")
@@ -125,7 +125,7 @@ def test_fp32_input(hj, form):
         oracle.join_count_brute(x.astype(np.float64), b.astype(np.float64), eps)
 
 
-@pytest.mark.parametrize("form", ["tf32", "bf16x3"])
+@pytest.mark.parametrize("form", ["tf32", "bf16x3", "fp16"])
 def test_tc_signed_and_scaled_data(hj, form):
     """Mixed-sign coordinates and large magnitudes exercise the band bound."""
     rng = np.random.default_rng(8)

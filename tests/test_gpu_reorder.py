@@ -56,7 +56,7 @@ def test_dim_order_matches_oracle(hj, n, d, eps, kind, seed):
     assert sorted(rd.tolist()) == list(range(d))
 
 
-@pytest.mark.parametrize("form", ["plain", "tf32", "bf16x3"])
+@pytest.mark.parametrize("form", ["plain", "tf32", "bf16x3", "fp16"])
 def test_reorder_keeps_self_counts(hj, form):
     n, d = 60_000, 8
     x = skewed(n, d, 11, flat=3, dtype=np.float32)

@@ -32,7 +32,7 @@ def bound_constants(hj, form, a, b):
     return st["band_halfwidth_rel"]
 
 
-@pytest.mark.parametrize("form", ["tf32", "bf16x3"])
+@pytest.mark.parametrize("form", ["tf32", "bf16x3", "fp16"])
 @pytest.mark.parametrize("d,kind", [(4, "u"), (20, "u"), (32, "u"), (64, "u"), (100, "u"), (128, "u"),
                                     (64, "signed"), (28, "gmm")])
 def test_estimates_within_bound(hj, form, d, kind):
@@ -63,7 +63,7 @@ def test_estimates_within_bound(hj, form, d, kind):
     assert np.abs(est - ex).max() > 0
 
 
-@pytest.mark.parametrize("form", ["tf32", "bf16x3"])
+@pytest.mark.parametrize("form", ["tf32", "bf16x3", "fp16"])
 def test_band_pairs_are_rechecked(hj, form):
     """eps set at the median distance puts many pairs in the band; the count is
     still the FP64 count and the reported max error respects the bound."""
@@ -84,5 +84,24 @@ def test_forms_agree_dense(hj):
     x = W.uniform(20000, 64, 22, dtype=np.float32)
     eps = W.calibrate_eps(x, 20000, 32)
     want = oracle.self_count_brute(x.astype(np.float64), eps)
-    for form in ("plain", "tf32", "bf16x3"):
+    for form in ("plain", "tf32", "bf16x3", "fp16"):
         assert hj.self_join_count(x, eps, form=form) == want, form
+
+
+def test_fp16_scaling_extremes(hj):
+    """FP16 operands are scaled so the largest centred coordinate lands in
+    [2^14, 2^15): a dim whose range dwarfs the others drives the small ones
+    into FP16 subnormals (covered by the bound's absolute term), and offsets
+    far from zero are removed by the centring. Counts stay the FP64 counts."""
+    rng = np.random.default_rng(44)
+    x = rng.random((4000, 12))
+    x[:, 0] *= 1e6
+    x[:, 1:] *= 1e-3
+    for eps in (2e3, 5e4):
+        assert hj.self_join_count(x, eps, form="fp16") == oracle.self_count_brute(x, eps)
+    y = rng.random((3000, 20)) + 1e12
+    eps = float(np.sqrt(np.median(exact_dist2(y[:300] - 1e12, y[300:900] - 1e12)))) * 0.5
+    assert hj.self_join_count(y, eps, form="fp16") == oracle.self_count_brute(y, eps)
+    z = rng.standard_normal((3000, 40)) * 1e-9
+    eps = 4e-9
+    assert hj.self_join_count(z, eps, form="fp16") == oracle.self_count_brute(z, eps)
