@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="tf32", choices=["tf32", "fp16", "bf16x3", "plain"])
+    ap.add_argument("--form", default="fp16", choices=["fp16", "tf32", "bf16x3", "plain"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison step")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--n", type=int, default=N_POINTS, help=argparse.SUPPRESS)
@@ -212,7 +212,7 @@ def run_serving(args):
     import torch
     torch.cuda.set_device(0)
     from hilbertjoin_b200 import serving
-    r = serving.run_benchmark(n_requests=args.requests, form=args.form if args.form != "plain" else "tf32",
+    r = serving.run_benchmark(n_requests=args.requests, form=args.form if args.form != "plain" else "fp16",
                               baseline_requests=args.baseline_requests)
     line = {"metric": "join-serving requests/s (p50/p99 latency)", "value": r["saturated"]["requests_per_s"],
             "unit": "requests/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",

@@ -10,7 +10,7 @@
 //   -s S    active dimensions, (3^S+1)/2 stripes (0..5; the join ignores it as
 //           the reference does, which hard-codes 2)
 //   -t T, -k K, -a A   accepted and ignored, as in the reference
-// Extensions: -F plain|tf32|bf16x3|auto (distance form, default plain),
+// Extensions: -F plain|fp16|tf32|bf16x3|auto (distance form, default plain),
 //             -r (count like the reference: first 8*floor(n/8) EGO-sorted points),
 //             -R 0|1 (dimension reordering off/on; on by default for the join,
 //             which the reference's join driver always reorders,
@@ -106,11 +106,11 @@ static bool read_points(const std::string &path, size_t n, size_t d, std::vector
 
 static void usage(const char *prog) {
 #ifdef HJ_CLI_JOIN
-    fprintf(stderr, "Usage: %s -n N -m M -e EPS -d D [-f fileA] [-g fileB] [-F plain|tf32|bf16x3|auto] [-r] [-R 0|1]\n",
+    fprintf(stderr, "Usage: %s -n N -m M -e EPS -d D [-f fileA] [-g fileB] [-F plain|fp16|tf32|bf16x3|auto] [-r] [-R 0|1]\n",
             prog);
     fprintf(stderr, "Example: %s -n 200000 -m 200000 -e 0.2 -d 20\n", prog);
 #else
-    fprintf(stderr, "Usage: %s -n N -e EPS -d D [-f file] [-s activedims] [-F plain|tf32|bf16x3|auto] [-r] [-R 0|1]\n",
+    fprintf(stderr, "Usage: %s -n N -e EPS -d D [-f file] [-s activedims] [-F plain|fp16|tf32|bf16x3|auto] [-r] [-R 0|1]\n",
             prog);
     fprintf(stderr, "Example: %s -n 200000 -e 0.2 -d 64\n", prog);
 #endif
@@ -147,6 +147,7 @@ int main(int argc, char **argv) {
             case 'F':
                 if (!strcmp(optarg, "plain")) form = HJ_FORM_PLAIN_FP64;
                 else if (!strcmp(optarg, "tf32")) form = HJ_FORM_TC_TF32;
+                else if (!strcmp(optarg, "fp16")) form = HJ_FORM_TC_FP16;
                 else if (!strcmp(optarg, "bf16x3")) form = HJ_FORM_TC_BF16X3;
                 else if (!strcmp(optarg, "auto")) form = HJ_FORM_AUTO;
                 else {

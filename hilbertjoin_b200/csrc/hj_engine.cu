@@ -381,7 +381,7 @@ static int prepare_join(Ctx *c, cudaStream_t st, const JoinIn &in, const hj_opts
         unsigned long long bits = c->h_small[0];
         std::memcpy(&maxabs, &bits, 8);
     }
-    if (form == HJ_FORM_AUTO) form = (d <= 256 && maxabs < 1e18) ? HJ_FORM_TC_TF32 : HJ_FORM_PLAIN_FP64;
+    if (form == HJ_FORM_AUTO) form = (d <= 256 && maxabs < 1e18) ? HJ_FORM_TC_FP16 : HJ_FORM_PLAIN_FP64;
     if (form_is_tc(form) && d > 256) return fail(HJ_ERR_UNSUPPORTED, "tensor-core forms support d <= 256");
     if (form_is_tc(form) && !(maxabs < 1e18)) return fail(HJ_ERR_UNSUPPORTED, "tensor-core forms need |x| < 1e18");
     if (form == HJ_FORM_PLAIN_FP64 && d > 128) return fail(HJ_ERR_UNSUPPORTED, "plain FP64 form supports d <= 128");

@@ -26,7 +26,7 @@ def _reduce_sum(part: int, group=None) -> int:
     return int(t.item())
 
 
-def sharded_self_join_count(points, eps: float, form: str = "tf32", group=None,
+def sharded_self_join_count(points, eps: float, form: str = "fp16", group=None,
                             count_fn: Optional[Callable[[Tuple[int, int]], int]] = None, **kw) -> int:
     """Self-join count of `points` over all ranks of `group`; every rank returns the total.
 
@@ -43,7 +43,7 @@ def sharded_self_join_count(points, eps: float, form: str = "tf32", group=None,
     return _reduce_sum(part, group)
 
 
-def sharded_join_count(a, b, eps: float, form: str = "tf32", group=None,
+def sharded_join_count(a, b, eps: float, form: str = "fp16", group=None,
                        count_fn: Optional[Callable[[Tuple[int, int]], int]] = None, **kw) -> int:
     """Two-set join count (ordered pairs) over all ranks of `group`."""
     import torch.distributed as dist

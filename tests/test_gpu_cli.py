@@ -27,7 +27,7 @@ def run(args):
 
 
 @pytest.mark.parametrize("fmt", ["csv", "bin", "f32"])
-@pytest.mark.parametrize("form", ["plain", "tf32"])
+@pytest.mark.parametrize("form", ["plain", "tf32", "fp16"])
 def test_self_cli(gpu, tmp_path, fmt, form):
     x = np.random.default_rng(4).random((3000, 16))
     if fmt == "f32":
