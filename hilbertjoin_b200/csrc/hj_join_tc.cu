@@ -50,7 +50,18 @@
 
 namespace hj {
 
-constexpr int kEpiWarps = 8;  // two per TMEM lane quadrant, each on half of the columns
+#ifndef HJ_EPI_WARPS
+#define HJ_EPI_WARPS 8
+#endif
+// Epilogue warps: kEpiWarps / 4 per TMEM lane quadrant, each on kEpiCols of the
+// 256 accumulator columns, in two chunks of kChunkCols (one TMEM load each).
+constexpr int kEpiWarps = HJ_EPI_WARPS;
+constexpr int kEpiCols = 4 * kTcTileB / kEpiWarps;
+constexpr int kChunkCols = kEpiCols / 2;
+constexpr int kChunkGroups = kChunkCols / 32;  // 32-column groups per chunk
+constexpr int kEpiChunks = 2;
+constexpr int kEpiVec = kEpiCols / 32;  // norms per lane, group minima per warp
+static_assert(kEpiWarps == 8 || kEpiWarps == 16, "8 or 16 epilogue warps");
 constexpr int kTcThreads = 64 + 32 * kEpiWarps;
 constexpr uint32_t kAtomBytes = 128;                  // bytes of K per row per swizzle atom
 constexpr uint32_t kAStageBytes = kTcTileA * kAtomBytes;  // 16 KB per A atom
@@ -195,6 +206,13 @@ __device__ __forceinline__ void tmem_ld128(uint32_t taddr, float (&v)[128]) {
     for (int i = 0; i < 128; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// max(a, b, c) in one instruction (three-input max.f32, sm_100).
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // Shared-memory matrix descriptor: K-major operand in 128-byte swizzle atoms
 // (8 rows x 128 B, atoms stacked along M/N every 1024 B).
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
@@ -233,7 +251,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __shared__ __align__(8) uint64_t bar_afull[2], bar_aempty[2], bar_accfull[2], bar_accempty[2], bar_drain;
     __shared__ __align__(8) uint64_t bar_bfull[8], bar_bempty[8];
     __shared__ uint32_t tmem_base_sh;
-    __shared__ __align__(16) float epi_nb[kEpiWarps][128];
+    __shared__ __align__(16) float epi_nb[kEpiWarps][kEpiCols];
     __shared__ __align__(16) float epi_row[kEpiWarps][32];
     __shared__ unsigned long long cta_count;
 
@@ -382,7 +400,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     } else {
         // ------------------------------------------------ epilogue
         const uint32_t quad = warp & 3u;
-        const uint32_t half = (warp - 2) >> 2;  // columns [128 half, 128 half + 128)
+        const uint32_t half = (warp - 2) >> 2;  // columns [kEpiCols half, kEpiCols (half + 1))
         const uint32_t lane_base = (quad * 32u) << 16;
         float *snb = epi_nb[warp - 2];
         float *srow = epi_row[warp - 2];
@@ -401,12 +419,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         WorkItem w = it < p.n_items ? p.items[it] : WorkItem{0, 0, 0, 0};
         WorkItem wn = it + stride < p.n_items ? p.items[it + stride] : WorkItem{0, 0, 0, 0};
         uint32_t bt = w.b0;
-        float4 pf_nbv = make_float4(0, 0, 0, 0), pf_gmin = make_float4(0, 0, 0, 0);
+        float pf_nbv[kEpiVec], pf_gmin[kEpiVec];
+#pragma unroll
+        for (int q = 0; q < kEpiVec; ++q) pf_nbv[q] = pf_gmin[q] = 0.f;
         float pf_tmax = 0.f, pf_na = kPadNorm;
         auto prefetch = [&](const WorkItem &ww, uint32_t b) {
-            const uint64_t g = (uint64_t)b * kTcTileB + half * 128;
-            pf_nbv = __ldg(reinterpret_cast<const float4 *>(p.norm_b + g) + lane);
-            pf_gmin = __ldg(reinterpret_cast<const float4 *>(p.gmin_b + g / 32));
+            const uint64_t g = (uint64_t)b * kTcTileB + half * kEpiCols;
+            if constexpr (kEpiVec == 4) {
+                const float4 t = __ldg(reinterpret_cast<const float4 *>(p.norm_b + g) + lane);
+                const float4 m = __ldg(reinterpret_cast<const float4 *>(p.gmin_b + g / 32));
+                pf_nbv[0] = t.x, pf_nbv[1] = t.y, pf_nbv[2] = t.z, pf_nbv[3] = t.w;
+                pf_gmin[0] = m.x, pf_gmin[1] = m.y, pf_gmin[2] = m.z, pf_gmin[3] = m.w;
+            } else {
+                const float2 t = __ldg(reinterpret_cast<const float2 *>(p.norm_b + g) + lane);
+                const float2 m = __ldg(reinterpret_cast<const float2 *>(p.gmin_b + g / 32));
+                pf_nbv[0] = t.x, pf_nbv[1] = t.y;
+                pf_gmin[0] = m.x, pf_gmin[1] = m.y;
+            }
             pf_tmax = __ldg(p.tmax_b + b);
             const uint64_t r = (uint64_t)ww.a * kTcTileA + quad * 32 + lane;
             pf_na = r < p.na ? __ldg(p.norm_a + r) : kPadNorm;
@@ -416,7 +445,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             const uint64_t gi = (uint64_t)w.a * kTcTileA + quad * 32 + lane;
             const bool row_ok = gi < p.na;
             const float na = pf_na;
-            const float4 nbv = pf_nbv, gmin = pf_gmin;
+            float nbv[kEpiVec], gmin[kEpiVec];
+#pragma unroll
+            for (int q = 0; q < kEpiVec; ++q) nbv[q] = pf_nbv[q], gmin[q] = pf_gmin[q];
             const float tmaxb = pf_tmax;
             const uint32_t cur_bt = bt;
             // advance, and prefetch the next tile
@@ -431,7 +462,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (it < p.n_items) prefetch(w, bt);
             {
                 const uint32_t acc = t_cnt & 1u;
-                const uint64_t gj0 = (uint64_t)cur_bt * kTcTileB + half * 128;
+                const uint64_t gj0 = (uint64_t)cur_bt * kTcTileB + half * kEpiCols;
                 // With tau_max = c_rel (|a|^2 + max_tile |b|^2) + c_abs >= tau of every
                 // pair in the tile, and t_j = |b_j|^2 - 2 v_j, s_j = |a|^2 + t_j:
                 //   t_j <= thr_in  => s_j + tau <= eps^2  (certainly inside),
@@ -444,43 +475,55 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 float thr_in = (T_lo - tau_max) - na - marg;
                 if (!row_ok) thr_out = thr_in = -3.0e38f;
                 // columns that may be counted at all: gj < nb, and gj > gi for a self-join
-                int jlo = 0, jhi = 128;
+                int jlo = 0, jhi = kEpiCols;
                 {
                     const int64_t lim = (int64_t)p.nb - (int64_t)gj0;
-                    jhi = lim < 128 ? (lim < 0 ? 0 : (int)lim) : 128;
+                    jhi = lim < kEpiCols ? (lim < 0 ? 0 : (int)lim) : kEpiCols;
                     if (p.self) {
                         const int64_t first = (int64_t)gi + 1 - (int64_t)gj0;
-                        jlo = first > 0 ? (first > 128 ? 128 : (int)first) : 0;
+                        jlo = first > 0 ? (first > kEpiCols ? kEpiCols : (int)first) : 0;
                     }
                 }
                 mbar_wait(&bar_accfull[acc], (t_cnt >> 1) & 1u, err);
                 tc_fence_after();
-                reinterpret_cast<float4 *>(snb)[lane] = nbv;
+                if constexpr (kEpiVec == 4)
+                    reinterpret_cast<float4 *>(snb)[lane] = make_float4(nbv[0], nbv[1], nbv[2], nbv[3]);
+                else
+                    reinterpret_cast<float2 *>(snb)[lane] = make_float2(nbv[0], nbv[1]);
                 __syncwarp();
-#pragma unroll 1
-                for (uint32_t c = 0; c < 2; ++c) {
-                    float v[64];
-                    tmem_ld64(tmem + lane_base + acc * kTcTileB + half * 128 + c * 64, v);
+#pragma unroll
+                for (uint32_t c = 0; c < kEpiChunks; ++c) {
+                    float v[kChunkCols];
+                    const uint32_t taddr = tmem + lane_base + acc * kTcTileB + half * kEpiCols + c * kChunkCols;
+                    if constexpr (kChunkCols == 64)
+                        tmem_ld64(taddr, *reinterpret_cast<float(*)[64]>(v));
+                    else
+                        tmem_ld32(taddr, *reinterpret_cast<float(*)[32]>(v));
                     // max_j v_j per 32-column group: with the group's minimum norm,
                     // min_j (|b_j|^2 - 2 v_j) >= gmin - 2 max_j v_j
-                    float mx[8];
+                    float mg[kChunkGroups];
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) mx[q] = -3.0e38f;
+                    for (int g = 0; g < kChunkGroups; ++g) {
+                        float mx[4];
 #pragma unroll
-                    for (int j = 0; j < 64; ++j) mx[(j & 3) + (j >= 32 ? 4 : 0)] = fmaxf(mx[(j & 3) + (j >= 32 ? 4 : 0)], v[j]);
-                    const float g0 = c ? gmin.z : gmin.x, g1 = c ? gmin.w : gmin.y;
-                    const float mlo = fmaf(-2.0f, fmaxf(fmaxf(mx[0], mx[1]), fmaxf(mx[2], mx[3])), g0);
-                    const float mhi = fmaf(-2.0f, fmaxf(fmaxf(mx[4], mx[5]), fmaxf(mx[6], mx[7])), g1);
+                        for (int q = 0; q < 4; ++q) mx[q] = fmaxf(v[32 * g + q], v[32 * g + q + 4]);
 #pragma unroll
-                    for (int h2 = 0; h2 < 2; ++h2) {
+                        for (int j = 8; j < 32; j += 8)
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) mx[q] = fmax3(mx[q], v[32 * g + j + q], v[32 * g + j + q + 4]);
+                        mg[g] = fmaf(-2.0f, fmaxf(fmaxf(mx[0], mx[1]), fmaxf(mx[2], mx[3])),
+                                     gmin[c * kChunkGroups + g]);
+                    }
+#pragma unroll
+                    for (int h2 = 0; h2 < kChunkGroups; ++h2) {
                         // Rare: a 32-column half of some rows of the warp may hold a
                         // pair that is not certainly outside. For each such row the
                         // owning lane publishes its 32 values through shared memory
                         // and the whole warp classifies the 32 columns at once (lane
                         // = column), branch-free; band pairs are queued.
-                        const bool need = (h2 ? mhi : mlo) <= thr_out || (p.dbg != nullptr && row_ok);
+                        const bool need = mg[h2] <= thr_out || (p.dbg != nullptr && row_ok);
                         uint32_t rows = __ballot_sync(0xffffffffu, need);
-                        const int cb = (int)(c * 64 + h2 * 32);
+                        const int cb = (int)(c * kChunkCols + h2 * 32);
                         const float nbl = snb[cb + lane];
                         while (rows) {
                             const int L = __ffs(rows) - 1;
