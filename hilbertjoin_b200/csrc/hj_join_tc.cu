@@ -251,7 +251,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __shared__ __align__(8) uint64_t bar_afull[2], bar_aempty[2], bar_accfull[2], bar_accempty[2], bar_drain;
     __shared__ __align__(8) uint64_t bar_bfull[8], bar_bempty[8];
     __shared__ uint32_t tmem_base_sh;
-    __shared__ __align__(16) float epi_nb[kEpiWarps][kEpiCols];
     __shared__ __align__(16) float epi_row[kEpiWarps][32];
     __shared__ unsigned long long cta_count;
 
@@ -402,7 +401,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const uint32_t quad = warp & 3u;
         const uint32_t half = (warp - 2) >> 2;  // columns [kEpiCols half, kEpiCols (half + 1))
         const uint32_t lane_base = (quad * 32u) << 16;
-        float *snb = epi_nb[warp - 2];
         float *srow = epi_row[warp - 2];
         unsigned long long cnt = 0;
         uint32_t t_cnt = 0;
@@ -411,47 +409,64 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // part of c_rel. A pair is inside if s + tau <= T_lo, outside if
         // s - tau > T_hi, and in the band otherwise.
         const float T_lo = p.T_lo, T_hi = p.T_hi, crel = p.c_rel_f, cabs = p.c_abs_f;
-        // Flat walk over (item, B tile) with the next tile's norms, group minima
-        // and tile maximum (and the next item) loaded one step ahead, so that
-        // their memory latency overlaps the current tile.
+        // Walk over (item, B tile). Per item: this lane's row (A rank), its norm
+        // and the classification thresholds, taken against the largest B-tile
+        // norm of the item (a band at least as wide as any tile's: still
+        // exact). Per tile only the group minima are needed on the fast path;
+        // they are loaded one tile ahead so that their latency overlaps the
+        // current tile. B norms and column bounds are read on the slow path.
         const uint64_t stride = gridDim.x;
         uint64_t it = blockIdx.x;
         WorkItem w = it < p.n_items ? p.items[it] : WorkItem{0, 0, 0, 0};
         WorkItem wn = it + stride < p.n_items ? p.items[it + stride] : WorkItem{0, 0, 0, 0};
         uint32_t bt = w.b0;
-        float pf_nbv[kEpiVec], pf_gmin[kEpiVec];
-#pragma unroll
-        for (int q = 0; q < kEpiVec; ++q) pf_nbv[q] = pf_gmin[q] = 0.f;
-        float pf_tmax = 0.f, pf_na = kPadNorm;
-        auto prefetch = [&](const WorkItem &ww, uint32_t b) {
+        float pf_gmin[kEpiVec];
+        auto prefetch = [&](uint32_t b) {
             const uint64_t g = (uint64_t)b * kTcTileB + half * kEpiCols;
             if constexpr (kEpiVec == 4) {
-                const float4 t = __ldg(reinterpret_cast<const float4 *>(p.norm_b + g) + lane);
                 const float4 m = __ldg(reinterpret_cast<const float4 *>(p.gmin_b + g / 32));
-                pf_nbv[0] = t.x, pf_nbv[1] = t.y, pf_nbv[2] = t.z, pf_nbv[3] = t.w;
                 pf_gmin[0] = m.x, pf_gmin[1] = m.y, pf_gmin[2] = m.z, pf_gmin[3] = m.w;
             } else {
-                const float2 t = __ldg(reinterpret_cast<const float2 *>(p.norm_b + g) + lane);
                 const float2 m = __ldg(reinterpret_cast<const float2 *>(p.gmin_b + g / 32));
-                pf_nbv[0] = t.x, pf_nbv[1] = t.y;
                 pf_gmin[0] = m.x, pf_gmin[1] = m.y;
             }
-            pf_tmax = __ldg(p.tmax_b + b);
-            const uint64_t r = (uint64_t)ww.a * kTcTileA + quad * 32 + lane;
-            pf_na = r < p.na ? __ldg(p.norm_a + r) : kPadNorm;
         };
-        if (it < p.n_items) prefetch(w, bt);
-        while (it < p.n_items) {
-            const uint64_t gi = (uint64_t)w.a * kTcTileA + quad * 32 + lane;
-            const bool row_ok = gi < p.na;
-            const float na = pf_na;
-            float nbv[kEpiVec], gmin[kEpiVec];
 #pragma unroll
-            for (int q = 0; q < kEpiVec; ++q) nbv[q] = pf_nbv[q], gmin[q] = pf_gmin[q];
-            const float tmaxb = pf_tmax;
+        for (int q = 0; q < kEpiVec; ++q) pf_gmin[q] = 0.f;
+        if (it < p.n_items) prefetch(bt);
+        // per-item row state
+        uint64_t gi = 0;
+        bool row_ok = false;
+        float na = kPadNorm, thr_out = -3.0e38f, thr_in = -3.0e38f;
+        auto item_rows = [&](const WorkItem &ww) {
+            gi = (uint64_t)ww.a * kTcTileA + quad * 32 + lane;
+            row_ok = gi < p.na;
+            na = row_ok ? __ldg(p.norm_a + gi) : kPadNorm;
+            float tmaxb = 0.f;
+            for (uint32_t b = ww.b0 + lane; b < ww.b1; b += 32) tmaxb = fmaxf(tmaxb, __ldg(p.tmax_b + b));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) tmaxb = fmaxf(tmaxb, __shfl_xor_sync(0xffffffffu, tmaxb, o));
+            // With tau_max = c_rel (|a|^2 + max |b|^2) + c_abs >= tau of every pair
+            // of the item, and t_j = |b_j|^2 - 2 v_j, s_j = |a|^2 + t_j:
+            //   t_j <= thr_in  => s_j + tau <= eps^2  (certainly inside),
+            //   t_j >  thr_out => s_j - tau >  eps^2  (certainly outside),
+            // anything between is a band pair. Both thresholds carry margins
+            // for their own FP32 rounding (rounded inward / outward).
+            const float tau_max = fmaf(crel, na + tmaxb, cabs) * 1.001f;
+            const float marg = 8.0f * 5.9604645e-8f * (fabsf(T_hi) + fabsf(na) + tmaxb + tau_max);
+            thr_out = (T_hi + tau_max) - na + marg;
+            thr_in = (T_lo - tau_max) - na - marg;
+            if (!row_ok) thr_out = thr_in = -3.0e38f;
+        };
+        if (it < p.n_items) item_rows(w);
+        while (it < p.n_items) {
+            float gmin[kEpiVec];
+#pragma unroll
+            for (int q = 0; q < kEpiVec; ++q) gmin[q] = pf_gmin[q];
             const uint32_t cur_bt = bt;
-            // advance, and prefetch the next tile
-            if (bt + 1 < w.b1) {
+            // the item's rows stay for its last tile; the next item's are set after it
+            const bool last_tile = bt + 1 >= w.b1;
+            if (!last_tile) {
                 ++bt;
             } else {
                 it += stride;
@@ -459,38 +474,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 bt = w.b0;
                 wn = it + stride < p.n_items ? p.items[it + stride] : WorkItem{0, 0, 0, 0};
             }
-            if (it < p.n_items) prefetch(w, bt);
+            if (it < p.n_items) prefetch(bt);
             {
                 const uint32_t acc = t_cnt & 1u;
                 const uint64_t gj0 = (uint64_t)cur_bt * kTcTileB + half * kEpiCols;
-                // With tau_max = c_rel (|a|^2 + max_tile |b|^2) + c_abs >= tau of every
-                // pair in the tile, and t_j = |b_j|^2 - 2 v_j, s_j = |a|^2 + t_j:
-                //   t_j <= thr_in  => s_j + tau <= eps^2  (certainly inside),
-                //   t_j >  thr_out => s_j - tau >  eps^2  (certainly outside),
-                // anything between is a band pair. Both thresholds carry margins
-                // for their own FP32 rounding (rounded inward / outward).
-                const float tau_max = fmaf(crel, na + tmaxb, cabs) * 1.001f;
-                const float marg = 8.0f * 5.9604645e-8f * (fabsf(T_hi) + fabsf(na) + tmaxb + tau_max);
-                float thr_out = (T_hi + tau_max) - na + marg;
-                float thr_in = (T_lo - tau_max) - na - marg;
-                if (!row_ok) thr_out = thr_in = -3.0e38f;
-                // columns that may be counted at all: gj < nb, and gj > gi for a self-join
-                int jlo = 0, jhi = kEpiCols;
-                {
-                    const int64_t lim = (int64_t)p.nb - (int64_t)gj0;
-                    jhi = lim < kEpiCols ? (lim < 0 ? 0 : (int)lim) : kEpiCols;
-                    if (p.self) {
-                        const int64_t first = (int64_t)gi + 1 - (int64_t)gj0;
-                        jlo = first > 0 ? (first > kEpiCols ? kEpiCols : (int)first) : 0;
-                    }
-                }
                 mbar_wait(&bar_accfull[acc], (t_cnt >> 1) & 1u, err);
                 tc_fence_after();
-                if constexpr (kEpiVec == 4)
-                    reinterpret_cast<float4 *>(snb)[lane] = make_float4(nbv[0], nbv[1], nbv[2], nbv[3]);
-                else
-                    reinterpret_cast<float2 *>(snb)[lane] = make_float2(nbv[0], nbv[1]);
-                __syncwarp();
 #pragma unroll
                 for (uint32_t c = 0; c < kEpiChunks; ++c) {
                     float v[kChunkCols];
@@ -523,8 +512,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         // = column), branch-free; band pairs are queued.
                         const bool need = mg[h2] <= thr_out || (p.dbg != nullptr && row_ok);
                         uint32_t rows = __ballot_sync(0xffffffffu, need);
+                        if (!rows) continue;
                         const int cb = (int)(c * kChunkCols + h2 * 32);
-                        const float nbl = snb[cb + lane];
+                        const float nbl = __ldg(p.norm_b + gj0 + cb + lane);
+                        // columns that may be counted at all: gj < nb, and gj > gi for a self-join
+                        int jlo = 0, jhi = kEpiCols;
+                        {
+                            const int64_t lim = (int64_t)p.nb - (int64_t)gj0;
+                            jhi = lim < kEpiCols ? (lim < 0 ? 0 : (int)lim) : kEpiCols;
+                            if (p.self) {
+                                const int64_t first = (int64_t)gi + 1 - (int64_t)gj0;
+                                jlo = first > 0 ? (first > kEpiCols ? kEpiCols : (int)first) : 0;
+                            }
+                        }
                         while (rows) {
                             const int L = __ffs(rows) - 1;
                             rows &= rows - 1;
@@ -568,6 +568,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 if (lane == 0) mbar_arrive(&bar_accempty[acc]);
                 ++t_cnt;
             }
+            if (last_tile && it < p.n_items) item_rows(w);
         }
         cnt = warp_sum_u64(cnt);
         if (lane == 0 && cnt) atomicAdd(&cta_count, cnt);
