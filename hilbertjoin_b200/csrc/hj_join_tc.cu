@@ -703,12 +703,12 @@ static TcLayout tc_layout(int form, uint32_t d) {
     L.ka = form == HJ_FORM_TC_TF32 ? (d + 31) / 32 : (d + 63) / 64;
     const uint32_t a_atoms = form == HJ_FORM_TC_BF16X3 ? 2 * L.ka : L.ka;
     const size_t a_bytes = (size_t)a_atoms * kAStageBytes;
-    const size_t budget = 216 * 1024;  // + 1 KB alignment + ~5 KB static smem <= 227 KB per block
+    const size_t budget = 224 * 1024;  // + 1 KB alignment + ~1.3 KB static smem <= 227 KB per block
     L.a_bufs = 2 * a_bytes + 3 * kBStageBytes <= budget ? 2 : 1;
     size_t left = budget - L.a_bufs * a_bytes;
     L.nst = (uint32_t)(left / kBStageBytes);
     if (L.nst > 8) L.nst = 8;
-    L.smem = L.a_bufs * a_bytes + (size_t)L.nst * kBStageBytes + 1024;  // <= 217 KB
+    L.smem = L.a_bufs * a_bytes + (size_t)L.nst * kBStageBytes + 1024;  // <= 225 KB
     return L;
 }
 
@@ -778,13 +778,13 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, bool self, uint64_t n
     uint64_t grid = (uint64_t)num_sms;
     if (grid > idx.n_items) grid = idx.n_items;
     if (tp.form == HJ_FORM_TC_TF32) {
-        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_TF32>, 217 * 1024);
+        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_TF32>, 225 * 1024);
         k_join_tc<HJ_FORM_TC_TF32><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
     } else if (tp.form == HJ_FORM_TC_FP16) {
-        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_FP16>, 217 * 1024);
+        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_FP16>, 225 * 1024);
         k_join_tc<HJ_FORM_TC_FP16><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
     } else {
-        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_BF16X3>, 217 * 1024);
+        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_BF16X3>, 225 * 1024);
         k_join_tc<HJ_FORM_TC_BF16X3><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
     }
     cudaError_t e = cudaGetLastError();
