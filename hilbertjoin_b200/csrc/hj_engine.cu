@@ -44,6 +44,8 @@ struct Ctx {
     cudaEvent_t ev[8] = {};
     unsigned long long *d_small = nullptr;  // [16] counters
     unsigned long long *h_small = nullptr;  // pinned [16]
+    TcJob *h_job = nullptr;                 // pinned: the job table of a single join
+    TcJob *d_job = nullptr;
     bool ok = false;
 };
 
@@ -118,7 +120,9 @@ static int get_ctx(int device, Ctx **out) {
     for (auto &e : c->ev) cudaEventCreate(&e);
     cudaMalloc(&c->d_small, 16 * sizeof(unsigned long long));
     cudaMallocHost(&c->h_small, 16 * sizeof(unsigned long long));
-    if (!c->d_small || !c->h_small) return fail(HJ_ERR_OOM, "context allocation failed");
+    cudaMallocHost(&c->h_job, sizeof(TcJob));
+    cudaMalloc(&c->d_job, sizeof(TcJob));
+    if (!c->d_small || !c->h_small || !c->h_job || !c->d_job) return fail(HJ_ERR_OOM, "context allocation failed");
     c->ok = true;
     tl_ctx[dev] = c;
     *out = c;
@@ -528,10 +532,11 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
         cudaEventRecord(c->ev[5], st);
     } else {
         // the FP16 form works in scaled units: norms, eps^2 and the bound times op_scale^2
-        const double s2 = A.op_scale * A.op_scale;
-        tc_band_constants(form, d, maxabs, &c_rel, &c_abs);
-        const double T_tc = T * s2;
-        TcParams p{form, T_tc, c_rel, c_abs};
+        // one-entry job table: counted ranks, thresholds and bound in the operand units
+        fill_tc_job(c->h_job, form, d, T, A.op_scale, maxabs, 0, na_eff, 0, nb_eff, in.self, d_count, A.rows,
+                    B.rows, &c_rel, &c_abs);
+        cudaMemcpyAsync(c->d_job, c->h_job, sizeof(TcJob), cudaMemcpyHostToDevice, st);
+        const double T_tc = T * A.op_scale * A.op_scale;
         // Items whose error band would exceed half of eps^2 (eps^2 tiny against
         // the squared norms: the cancellation limit of the norm expansion) run
         // on the FP64 kernel instead.
@@ -570,7 +575,7 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
                 cudaMemsetAsync(d_band, 0, 2 * sizeof(unsigned long long), st);
                 std::string terr;
                 cudaEventRecord(c->ev[6], st);
-                if (launch_join_tc(A, B, in.self, na_eff, nb_eff, p, idx_tc, d_count, band, cap, d_band, d_err,
+                if (launch_join_tc(A, B, form, c->d_job, na_eff, nb_eff, idx_tc, band, cap, d_band, d_err,
                                    c->num_sms, st, &terr))
                     return fail(HJ_ERR_CUDA, terr);
                 ++launches;
@@ -579,7 +584,7 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
                 if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("tensor-core join");
                 band_total = c->h_small[4];
                 if (band_total <= cap) {
-                    launch_recheck(A, B, T, band, d_band, cap, d_count,
+                    launch_recheck(c->d_job, A.dtype_bytes, band, d_band, cap,
                                    reinterpret_cast<unsigned int *>(c->d_small + 5), st);
                     ++launches;
                     cudaEventRecord(c->ev[5], st);

@@ -203,23 +203,43 @@ void launch_pairs_fp64(const SortedSet &A, const SortedSet &B, bool self, uint64
                        double T, const IndexResult &idx, uint32_t *item_cnt, uint32_t *out_i, uint32_t *out_j,
                        uint32_t *d_err, int num_sms, cudaStream_t st);
 
-// Tensor-core kernel + FP64 recheck of the band. Adds into *d_count; band pair
-// count into *d_band_total (may exceed `band_cap`: then the caller regrows).
-struct TcParams {
-    int form;             // HJ_FORM_TC_TF32, HJ_FORM_TC_BF16X3 or HJ_FORM_TC_FP16
-    double T;             // eps * eps (FP16 form: times op_scale^2, the units of the norms)
-    double c_rel;         // band half-width: c_rel * (|a|^2 + |b|^2) + c_abs
-    double c_abs;
-};
-// Band entries are 16 bytes (kBandEntryBytes).
+// Tensor-core kernel + FP64 recheck of the band. Adds into each job's count;
+// band pair count into *d_band_total (may exceed `band_cap`: then the caller
+// regrows). Band entries are 16 bytes (kBandEntryBytes).
 constexpr size_t kBandEntryBytes = 16;
-int launch_join_tc(const SortedSet &A, const SortedSet &B, bool self, uint64_t na_eff, uint64_t nb_eff,
-                   const TcParams &p, const IndexResult &idx, unsigned long long *d_count, uint2 *band,
-                   uint64_t band_cap, unsigned long long *d_band_total, uint32_t *d_err, int num_sms,
-                   cudaStream_t st, std::string *err);
-void launch_recheck(const SortedSet &A, const SortedSet &B, double T, const uint2 *band,
-                    const unsigned long long *d_band_total, uint64_t band_cap, unsigned long long *d_count,
-                    unsigned int *d_max_err_bits, cudaStream_t st);
+// One join of a tensor-core launch. A launch runs the work items of one or
+// more jobs (WorkItem.pad = job index) over operand matrices whose rows hold
+// all jobs' sets; rows are global ranks of those matrices.
+struct TcJob {
+    uint64_t a_row0, a_end;       // counted A ranks: [a_row0, a_end)
+    uint64_t b_row0, b_end;       // counted B ranks: [b_row0, b_end)
+    double T;                     // eps^2 (FP64), for the recheck
+    unsigned long long *count;    // where the job's count accumulates
+    const void *rows_a, *rows_b;  // sorted rows (input precision); rank r at (r - row0) * d
+    float T_lo, T_hi;             // eps^2 in operand units, rounded down / up to FP32
+    float c_rel_f, c_abs_f;       // error bound constants, rounded up to FP32
+    float s_unscale;              // 1 / op_scale^2 (exact): estimates back to the caller's units
+    uint32_t self;                // unordered pairs within one set (A = B)
+    uint32_t ka;                  // K atoms of this job's operands
+    uint32_t d;
+};
+// Fills a job for form `form`, dimension d, eps^2 = T, FP16 operand scale
+// op_scale (1 for other forms), largest |coordinate| maxabs. Returns the
+// error-bound constants through c_rel / c_abs (operand units) if non-null.
+void fill_tc_job(TcJob *j, int form, uint32_t d, double T, double op_scale, double maxabs, uint64_t a_row0,
+                 uint64_t na_eff, uint64_t b_row0, uint64_t nb_eff, bool self, unsigned long long *count,
+                 const void *rows_a, const void *rows_b, double *c_rel, double *c_abs);
+
+// Launches the tensor-core kernel over `idx` with the job table d_jobs (device).
+// A and B describe the operand matrices (layout pointers, npad_tc rows, kpad,
+// norms and their tile maxima and group minima); their d is the largest of the
+// jobs'. na0 / nb0: job 0's counted ranks (debug output only).
+int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob *d_jobs, uint64_t na0, uint64_t nb0,
+                   const IndexResult &idx, uint2 *band, uint64_t band_cap, unsigned long long *d_band_total,
+                   uint32_t *d_err, int num_sms, cudaStream_t st, std::string *err);
+// FP64 recheck of the band pairs, each against its job's rows and eps^2.
+void launch_recheck(const TcJob *d_jobs, int dtype_bytes, const uint2 *band, const unsigned long long *d_band_total,
+                    uint64_t band_cap, unsigned int *d_max_err_bits, cudaStream_t st);
 // Test hook: when non-null, the tensor-core kernel writes its dist^2 estimate
 // of every pair to dbg[ia * nb + jb] (EGO ranks). Not thread-safe.
 void set_tc_debug_output(float *dbg);

@@ -75,7 +75,7 @@ struct BandEntry {
 };
 
 struct TcArgs {
-    uint32_t ka;        // K atoms per operand (TF32: kpad/32; BF16: kpad16/64)
+    uint32_t ka;        // K atoms per operand buffer, the largest of the jobs' (TF32: kpad/32; BF16, FP16: kpad16/64)
     uint32_t a_bufs;    // 1 or 2 A buffers
     uint32_t nst;       // B ring stages
     const WorkItem *items;
@@ -83,17 +83,12 @@ struct TcArgs {
     const float *norm_a, *norm_b;   // FP32 |x|^2 per EGO rank (padding: kPadNorm)
     const float *tmax_b;            // per 256-rank B tile: max |x|^2
     const float *gmin_b;            // per 32-rank B group: min |x|^2
-    uint64_t na, nb;                // ranks counted
-    int self;
-    double T, c_rel, c_abs;
-    float T_lo, T_hi;      // eps^2 rounded down / up to FP32
-    float c_rel_f, c_abs_f;  // rounded up to FP32
-    unsigned long long *count;
+    const TcJob *jobs;              // per job: counted rows, thresholds, count (item.pad = job)
+    uint64_t na, nb;                // job 0's counted ranks (debug output only)
     BandEntry *band;
     uint64_t band_cap;
     unsigned long long *band_total;
     uint32_t *err;
-    float s_unscale;                // 1 / op_scale^2: s_hat back to the caller's units (band, dbg)
     float *dbg;                     // optional: s_hat for every pair, input order [na][nb] (tests)
     const uint32_t *perm_a, *perm_b;  // EGO rank -> input index (for dbg)
 };
@@ -244,7 +239,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     constexpr bool kBf = FORM == HJ_FORM_TC_BF16X3;
     constexpr int32_t kAtomElems = FORM == HJ_FORM_TC_TF32 ? 32 : 64;  // K elements per 128-byte atom
     const uint32_t a_atoms = kBf ? 2 * p.ka : p.ka;
-    const uint32_t b_atoms = a_atoms;
     const uint32_t a_buf_bytes = a_atoms * kAStageBytes;
 
     extern __shared__ unsigned char smem_raw[];
@@ -252,7 +246,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     __shared__ __align__(8) uint64_t bar_bfull[8], bar_bempty[8];
     __shared__ uint32_t tmem_base_sh;
     __shared__ __align__(16) float epi_row[kEpiWarps][32];
-    __shared__ unsigned long long cta_count;
 
     const uint32_t smem_base = (smem_u32(smem_raw) + 1023u) & ~1023u;
     const uint32_t a_base = smem_base;
@@ -272,7 +265,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             mbar_init(&bar_bempty[i], 1);
         }
         mbar_init(&bar_drain, 1);
-        cta_count = 0;
         fence_barrier_init();
     }
     if (warp == 0) {
@@ -297,19 +289,21 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             uint32_t a_cnt = 0, b_cnt = 0;
             for (uint64_t it = blockIdx.x; it < p.n_items; it += gridDim.x) {
                 const WorkItem w = p.items[it];
+                const uint32_t ka = p.jobs[w.pad].ka;  // this job's K atoms (<= p.ka)
+                const uint32_t ja_atoms = kBf ? 2 * ka : ka;
                 const uint32_t abuf = a_cnt % p.a_bufs, au = a_cnt / p.a_bufs;
                 if (au >= 1) mbar_wait(&bar_aempty[abuf], (au - 1) & 1u, err);
-                mbar_arrive_expect_tx(&bar_afull[abuf], a_buf_bytes);
+                mbar_arrive_expect_tx(&bar_afull[abuf], ja_atoms * kAStageBytes);
                 const uint32_t adst = a_base + abuf * a_buf_bytes;
-                for (uint32_t q = 0; q < a_atoms; ++q) {
-                    const bool lo = kBf && q >= p.ka;
-                    const uint32_t kq = kBf ? (lo ? q - p.ka : q) : q;
+                for (uint32_t q = 0; q < ja_atoms; ++q) {
+                    const bool lo = kBf && q >= ka;
+                    const uint32_t kq = kBf ? (lo ? q - ka : q) : q;
                     tma_load_2d(smem_raw + (adst + q * kAStageBytes - smem_u32(smem_raw)), lo ? &tm_a2 : &tm_a,
                                 (int32_t)(kq * kAtomElems), (int32_t)(w.a * kTcTileA), &bar_afull[abuf]);
                 }
                 ++a_cnt;
                 for (uint32_t bt = w.b0; bt < w.b1; ++bt) {
-                    for (uint32_t q = 0; q < b_atoms; ++q) {
+                    for (uint32_t q = 0; q < ja_atoms; ++q) {
                         const uint32_t s = b_cnt % p.nst, u = b_cnt / p.nst;
                         if (u >= 1) mbar_wait(&bar_bempty[s], (u - 1) & 1u, err);
                         mbar_arrive_expect_tx(&bar_bfull[s], kBStageBytes);
@@ -337,6 +331,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             bool issued_any = false;
             for (uint64_t it = blockIdx.x; it < p.n_items; it += gridDim.x) {
                 const WorkItem w = p.items[it];
+                const uint32_t ka = p.jobs[w.pad].ka;
+                const uint32_t jb_atoms = kBf ? 2 * ka : ka;
                 const uint32_t abuf = a_cnt % p.a_bufs, au = a_cnt / p.a_bufs;
                 mbar_wait(&bar_afull[abuf], au & 1u, err);
                 tc_fence_after();
@@ -347,7 +343,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     tc_fence_after();
                     const uint32_t dcol = tmem + acc * kTcTileB;
                     uint32_t accumulate = 0;
-                    for (uint32_t q = 0; q < b_atoms; ++q) {
+                    for (uint32_t q = 0; q < jb_atoms; ++q) {
                         const uint32_t s = b_cnt % p.nst;
                         mbar_wait(&bar_bfull[s], (b_cnt / p.nst) & 1u, err);
                         tc_fence_after();
@@ -363,7 +359,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         } else {
                             const uint32_t kq = q >> 1;
                             const uint32_t a_hi = abase + kq * kAStageBytes;
-                            const uint32_t a_lo = abase + (p.ka + kq) * kAStageBytes;
+                            const uint32_t a_lo = abase + (ka + kq) * kAStageBytes;
                             if ((q & 1u) == 0) {  // B_hi atom: A_hi.B_hi + A_lo.B_hi
 #pragma unroll
                                 for (uint32_t kk = 0; kk < 4; ++kk) {
@@ -408,7 +404,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // and the bound rounded up; the FP32 rounding of the epilogue itself is
         // part of c_rel. A pair is inside if s + tau <= T_lo, outside if
         // s - tau > T_hi, and in the band otherwise.
-        const float T_lo = p.T_lo, T_hi = p.T_hi, crel = p.c_rel_f, cabs = p.c_abs_f;
         // Walk over (item, B tile). Per item: this lane's row (A rank), its norm
         // and the classification thresholds, taken against the largest B-tile
         // norm of the item (a band at least as wide as any tile's: still
@@ -434,13 +429,28 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 #pragma unroll
         for (int q = 0; q < kEpiVec; ++q) pf_gmin[q] = 0.f;
         if (it < p.n_items) prefetch(bt);
-        // per-item row state
-        uint64_t gi = 0;
-        bool row_ok = false;
-        float na = kPadNorm, thr_out = -3.0e38f, thr_in = -3.0e38f;
+        // per-item row state, and the job whose count the warp is accumulating
+        uint64_t gi = 0, b_end = 0;
+        bool row_ok = false, self = false;
+        float na = kPadNorm, thr_out = -3.0e38f, thr_in = -3.0e38f, s_unscale = 1.f;
+        uint32_t job = 0xffffffffu;
+        auto flush = [&]() {
+            const unsigned long long wc = warp_sum_u64(cnt);
+            if (lane == 0 && wc) atomicAdd(p.jobs[job].count, wc);
+            cnt = 0;
+        };
         auto item_rows = [&](const WorkItem &ww) {
+            if (ww.pad != job) {
+                if (job != 0xffffffffu) flush();
+                job = ww.pad;
+            }
+            const TcJob &J = p.jobs[job];
+            const float T_lo = J.T_lo, T_hi = J.T_hi, crel = J.c_rel_f, cabs = J.c_abs_f;
+            b_end = J.b_end;
+            self = J.self != 0;
+            s_unscale = J.s_unscale;
             gi = (uint64_t)ww.a * kTcTileA + quad * 32 + lane;
-            row_ok = gi < p.na;
+            row_ok = gi >= J.a_row0 && gi < J.a_end;
             na = row_ok ? __ldg(p.norm_a + gi) : kPadNorm;
             float tmaxb = 0.f;
             for (uint32_t b = ww.b0 + lane; b < ww.b1; b += 32) tmaxb = fmaxf(tmaxb, __ldg(p.tmax_b + b));
@@ -518,9 +528,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         // columns that may be counted at all: gj < nb, and gj > gi for a self-join
                         int jlo = 0, jhi = kEpiCols;
                         {
-                            const int64_t lim = (int64_t)p.nb - (int64_t)gj0;
+                            const int64_t lim = (int64_t)b_end - (int64_t)gj0;
                             jhi = lim < kEpiCols ? (lim < 0 ? 0 : (int)lim) : kEpiCols;
-                            if (p.self) {
+                            if (self) {
                                 const int64_t first = (int64_t)gi + 1 - (int64_t)gj0;
                                 jlo = first > 0 ? (first > kEpiCols ? kEpiCols : (int)first) : 0;
                             }
@@ -544,18 +554,19 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                             const uint64_t giL = gi - (uint64_t)lane + (uint64_t)L;
                             const float t = fmaf(-2.0f, srow[lane], nbl);
                             const int col = cb + (int)lane;
-                            const bool ok = (unsigned)(col - jloL) < (unsigned)(jhiL - jloL) && giL < p.na;
+                            const bool rokL = __shfl_sync(0xffffffffu, row_ok, L);
+                            const bool ok = (unsigned)(col - jloL) < (unsigned)(jhiL - jloL) && rokL;
                             cnt += (ok && t <= tinL) ? 1ull : 0ull;
                             if (p.dbg != nullptr && giL < p.na && gj0 + col < p.nb)
-                                p.dbg[(uint64_t)p.perm_a[giL] * p.nb + p.perm_b[gj0 + col]] = (naL + t) * p.s_unscale;
+                                p.dbg[(uint64_t)p.perm_a[giL] * p.nb + p.perm_b[gj0 + col]] = (naL + t) * s_unscale;
                             if (ok && t > tinL && t <= toutL) {  // band pair: very rare
                                 const unsigned long long k = atomicAdd(p.band_total, 1ull);
                                 if (k < p.band_cap) {
                                     BandEntry e;
                                     e.ia = (uint32_t)giL;
                                     e.jb = (uint32_t)(gj0 + col);
-                                    e.s_hat = (naL + t) * p.s_unscale;
-                                    e.pad = 0;
+                                    e.s_hat = (naL + t) * s_unscale;
+                                    e.pad = job;
                                     p.band[k] = e;
                                 }
                             }
@@ -570,46 +581,56 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             }
             if (last_tile && it < p.n_items) item_rows(w);
         }
-        cnt = warp_sum_u64(cnt);
-        if (lane == 0 && cnt) atomicAdd(&cta_count, cnt);
+        if (job != 0xffffffffu) flush();
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     if (warp == 0) tmem_dealloc(tmem, kTmemCols);
-    if (threadIdx.x == 0 && cta_count) atomicAdd(p.count, cta_count);
+
 }
 
 // ---------------------------------------------------------------- recheck
 
-// FP64 pair test (the oracle's) on every band pair; also the largest
-// |s_hat - dist2| seen, as FP32 bits in max_err_bits.
+// FP64 pair test (the oracle's) on every band pair, against the pair's job
+// (BandEntry.pad); also the largest |s_hat - dist2| seen, as FP32 bits in
+// max_err_bits.
 template <typename TIn>
-__global__ void k_recheck(const TIn *__restrict__ ra, const TIn *__restrict__ rb, uint32_t d, double T,
-                          const BandEntry *__restrict__ band, const unsigned long long *band_total, uint64_t cap,
-                          unsigned long long *count, unsigned int *max_err_bits) {
+__global__ void k_recheck(const TcJob *__restrict__ jobs, const BandEntry *__restrict__ band,
+                          const unsigned long long *band_total, uint64_t cap, unsigned int *max_err_bits) {
     const uint64_t n = min((unsigned long long)cap, *band_total);
-    unsigned long long c = 0;
+    const uint32_t lane = threadIdx.x & 31u;
     float emax = 0.f;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const BandEntry e = band[i];
-        const TIn *a = ra + (uint64_t)e.ia * d;
-        const TIn *b = rb + (uint64_t)e.jb * d;
-        double acc = 0.0;
-        for (uint32_t k = 0; k < d; ++k) {
-            const double df = __dsub_rn((double)a[k], (double)b[k]);
-            acc = __fma_rn(df, df, acc);
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < n; i0 += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = i0 + threadIdx.x;
+        unsigned long long c = 0;
+        uint32_t job = 0xffffffffu;
+        if (i < n) {
+            const BandEntry e = band[i];
+            job = e.pad;
+            const TcJob &J = jobs[job];
+            const TIn *a = static_cast<const TIn *>(J.rows_a) + (uint64_t)(e.ia - J.a_row0) * J.d;
+            const TIn *b = static_cast<const TIn *>(J.rows_b) + (uint64_t)(e.jb - J.b_row0) * J.d;
+            double acc = 0.0;
+            for (uint32_t k = 0; k < J.d; ++k) {
+                const double df = __dsub_rn((double)a[k], (double)b[k]);
+                acc = __fma_rn(df, df, acc);
+            }
+            c = acc <= J.T ? 1ull : 0ull;
+            emax = fmaxf(emax, (float)fabs((double)e.s_hat - acc));
         }
-        c += acc <= T ? 1ull : 0ull;
-        emax = fmaxf(emax, (float)fabs((double)e.s_hat - acc));
+        // one atomic per warp when the warp's entries share a job (the usual case)
+        const uint32_t j0 = __shfl_sync(0xffffffffu, job, 0);
+        if (__all_sync(0xffffffffu, job == j0 || job == 0xffffffffu)) {
+            c = warp_sum_u64(c);
+            if (lane == 0 && c) atomicAdd(jobs[j0].count, c);
+        } else if (c) {
+            atomicAdd(jobs[job].count, c);
+        }
     }
-    c = warp_sum_u64(c);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) emax = fmaxf(emax, __shfl_xor_sync(0xffffffffu, emax, o));
-    if ((threadIdx.x & 31u) == 0) {
-        if (c) atomicAdd(count, c);
-        atomicMax(max_err_bits, __float_as_uint(emax));
-    }
+    if (lane == 0) atomicMax(max_err_bits, __float_as_uint(emax));
 }
 
 // ---------------------------------------------------------------- host side
@@ -714,23 +735,52 @@ static TcLayout tc_layout(int form, uint32_t d) {
 
 static float *g_dbg_out = nullptr;  // set by tests through hj_debug_tc_estimates
 
-int launch_join_tc(const SortedSet &A, const SortedSet &B, bool self, uint64_t na_eff, uint64_t nb_eff,
-                   const TcParams &tp, const IndexResult &idx, unsigned long long *d_count, uint2 *band,
-                   uint64_t band_cap, unsigned long long *d_band_total, uint32_t *d_err, int num_sms, cudaStream_t st,
-                   std::string *err) {
+void fill_tc_job(TcJob *j, int form, uint32_t d, double T, double op_scale, double maxabs, uint64_t a_row0,
+                 uint64_t na_eff, uint64_t b_row0, uint64_t nb_eff, bool self, unsigned long long *count,
+                 const void *rows_a, const void *rows_b, double *c_rel_out, double *c_abs_out) {
+    double c_rel = 0, c_abs = 0;
+    tc_band_constants(form, d, maxabs, &c_rel, &c_abs);
+    const double s2 = op_scale * op_scale;  // FP16: the units of the norms; 1 otherwise
+    const double T_tc = T * s2;
+    memset(j, 0, sizeof(*j));
+    j->a_row0 = a_row0;
+    j->a_end = a_row0 + na_eff;
+    j->b_row0 = b_row0;
+    j->b_end = b_row0 + nb_eff;
+    j->T = T;
+    j->count = count;
+    j->rows_a = rows_a;
+    j->rows_b = rows_b;
+    const float t = (float)T_tc;  // outward rounding of eps^2 and upward rounding of the bound
+    j->T_lo = (double)t <= T_tc ? t : std::nextafter(t, -INFINITY);
+    j->T_hi = (double)t >= T_tc ? t : std::nextafter(t, INFINITY);
+    const float cr = (float)c_rel, ca = (float)c_abs;
+    j->c_rel_f = (double)cr >= c_rel ? cr : std::nextafter(cr, INFINITY);
+    j->c_abs_f = (double)ca >= c_abs ? ca : std::nextafter(ca, INFINITY);
+    j->s_unscale = (float)(1.0 / s2);  // a power of two: exact
+    j->self = self ? 1u : 0u;
+    j->ka = tc_layout(form, d).ka;
+    j->d = d;
+    if (c_rel_out) *c_rel_out = c_rel;
+    if (c_abs_out) *c_abs_out = c_abs;
+}
+
+int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob *d_jobs, uint64_t na0, uint64_t nb0,
+                   const IndexResult &idx, uint2 *band, uint64_t band_cap, unsigned long long *d_band_total,
+                   uint32_t *d_err, int num_sms, cudaStream_t st, std::string *err) {
     if (idx.n_items == 0) return 0;
-    const TcLayout L = tc_layout(tp.form, A.d);
+    const TcLayout L = tc_layout(form, A.d);
     if (L.nst < 2) {
         *err = "dimension too large for the tensor-core kernel";
         return 1;
     }
     CUtensorMap ma, ma2, mb, mb2;
-    if (tp.form == HJ_FORM_TC_TF32) {
+    if (form == HJ_FORM_TC_TF32) {
         if (!make_map(&ma, A.tf32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, A.npad_tc, A.kpad_tf32, kTcTileA, err)) return 1;
         if (!make_map(&mb, B.tf32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, B.npad_tc, B.kpad_tf32, kTcTileB, err)) return 1;
         ma2 = ma;
         mb2 = mb;
-    } else if (tp.form == HJ_FORM_TC_FP16) {
+    } else if (form == HJ_FORM_TC_FP16) {
         if (!make_map(&ma, A.bf_hi, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, A.npad_tc, A.kpad_bf16, kTcTileA, err)) return 1;
         if (!make_map(&mb, B.bf_hi, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, B.npad_tc, B.kpad_bf16, kTcTileB, err)) return 1;
         ma2 = ma;
@@ -743,6 +793,7 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, bool self, uint64_t n
         if (!make_map(&mb2, B.bf_lo, t, B.npad_tc, B.kpad_bf16, kTcTileB, err)) return 1;
     }
     TcArgs a;
+    memset(&a, 0, sizeof(a));
     a.ka = L.ka;
     a.a_bufs = L.a_bufs;
     a.nst = L.nst;
@@ -752,35 +803,22 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, bool self, uint64_t n
     a.norm_b = B.norms;
     a.tmax_b = B.tile_maxnorm_b;
     a.gmin_b = B.group_minnorm;
-    a.na = na_eff;
-    a.nb = nb_eff;
-    a.self = self ? 1 : 0;
-    a.T = tp.T;
-    a.c_rel = tp.c_rel;
-    a.c_abs = tp.c_abs;
-    {
-        float t = (float)tp.T;  // outward rounding of eps^2 and upward rounding of the bound
-        a.T_lo = (double)t <= tp.T ? t : std::nextafter(t, -INFINITY);
-        a.T_hi = (double)t >= tp.T ? t : std::nextafter(t, INFINITY);
-        float cr = (float)tp.c_rel, ca = (float)tp.c_abs;
-        a.c_rel_f = (double)cr >= tp.c_rel ? cr : std::nextafter(cr, INFINITY);
-        a.c_abs_f = (double)ca >= tp.c_abs ? ca : std::nextafter(ca, INFINITY);
-    }
-    a.count = d_count;
+    a.jobs = d_jobs;
+    a.na = na0;
+    a.nb = nb0;
     a.band = reinterpret_cast<BandEntry *>(band);
     a.band_cap = band_cap;
     a.band_total = d_band_total;
     a.err = d_err;
-    a.s_unscale = (float)(1.0 / (A.op_scale * A.op_scale));  // a power of two: exact
     a.dbg = g_dbg_out;
     a.perm_a = A.perm;
     a.perm_b = B.perm;
     uint64_t grid = (uint64_t)num_sms;
     if (grid > idx.n_items) grid = idx.n_items;
-    if (tp.form == HJ_FORM_TC_TF32) {
+    if (form == HJ_FORM_TC_TF32) {
         ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_TF32>, 225 * 1024);
         k_join_tc<HJ_FORM_TC_TF32><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
-    } else if (tp.form == HJ_FORM_TC_FP16) {
+    } else if (form == HJ_FORM_TC_FP16) {
         ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_FP16>, 225 * 1024);
         k_join_tc<HJ_FORM_TC_FP16><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
     } else {
@@ -795,17 +833,13 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, bool self, uint64_t n
     return 0;
 }
 
-void launch_recheck(const SortedSet &A, const SortedSet &B, double T, const uint2 *band,
-                    const unsigned long long *d_band_total, uint64_t band_cap, unsigned long long *d_count,
-                    unsigned int *d_max_err_bits, cudaStream_t st) {
+void launch_recheck(const TcJob *d_jobs, int dtype_bytes, const uint2 *band, const unsigned long long *d_band_total,
+                    uint64_t band_cap, unsigned int *d_max_err_bits, cudaStream_t st) {
     const BandEntry *b = reinterpret_cast<const BandEntry *>(band);
-    if (A.dtype_bytes == 8)
-        k_recheck<double><<<1184, 256, 0, st>>>(static_cast<const double *>(A.rows),
-                                                static_cast<const double *>(B.rows), A.d, T, b, d_band_total, band_cap,
-                                                d_count, d_max_err_bits);
+    if (dtype_bytes == 8)
+        k_recheck<double><<<1184, 256, 0, st>>>(d_jobs, b, d_band_total, band_cap, d_max_err_bits);
     else
-        k_recheck<float><<<1184, 256, 0, st>>>(static_cast<const float *>(A.rows), static_cast<const float *>(B.rows),
-                                               A.d, T, b, d_band_total, band_cap, d_count, d_max_err_bits);
+        k_recheck<float><<<1184, 256, 0, st>>>(d_jobs, b, d_band_total, band_cap, d_max_err_bits);
 }
 
 void set_tc_debug_output(float *dbg) { g_dbg_out = dbg; }
