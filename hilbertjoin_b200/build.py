@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "lib", "libhj.so")
 BIN = os.path.join(HERE, "bin")
 
 CU_SOURCES = ["hj_engine.cu", "hj_prep.cu", "hj_index.cu", "hj_join_fp64.cu", "hj_join_tc.cu", "hj_server.cu",
-              "hj_noalloc.cu"]
+              "hj_noalloc.cu", "hj_batch.cu"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
               "--expt-relaxed-constexpr"]

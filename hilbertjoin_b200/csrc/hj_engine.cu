@@ -916,6 +916,50 @@ static int dim_order_host(const double *pts, uint64_t n, uint32_t d, double eps,
     return HJ_OK;
 }
 
+int engine_fail(int code, const std::string &msg) { return fail(code, msg); }
+
+int engine_prepare_job(cudaStream_t st_in, const void *a, const void *b, uint64_t na, uint64_t nb, int dtype_bytes,
+                       uint32_t d, double eps, bool self, const hj_opts *opts, int form, PreparedJob *out) {
+    if (!form_is_tc(form)) return fail(HJ_ERR_INVALID_ARG, "a batch runs a tensor-core form");
+    if (dtype_bytes != 4 && dtype_bytes != 8) return fail(HJ_ERR_INVALID_ARG, "dtype_bytes must be 4 or 8");
+    if (!a || (!self && !b) || na == 0 || (!self && nb == 0)) return fail(HJ_ERR_INVALID_ARG, "empty or null job");
+    if (int r = validate(na, nb, d, eps)) return r;
+    Ctx *c;
+    if (int r = get_ctx(opts ? opts->device : -1, &c)) return r;
+    cudaStream_t st = st_in ? st_in : c->stream;
+    JoinIn in{a, self ? a : b, na, self ? na : nb, dtype_bytes, d, eps, self};
+    Prepared P;
+    if (int r = prepare_join(c, st, in, opts, form, &P)) return r;
+    PreparedJob &J = *out;
+    J = PreparedJob();
+    J.A = P.A;
+    J.B = P.B;
+    J.na_eff = P.na_eff;
+    J.nb_eff = P.nb_eff;
+    J.op_scale = P.A.op_scale;
+    J.maxabs = P.maxabs;
+    J.form = P.form;
+    J.num_sms = c->num_sms;
+    int launches = P.launches;
+    tc_band_constants(P.form, d, P.maxabs, &J.c_rel, &J.c_abs);
+    const double T_tc = eps * eps * J.op_scale * J.op_scale;
+    AllocCtx actx{c, st};
+    int sr = split_items_by_precision(P.idx, J.A, J.B, J.c_rel, J.c_abs, 0.5 * T_tc, slot_alloc_cb, &actx, st,
+                                      &J.idx_tc, &J.idx_fp);
+    if (sr == 2) return fail(HJ_ERR_OOM, "out of device memory (work list split)");
+    if (sr) return check_cuda("work list split");
+    launches += 2;
+    if (J.idx_fp.n_items) {
+        if (int rr = ensure_plain_tiles(c, st, &J.A, false, &launches)) return rr;
+        if (self)
+            J.B.tiles64 = J.A.tiles64, J.B.n_tiles64 = J.A.n_tiles64;
+        else if (int rr = ensure_plain_tiles(c, st, &J.B, true, &launches))
+            return rr;
+    }
+    J.launches = launches;
+    return check_cuda("batch job preparation");
+}
+
 static int stripes_to_active_dims(int stripes) {
     int s = 0, p3 = 1;
     while (s < kMaxActiveDims && (p3 + 1) / 2 < stripes) {

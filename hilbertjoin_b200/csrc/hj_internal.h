@@ -10,6 +10,8 @@
 #include <string>
 #include <vector>
 
+#include "../../include/hj.h"
+
 namespace hj {
 
 // Point-tile sizes of the two distance kernels.
@@ -245,5 +247,32 @@ void launch_recheck(const TcJob *d_jobs, int dtype_bytes, const uint2 *band, con
 void set_tc_debug_output(float *dbg);
 // Error-bound constant of a tensor-core form for dimension d.
 void tc_band_constants(int form, uint32_t d, double maxabs, double *c_rel, double *c_abs);
+
+// ---------------------------------------------------------------- batching
+// One job prepared by the engine for a batched tensor-core launch: its sorted
+// sets in every layout the kernels need and its work list split by precision.
+// All pointers live in the calling thread's engine buffers and stay valid
+// only until that thread's next engine call.
+struct PreparedJob {
+    SortedSet A, B;
+    IndexResult idx_tc, idx_fp;  // tensor-core items; items routed to the FP64 kernel (64 x 64 tiles)
+    uint64_t na_eff = 0, nb_eff = 0;
+    double op_scale = 1.0, maxabs = 0.0, c_rel = 0.0, c_abs = 0.0;
+    int form = 0;
+    int launches = 0;
+    int num_sms = 0;
+};
+// Prepares one join (device inputs) for tensor-core form `form` on the current
+// device: cell statistics, EGO sort, layouts, index, precision split, and
+// the plain FP64 tiles when items were routed to the FP64 kernel. Synchronises
+// `st` a few times (planning read-backs). Returns an hj_status.
+int engine_prepare_job(cudaStream_t st, const void *a, const void *b, uint64_t na, uint64_t nb, int dtype_bytes,
+                       uint32_t d, double eps, bool self, const hj_opts *opts, int form, PreparedJob *out);
+// Sets the calling thread's last error text and returns code.
+int engine_fail(int code, const std::string &msg);
+// Norm summaries over a row-major norm array of npad rows (padding rows hold
+// kPadNorm): per 128-row and per 256-row tile maxima, per 32-row minima.
+void launch_norm_summaries(const float *norms, uint64_t npad, float *tmax128, float *tmax256, float *gmin32,
+                           cudaStream_t st);
 
 }  // namespace hj

@@ -565,4 +565,12 @@ void launch_gather(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const
     if (launches) *launches += L;
 }
 
+void launch_norm_summaries(const float *norms, uint64_t npad, float *tmax128, float *tmax256, float *gmin32,
+                           cudaStream_t st) {
+    if (npad == 0) return;
+    k_tile_max<<<(unsigned)hj_ceil_div(npad / 128, 256), 256, 0, st>>>(norms, npad, 128, tmax128);
+    k_tile_max<<<(unsigned)hj_ceil_div(npad / 256, 256), 256, 0, st>>>(norms, npad, 256, tmax256);
+    k_group_min<<<(unsigned)hj_ceil_div(npad / 32, 256), 256, 0, st>>>(norms, npad, 32, gmin32);
+}
+
 }  // namespace hj

@@ -247,6 +247,38 @@ HJ_API void hj_test_ego_loop3_noself(const size_t nA, const size_t nB, const int
 HJ_API int hj_debug_tc_estimates(const float *A, uint64_t nA, const float *B, uint64_t nB, uint32_t d, int form,
                                  float *out);
 
+/* ---------------------------------------------------------------- batching
+ * Many joins of uneven n, d and eps in one persistent tensor-core launch. The
+ * jobs' inputs are device rows (dtype_bytes 4 or 8, the same for all jobs);
+ * b == NULL makes a job a self-join. hj_batch_create plans the batch --
+ * every job's EGO sort, layouts and work list, merged into one work list over
+ * one operand matrix -- and runs it once (its counts are ready at once);
+ * hj_batch_run enqueues another run on `stream` (NULL = the batch's own
+ * stream) with no host synchronisation, so a run can be captured into a CUDA
+ * graph and replayed; hj_batch_counts waits for the last run and returns one
+ * count per job (the same as the job's own hj_*_join_count_device call).
+ * opts: form (HJ_FORM_TC_FP16 / _TF32 / _BF16X3; AUTO = FP16), active_dims,
+ * ref_compat, device, stream (for planning); d <= 256 per job. The input
+ * buffers are read only during hj_batch_create. No counterpart in the
+ * reference, which runs one join per process. */
+typedef struct {
+    const void *a;    /* device rows [na][d] */
+    const void *b;    /* device rows [nb][d], or NULL for a self-join of a */
+    uint64_t na, nb;
+    uint32_t d;
+    uint32_t reserved;
+    double eps;
+} hj_batch_job;
+typedef struct hj_batch hj_batch;
+HJ_API int hj_batch_create(const hj_batch_job *jobs, uint32_t n_jobs, int dtype_bytes, const hj_opts *opts,
+                           hj_batch **out);
+HJ_API int hj_batch_run(hj_batch *batch, void *stream);
+HJ_API int hj_batch_counts(hj_batch *batch, uint64_t *counts, hj_stats *stats);
+HJ_API int hj_batch_destroy(hj_batch *batch);
+/* create + counts + destroy. */
+HJ_API int hj_batch_count_device(const hj_batch_job *jobs, uint32_t n_jobs, int dtype_bytes, const hj_opts *opts,
+                                 uint64_t *counts, hj_stats *stats);
+
 /* ---------------------------------------------------------------- serving
  * A request loop with device-resident point sets: sets are uploaded once and
  * referenced by handle; joins are submitted from any thread, admitted against
