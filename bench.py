@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison step")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--n", type=int, default=N_POINTS, help=argparse.SUPPRESS)
-    ap.add_argument("--workload", default="selfjoin", choices=["selfjoin", "serving"],
+    ap.add_argument("--workload", default="selfjoin", choices=["selfjoin", "serving", "batch"],
                     help="serving: the join-serving stream (not the headline line)")
     ap.add_argument("--requests", type=int, default=2000)
     ap.add_argument("--baseline-requests", type=int, default=200)
@@ -220,10 +220,25 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args):
+    """Many joins in one persistent launch: jobs/s of single calls, of one
+    planned batch, and of replays of a graph-captured batch run."""
+    import torch
+    torch.cuda.set_device(0)
+    from hilbertjoin_b200 import batching
+    r = batching.run_benchmark(form=args.form if args.form != "plain" else "fp16")
+    line = {"metric": "batched joins/s (one persistent launch, graph replay)",
+            "value": r["batch_replay"]["jobs_per_s"], "unit": "joins/s", "n_gpus": 1, "higher_is_better": True,
+            "data": "synthetic", "config": {"workload": r["workload"], "form": r["form"]}, "batch": r}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.workload == "serving":
         return run_serving(args)
+    if args.workload == "batch":
+        return run_batch(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch

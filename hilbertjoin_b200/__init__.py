@@ -41,7 +41,7 @@ class HJError(RuntimeError):
 class Opts(ctypes.Structure):
     _fields_ = [("form", ctypes.c_int32), ("active_dims", ctypes.c_int32), ("ref_compat", ctypes.c_int32),
                 ("device", ctypes.c_int32), ("stream", ctypes.c_void_p), ("shard_index", ctypes.c_int32),
-                ("shard_count", ctypes.c_int32), ("reorder_dims", ctypes.c_int32), ("reserved_i", ctypes.c_int32),
+                ("shard_count", ctypes.c_int32), ("reorder_dims", ctypes.c_int32), ("item_chunk", ctypes.c_int32),
                 ("reserved", ctypes.c_uint64 * 2)]
 
 
@@ -129,7 +129,7 @@ def _check(status: int) -> None:
         raise HJError(status, lib().hj_last_error().decode())
 
 
-def _opts(form, active_dims, ref_compat, device, stream, shard=None, reorder_dims=False) -> Opts:
+def _opts(form, active_dims, ref_compat, device, stream, shard=None, reorder_dims=False, item_chunk=None) -> Opts:
     o = Opts()
     lib().hj_opts_init(ctypes.byref(o))
     o.form = FORMS[form] if isinstance(form, str) else int(form)
@@ -140,6 +140,7 @@ def _opts(form, active_dims, ref_compat, device, stream, shard=None, reorder_dim
     if shard is not None:
         o.shard_index, o.shard_count = int(shard[0]), int(shard[1])
     o.reorder_dims = int(bool(reorder_dims))
+    o.item_chunk = int(item_chunk or 0)
     return o
 
 
@@ -165,7 +166,7 @@ def _torch_stream(x, stream):
 
 
 def self_join_count(points, eps: float, form="plain", active_dims=None, ref_compat=False, device=None,
-                    stream=None, return_stats=False, shard=None, reorder_dims=False):
+                    stream=None, return_stats=False, shard=None, reorder_dims=False, item_chunk=None):
     """Number of unordered pairs {a, b}, a != b, of `points` with |a-b| <= eps.
 
     `points`: (n, d) float32/float64 numpy array (copied to the device inside
@@ -177,13 +178,13 @@ def self_join_count(points, eps: float, form="plain", active_dims=None, ref_comp
             raise ValueError("points must be a 2-D float32/float64 tensor")
         x = points.contiguous()
         opts = _opts(form, active_dims, ref_compat, x.device.index if device is None else device,
-                     _torch_stream(x, stream), shard, reorder_dims)
+                     _torch_stream(x, stream), shard, reorder_dims, item_chunk)
         _check(lib().hj_self_join_count_device(ctypes.c_void_p(x.data_ptr()), x.element_size(), x.shape[0],
                                                x.shape[1], float(eps), ctypes.byref(opts), ctypes.byref(c),
                                                ctypes.byref(o)))
     else:
         x = _host_array(points)
-        opts = _opts(form, active_dims, ref_compat, device, stream, shard, reorder_dims)
+        opts = _opts(form, active_dims, ref_compat, device, stream, shard, reorder_dims, item_chunk)
         fn = lib().hj_self_join_count if x.dtype == np.float64 else lib().hj_self_join_count_f32
         _check(fn(x.ctypes.data_as(ctypes.c_void_p), x.shape[0], x.shape[1], float(eps), ctypes.byref(opts),
                   ctypes.byref(c), ctypes.byref(o)))
@@ -191,7 +192,7 @@ def self_join_count(points, eps: float, form="plain", active_dims=None, ref_comp
 
 
 def join_count(a, b, eps: float, form="plain", active_dims=None, ref_compat=False, device=None, stream=None,
-               return_stats=False, shard=None, reorder_dims=False):
+               return_stats=False, shard=None, reorder_dims=False, item_chunk=None):
     """Number of ordered pairs (p in a, q in b) with |p-q| <= eps."""
     o = Stats()
     c = ctypes.c_uint64(0)
@@ -200,7 +201,7 @@ def join_count(a, b, eps: float, form="plain", active_dims=None, ref_compat=Fals
         if xa.dtype != xb.dtype or xa.shape[1] != xb.shape[1]:
             raise ValueError("a and b must have the same dtype and dimension")
         opts = _opts(form, active_dims, ref_compat, xa.device.index if device is None else device,
-                     _torch_stream(xa, stream), shard, reorder_dims)
+                     _torch_stream(xa, stream), shard, reorder_dims, item_chunk)
         _check(lib().hj_join_count_device(ctypes.c_void_p(xa.data_ptr()), xa.shape[0], ctypes.c_void_p(xb.data_ptr()),
                                           xb.shape[0], xa.element_size(), xa.shape[1], float(eps),
                                           ctypes.byref(opts), ctypes.byref(c), ctypes.byref(o)))
@@ -210,7 +211,7 @@ def join_count(a, b, eps: float, form="plain", active_dims=None, ref_compat=Fals
             xb = xb.astype(xa.dtype)
         if xa.shape[1] != xb.shape[1]:
             raise ValueError("a and b must have the same dimension")
-        opts = _opts(form, active_dims, ref_compat, device, stream, shard, reorder_dims)
+        opts = _opts(form, active_dims, ref_compat, device, stream, shard, reorder_dims, item_chunk)
         fn = lib().hj_join_count if xa.dtype == np.float64 else lib().hj_join_count_f32
         _check(fn(xa.ctypes.data_as(ctypes.c_void_p), xa.shape[0], xb.ctypes.data_as(ctypes.c_void_p), xb.shape[0],
                   xa.shape[1], float(eps), ctypes.byref(opts), ctypes.byref(c), ctypes.byref(o)))

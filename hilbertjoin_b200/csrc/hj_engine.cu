@@ -353,6 +353,7 @@ static int prepare_join(Ctx *c, cudaStream_t st, const JoinIn &in, const hj_opts
                         Prepared *P) {
     int form = form_override >= 0 ? form_override : (opts ? opts->form : HJ_FORM_PLAIN_FP64);
     if (form < HJ_FORM_PLAIN_FP64 || form > HJ_FORM_TC_FP16) return fail(HJ_ERR_INVALID_ARG, "unknown form");
+    if (opts && opts->item_chunk > 4096) return fail(HJ_ERR_INVALID_ARG, "item_chunk must be at most 4096");
     int active_dims = opts ? opts->active_dims : -1;
     const bool ref_compat = opts && opts->ref_compat;
     if (active_dims < 0) active_dims = in.self ? 3 : 2;
@@ -466,7 +467,8 @@ static int prepare_join(Ctx *c, cudaStream_t st, const JoinIn &in, const hj_opts
     }
     const bool tc = form_is_tc(form);
     const int tile_a = tc ? kTcTileA : kPlainTile, tile_b = tc ? kTcTileB : kPlainTile;
-    const uint32_t chunk = tc ? 32 : 16;
+    // B tiles per work item: 32 x 256 rows (tensor-core forms), 16 x 64 rows (plain), unless set
+    const uint32_t chunk = (opts && opts->item_chunk > 0) ? (uint32_t)opts->item_chunk : (tc ? 32u : 16u);
     IndexResult &idx = P->idx;
     AllocCtx actx{c, st};
     std::string err;

@@ -98,7 +98,10 @@ typedef struct {
                               before every join, mainJoin.cpp:97-100). Distances are still
                               summed in the caller's dim order, so the count is unchanged;
                               only the work (candidate pairs) changes. */
-    int32_t reserved_i;
+    int32_t item_chunk;    /* B tiles per work item of the distance kernel; 0 = default (32 for
+                              the tensor-core forms, 16 for the plain form). Smaller chunks
+                              balance small joins across the SMs, larger ones keep B tiles in
+                              L2; hilbertjoin_b200.autotune picks it per dimension. */
     uint64_t reserved[2];
 } hj_opts;
 

@@ -112,3 +112,19 @@ def test_batch_rejects_bad_jobs(env):
         B.batch_count([(x, None, 0.1)])
     with pytest.raises(hj.HJError):
         B.batch_count([(torch.rand(10, 4, device="cuda"), None, 0.1)], form="plain")
+
+
+def test_item_chunk_and_tuned_batches_are_exact(env):
+    torch, hj, B = env
+    from hilbertjoin_b200 import autotune
+    x = torch.from_numpy(W.gmm(30000, 24, 5, components=8, dtype=np.float32)).cuda()
+    eps = W.calibrate_eps(x.cpu().numpy(), 30000, 24)
+    want = hj.self_join_count(x, eps)
+    for chunk in (1, 7, 64, 300):
+        for form in ("fp16", "tf32"):
+            assert hj.self_join_count(x, eps, form=form, item_chunk=chunk) == want
+    jobs, _ = make_jobs(torch, seed=3)
+    assert B.batch_count(jobs, tuned=True) == [alone(hj, j, "plain") for j in jobs]
+    assert autotune.config_for(24)["form"] in autotune.FORMS
+    with pytest.raises(hj.HJError):
+        hj.self_join_count(x, eps, form="fp16", item_chunk=5000)
