@@ -47,6 +47,10 @@ __global__ void k_dim_stats_init(DimStats *s, uint32_t d, unsigned long long *ma
 // Cells beyond +-2^62 cannot be represented; such inputs are rejected.
 constexpr double kCellLimit = 4.611686018427388e18;
 
+// Thread k handles dim t = k % d of rows k / d, k / d + R, ... (R = threads /
+// d): consecutive threads read consecutive coordinates of a row (coalesced),
+// and every thread keeps its dim's minima and maxima in registers; one
+// shared-memory atomic per thread and statistic at the end.
 __global__ void k_dim_stats(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, DimStats *s,
                             unsigned long long *maxabs_bits, uint32_t *bad) {
     extern __shared__ long long sh[];  // [4][d]
@@ -59,37 +63,48 @@ __global__ void k_dim_stats(const void *x, int dtype_bytes, uint64_t n, uint32_t
         sxmax[t] = 0ull;
     }
     __syncthreads();
-    const uint64_t total = n * d;
+    const uint64_t threads = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t rows_per_step = threads / d;  // >= 1 (the launch ensures threads >= d)
+    const uint32_t t = (uint32_t)(k % d);
+    long long cmin = LLONG_MAX, cmax = LLONG_MIN;
+    unsigned long long xmin = ~0ull, xmax = 0ull;
     double amax = 0.0;
     uint32_t lbad = 0;
-    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-         e += (uint64_t)gridDim.x * blockDim.x) {
-        double v = coord(x, dtype_bytes, e);
-        if (!isfinite(v)) {
-            lbad = 1;
-            continue;
+    if (k < rows_per_step * d) {
+        for (uint64_t r = k / d; r < n; r += rows_per_step) {
+            const double v = coord(x, dtype_bytes, r * d + t);
+            if (!isfinite(v)) {
+                lbad |= 1u;
+                continue;
+            }
+            const double c = floor(v / eps);
+            if (!(fabs(c) < kCellLimit)) {
+                lbad |= 2u;
+                continue;
+            }
+            amax = fmax(amax, fabs(v));
+            const long long ci = (long long)c;
+            cmin = min(cmin, ci);
+            cmax = max(cmax, ci);
+            const unsigned long long ov = ordered_from_double(v);
+            xmin = min(xmin, ov);
+            xmax = max(xmax, ov);
         }
-        double c = floor(v / eps);
-        if (!(fabs(c) < kCellLimit)) {
-            lbad = 2;
-            continue;
-        }
-        amax = fmax(amax, fabs(v));
-        uint32_t t = (uint32_t)(e % d);
-        long long ci = (long long)c;
-        atomicMin(&smin[t], ci);
-        atomicMax(&smax[t], ci);
-        const unsigned long long ov = ordered_from_double(v);
-        atomicMin(&sxmin[t], ov);
-        atomicMax(&sxmax[t], ov);
+    }
+    if (cmin != LLONG_MAX) {
+        atomicMin(&smin[t], cmin);
+        atomicMax(&smax[t], cmax);
+        atomicMin(&sxmin[t], xmin);
+        atomicMax(&sxmax[t], xmax);
     }
     __syncthreads();
-    for (uint32_t t = threadIdx.x; t < d; t += blockDim.x) {
-        if (smin[t] != LLONG_MAX) {
-            atomicMin(&s[t].cmin, smin[t]);
-            atomicMax(&s[t].cmax, smax[t]);
-            atomicMin(&s[t].xmin, sxmin[t]);
-            atomicMax(&s[t].xmax, sxmax[t]);
+    for (uint32_t u = threadIdx.x; u < d; u += blockDim.x) {
+        if (smin[u] != LLONG_MAX) {
+            atomicMin(&s[u].cmin, smin[u]);
+            atomicMax(&s[u].cmax, smax[u]);
+            atomicMin(&s[u].xmin, sxmin[u]);
+            atomicMax(&s[u].xmax, sxmax[u]);
         }
     }
     // non-negative doubles order like their bit patterns
@@ -107,52 +122,67 @@ void launch_dim_stats(const void *x, int dtype_bytes, uint64_t n, uint32_t d, do
     uint64_t total = n * d;
     int blocks = (int)std::min<uint64_t>(hj_ceil_div(total, 256 * 8), 148 * 8);
     if (blocks < 1) blocks = 1;
+    if ((uint64_t)blocks * 256 < d) blocks = (int)hj_ceil_div(d, 256);  // every dim gets a thread
     k_dim_stats<<<blocks, 256, 4 * d * sizeof(long long), st>>>(x, dtype_bytes, n, d, eps, dstats, d_maxabs_bits,
                                                                  d_bad);
 }
 
 // ------------------------------------------------------------ key packing
 
-// One thread per point: digit of every dim, OR-ed into the running key word.
+// One warp per point, the row read in rounds of 32 consecutive coordinates
+// (coalesced). In a round each lane computes its dim's field; lanes whose
+// fields share a key word (the field layout decides which, in any dimension
+// order) are grouped by __match_any_sync and OR-reduced, and the group's
+// lowest lane ORs the result into the warp's word accumulators in shared
+// memory; the W words are written at the end.
 __global__ void k_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, GridDev g,
                             uint32_t W, uint32_t *keys_wm) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    uint32_t cur_word = 0, acc = 0;
-    for (uint32_t pos = 0; pos < d; ++pos) {  // fields in key order: words never decrease
-        const uint32_t t = grid_dim_at(g, pos);
-        uint32_t w = g.word[t];
-        if (w != cur_word) {
-            keys_wm[(uint64_t)cur_word * n + i] = acc;
-            for (uint32_t z = cur_word + 1; z < w; ++z) keys_wm[(uint64_t)z * n + i] = 0u;
-            cur_word = w;
-            acc = 0;
+    extern __shared__ uint32_t kacc[];  // [warps per block][W]
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= n) return;  // whole warps leave together
+    uint32_t *acc = kacc + (size_t)wib * W;
+    for (uint32_t w = lane; w < W; w += 32) acc[w] = 0u;
+    __syncwarp();
+    for (uint32_t t0 = 0; t0 < d; t0 += 32) {
+        const uint32_t t = t0 + lane;
+        uint32_t field = 0, word = 0xffffffffu;
+        if (t < d) {
+            const double c = floor(coord(x, dtype_bytes, i * d + t) / eps);
+            field = (uint32_t)((long long)c - g.off[t]) << g.shift[t];
+            word = g.word[t];
         }
-        double c = floor(coord(x, dtype_bytes, i * d + t) / eps);
-        long long dig = (long long)c - g.off[t];
-        acc |= (uint32_t)dig << g.shift[t];
+        const uint32_t peers = __match_any_sync(0xffffffffu, word);
+        const uint32_t v = __reduce_or_sync(peers, field);
+        if (t < d && lane == (uint32_t)(__ffs(peers) - 1)) acc[word] |= v;
+        __syncwarp();
     }
-    keys_wm[(uint64_t)cur_word * n + i] = acc;
-    for (uint32_t z = cur_word + 1; z < W; ++z) keys_wm[(uint64_t)z * n + i] = 0u;
+    for (uint32_t w = lane; w < W; w += 32) keys_wm[(uint64_t)w * n + i] = acc[w];
 }
 
+// One warp per point: |x - center|^2 over lanes (coalesced), warp sum.
 __global__ void k_norm_key(const void *x, int dtype_bytes, uint64_t n, uint32_t d,
                            const double *__restrict__ center, double scale, uint32_t *key_out) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
     if (i >= n) return;
     double s = 0.0;
-    for (uint32_t k = 0; k < d; ++k) {
-        double v = coord(x, dtype_bytes, i * d + k) - center[k];
+    for (uint32_t k = lane; k < d; k += 32) {
+        const double v = coord(x, dtype_bytes, i * d + k) - center[k];
         s = fma(v, v, s);
     }
-    double q = floor(s * scale);
-    key_out[i] = q < 65535.0 ? (uint32_t)q : 65535u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+        const double q = floor(s * scale);
+        key_out[i] = q < 65535.0 ? (uint32_t)q : 65535u;
+    }
 }
 
 void launch_norm_key(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const double *center, double scale,
                      uint32_t *key_out, cudaStream_t st) {
     if (n == 0) return;
-    k_norm_key<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(x, dtype_bytes, n, d, center, scale, key_out);
+    k_norm_key<<<(unsigned)hj_ceil_div(n, 8), 256, 0, st>>>(x, dtype_bytes, n, d, center, scale, key_out);
 }
 
 // Dimension cost (the selectivity estimate of the reference's
@@ -223,7 +253,9 @@ void launch_dim_cost(const void *x, int dtype_bytes, uint64_t n, uint32_t d, dou
 void launch_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, const GridDev &g,
                       uint32_t W, uint32_t *keys_wm, cudaStream_t st) {
     if (n == 0) return;
-    k_pack_keys<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(x, dtype_bytes, n, d, eps, g, W, keys_wm);
+    // 8 points (warps) per block of 256 threads
+    k_pack_keys<<<(unsigned)hj_ceil_div(n, 8), 256, 8 * W * sizeof(uint32_t), st>>>(x, dtype_bytes, n, d, eps, g, W,
+                                                                                   keys_wm);
 }
 
 // ------------------------------------------------------------ radix sort
@@ -396,23 +428,26 @@ void launch_iota(uint32_t *p, uint64_t n, cudaStream_t st) {
 // ------------------------------------------------------------ gather
 
 // Sorted keys row-major [n][W] (for binary searches) and sorted rows.
+// One warp per sorted rank: the key words and the row of input index perm[r]
+// (lanes over words and coordinates: coalesced reads and writes).
 __global__ void k_gather_keys_rows(const void *x, int dtype_bytes, uint64_t n, uint32_t d,
                                    const uint32_t *__restrict__ perm, const uint32_t *__restrict__ keys_wm,
                                    uint32_t W, uint32_t *__restrict__ keys_rm, void *rows_out) {
-    uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
     if (r >= n) return;
-    uint32_t src = perm[r];
+    const uint32_t src = perm[r];
     if (keys_rm)
-        for (uint32_t w = 0; w < W; ++w) keys_rm[r * W + w] = keys_wm[(uint64_t)w * n + src];
+        for (uint32_t w = lane; w < W; w += 32) keys_rm[r * W + w] = keys_wm[(uint64_t)w * n + src];
     if (rows_out) {
         if (dtype_bytes == 8) {
             const double *xs = static_cast<const double *>(x) + (uint64_t)src * d;
             double *o = static_cast<double *>(rows_out) + r * d;
-            for (uint32_t k = 0; k < d; ++k) o[k] = xs[k];
+            for (uint32_t k = lane; k < d; k += 32) o[k] = xs[k];
         } else {
             const float *xs = static_cast<const float *>(x) + (uint64_t)src * d;
             float *o = static_cast<float *>(rows_out) + r * d;
-            for (uint32_t k = 0; k < d; ++k) o[k] = xs[k];
+            for (uint32_t k = lane; k < d; k += 32) o[k] = xs[k];
         }
     }
 }
@@ -476,19 +511,22 @@ __global__ void k_gather_tc(const void *x, int dtype_bytes, uint64_t n, uint32_t
 // stored as FP32; padding rows get kPadNorm so that they never pass a threshold.
 __global__ void k_norms(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const uint32_t *__restrict__ perm,
                         const double *__restrict__ center, uint64_t npad, double scale2, float *norms) {
-    uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
     if (r >= npad) return;
     if (r >= n) {
-        norms[r] = kPadNorm;
+        if (lane == 0) norms[r] = kPadNorm;
         return;
     }
-    uint64_t src = perm[r];
+    const uint64_t src = perm[r];
     double s = 0.0;
-    for (uint32_t k = 0; k < d; ++k) {
-        double v = coord(x, dtype_bytes, src * d + k) - center[k];
+    for (uint32_t k = lane; k < d; k += 32) {
+        const double v = coord(x, dtype_bytes, src * d + k) - center[k];
         s = fma(v, v, s);
     }
-    norms[r] = (float)(s * scale2);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) norms[r] = (float)(s * scale2);
 }
 
 // Per-tile maximum norm over real rows (padding rows excluded).
@@ -518,7 +556,7 @@ void launch_gather(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const
     int L = 0;
     if (n == 0) return;
     if (flags & (kGatherKeys | kGatherRows)) {
-        k_gather_keys_rows<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(
+        k_gather_keys_rows<<<(unsigned)hj_ceil_div(n, 8), 256, 0, st>>>(  // a warp per rank
             x, dtype_bytes, n, d, perm, keys_wm, W, (flags & kGatherKeys) ? o.keys : nullptr,
             (flags & kGatherRows) ? const_cast<void *>(o.rows) : nullptr);
         ++L;
@@ -551,7 +589,7 @@ void launch_gather(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const
         ++L;
     }
     if (flags & kGatherNorms) {
-        k_norms<<<(unsigned)hj_ceil_div(o.npad_tc, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.center,
+        k_norms<<<(unsigned)hj_ceil_div(o.npad_tc, 8), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.center,
                                                                       o.npad_tc, o.op_scale * o.op_scale,
                                                                       o.norms);
         k_tile_max<<<(unsigned)hj_ceil_div(o.npad_tc / kTcTileA, 256), 256, 0, st>>>(o.norms, o.npad_tc, kTcTileA,
