@@ -498,6 +498,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         tmem_ld64(taddr, *reinterpret_cast<float(*)[64]>(v));
                     else
                         tmem_ld32(taddr, *reinterpret_cast<float(*)[32]>(v));
+                    if (c + 1 == kEpiChunks) {
+                        // the last chunk is in registers (its slow path too works from
+                        // them): the accumulator goes back to the MMA warp before the
+                        // chunk is classified
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(&bar_accempty[acc]);
+                    }
                     // max_j v_j per 32-column group: with the group's minimum norm,
                     // min_j (|b_j|^2 - 2 v_j) >= gmin - 2 max_j v_j
                     float mg[kChunkGroups];
@@ -574,9 +582,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         }
                     }
                 }
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&bar_accempty[acc]);
                 ++t_cnt;
             }
             if (last_tile && it < p.n_items) item_rows(w);
