@@ -57,11 +57,15 @@ namespace hj {
 // 256 accumulator columns, in two chunks of kChunkCols (one TMEM load each).
 constexpr int kEpiWarps = HJ_EPI_WARPS;
 constexpr int kEpiCols = 4 * kTcTileB / kEpiWarps;
-constexpr int kChunkCols = kEpiCols / 2;
+// 8 warps: two 64-column chunks each; 16 warps: one 64-column chunk each
+constexpr int kChunkCols = 64;
 constexpr int kChunkGroups = kChunkCols / 32;  // 32-column groups per chunk
-constexpr int kEpiChunks = 2;
+constexpr int kEpiChunks = kEpiCols / kChunkCols;
 constexpr int kEpiVec = kEpiCols / 32;  // norms per lane, group minima per warp
-static_assert(kEpiWarps == 8 || kEpiWarps == 16, "8 or 16 epilogue warps");
+// 16 epilogue warps (4 per quadrant) were measured slower: at 18 warps the
+// register cap is 96 (spills) and the static shared memory no longer fits next
+// to the 225 KB operand plan.
+static_assert(kEpiWarps == 8, "the shared-memory plan and register budget assume 8 epilogue warps");
 constexpr int kTcThreads = 64 + 32 * kEpiWarps;
 constexpr uint32_t kAtomBytes = 128;                  // bytes of K per row per swizzle atom
 constexpr uint32_t kAStageBytes = kTcTileA * kAtomBytes;  // 16 KB per A atom
