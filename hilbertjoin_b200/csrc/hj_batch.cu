@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -81,12 +82,16 @@ struct hj_batch {
     unsigned int *d_maxerr = nullptr;
     std::vector<FpJob> fp;
     std::vector<void *> allocs;
+    cudaStream_t alloc_stream = nullptr;  // planning stream: buffers are stream-ordered on it
     uint64_t candidate_pairs = 0, fp64_items = 0;
-    double plan_ms = 0;
+    std::vector<uint64_t> job_candidates;
 
+    // Stream-ordered allocations (cudaMallocAsync): no device-wide
+    // synchronisation, so batches built by concurrent server workers do not
+    // stall each other's kernels.
     void *alloc(size_t bytes) {
         void *p = nullptr;
-        if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) {
+        if (cudaMallocAsync(&p, bytes ? bytes : 16, alloc_stream) != cudaSuccess) {
             cudaGetLastError();
             return nullptr;
         }
@@ -94,7 +99,9 @@ struct hj_batch {
         return p;
     }
     ~hj_batch() {
-        for (void *p : allocs) cudaFree(p);
+        cudaStream_t fs = last ? last : alloc_stream;
+        for (void *p : allocs) cudaFreeAsync(p, fs);
+        if (fs) cudaStreamSynchronize(fs);
         if (own) cudaStreamDestroy(own);
     }
 };
@@ -153,11 +160,27 @@ static int batch_plan(const hj_batch_job *jobs, uint32_t n_jobs, int dtype_bytes
     if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return engine_fail(HJ_ERR_NO_DEVICE, "no CUDA device");
     if (cudaSetDevice(dev) != cudaSuccess) return engine_fail(HJ_ERR_NO_DEVICE, "no CUDA device");
     b->device = dev;
+    {
+        // keep freed batch buffers in the device's default pool between batches
+        // (the default threshold returns them to the system at every sync)
+        static std::once_flag once[64];
+        if (dev < 64)
+            std::call_once(once[dev], [dev] {
+                cudaMemPool_t pool;
+                if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+                    uint64_t keep = ~0ull;
+                    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+                }
+                cudaGetLastError();
+            });
+    }
     cudaStream_t st = opts && opts->stream ? (cudaStream_t)opts->stream : nullptr;
     if (cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) != cudaSuccess)
         return engine_fail(HJ_ERR_CUDA, "cudaStreamCreate failed");
     if (!st) st = b->own;
     b->last = st;
+    b->alloc_stream = st;
+    b->job_candidates.assign(n_jobs, 0);
 
     // row layout of the operand matrix
     std::vector<uint64_t> a_row0(n_jobs), b_row0(n_jobs), rows_off_a(n_jobs), rows_off_b(n_jobs);
@@ -252,6 +275,7 @@ static int batch_plan(const hj_batch_job *jobs, uint32_t n_jobs, int dtype_bytes
             n_items += P.idx_tc.n_items;
         }
         b->candidate_pairs += P.idx_tc.candidate_pairs;
+        b->job_candidates[j] = P.idx_tc.candidate_pairs + P.idx_fp.candidate_pairs;
         // items routed to the FP64 kernel keep their own plain tiles
         if (P.idx_fp.n_items) {
             FpJob f;
@@ -314,6 +338,13 @@ static int batch_plan(const hj_batch_job *jobs, uint32_t n_jobs, int dtype_bytes
     }
     return engine_fail(HJ_ERR_BAND_OVERFLOW, "band queue overflow");
 }
+
+namespace hj {
+int batch_job_candidates(const hj_batch *b, uint64_t *out) {
+    for (uint32_t j = 0; j < b->n_jobs; ++j) out[j] = b->job_candidates[j];
+    return HJ_OK;
+}
+}  // namespace hj
 
 extern "C" {
 

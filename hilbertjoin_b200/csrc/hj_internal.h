@@ -268,6 +268,8 @@ struct PreparedJob {
 // `st` a few times (planning read-backs). Returns an hj_status.
 int engine_prepare_job(cudaStream_t st, const void *a, const void *b, uint64_t na, uint64_t nb, int dtype_bytes,
                        uint32_t d, double eps, bool self, const hj_opts *opts, int form, PreparedJob *out);
+// Candidate pairs of every job of a planned batch (server statistics).
+int batch_job_candidates(const hj_batch *b, uint64_t *out);
 // Sets the calling thread's last error text and returns code.
 int engine_fail(int code, const std::string &msg);
 // Norm summaries over a row-major norm array of npad rows (padding rows hold

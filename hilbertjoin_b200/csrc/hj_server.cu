@@ -10,6 +10,13 @@
 // request larger than the whole budget is rejected with HJ_ERR_BUSY. Every
 // request's count is computed by the same pipeline as a standalone call, so a
 // result does not depend on what else is in flight.
+//
+// With batch_max > 1 (tensor-core forms) a free worker takes the queue's head
+// and then further queued requests of the same dtype while they fit in the
+// budget, up to batch_max, and runs them as one batch (hj_batch_count_device:
+// every request's sort and index, then ONE persistent launch over all their
+// work items). A request's count is the same either way; a batch that cannot
+// run (e.g. d > 256) falls back to one call per request.
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -23,6 +30,7 @@
 #include <vector>
 
 #include "../../include/hj.h"
+#include "hj_internal.h"
 
 namespace {
 
@@ -73,67 +81,130 @@ static uint64_t request_bytes(const DevSet &a, const DevSet &b, bool self) {
     return m + (64ull << 20);
 }
 
+// Fills a finished request's result and releases its memory and sets (lock held).
+static void finish_request(hj_server *s, uint64_t id, int status, uint64_t count, int form_used,
+                           uint64_t candidate_pairs, uint64_t band_pairs) {
+    Request &r = s->reqs[id];
+    r.t_end = Clock::now();
+    r.done = true;
+    r.res.count = count;
+    r.res.status = status;
+    r.res.form_used = status == HJ_OK ? form_used : -1;
+    r.res.queue_ms = std::chrono::duration<double, std::milli>(r.t_start - r.t_submit).count();
+    r.res.run_ms = std::chrono::duration<double, std::milli>(r.t_end - r.t_start).count();
+    r.res.latency_ms = std::chrono::duration<double, std::milli>(r.t_end - r.t_submit).count();
+    r.res.candidate_pairs = status == HJ_OK ? candidate_pairs : 0;
+    r.res.band_pairs = status == HJ_OK ? band_pairs : 0;
+    s->mem_in_use -= r.mem;
+    for (uint64_t sid : {r.a, r.b}) {
+        auto it = s->sets.find(sid);
+        if (it != s->sets.end()) {
+            if (--it->second.users == 0 && it->second.released) {
+                cudaFree(it->second.ptr);
+                s->sets.erase(it);
+            }
+        }
+        if (r.a == r.b) break;
+    }
+}
+
+static bool tc_form(int f) {
+    return f == HJ_FORM_TC_FP16 || f == HJ_FORM_TC_TF32 || f == HJ_FORM_TC_BF16X3 || f == HJ_FORM_AUTO;
+}
+
 static void worker_main(hj_server *s) {
     cudaSetDevice(s->device);
+    cudaStream_t stream = nullptr;
+    cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+    const int batch_max = tc_form(s->opts.form) && s->opts.batch_max > 1 ? s->opts.batch_max : 1;
     for (;;) {
-        uint64_t id = 0;
-        Request rq;
-        DevSet sa, sb;
+        std::vector<uint64_t> ids;
+        std::vector<Request> rqs;
+        std::vector<DevSet> sa, sb;
         {
             std::unique_lock<std::mutex> lk(s->mu);
             for (;;) {
-                if (s->stop) return;
+                if (s->stop) {
+                    if (stream) cudaStreamDestroy(stream);
+                    return;
+                }
                 if (!s->queue.empty()) {
                     Request &front = s->reqs[s->queue.front()];
                     if (s->mem_in_use + front.mem <= s->opts.memory_budget_bytes || s->mem_in_use == 0) break;
                 }
                 s->cv_work.wait(lk);
             }
-            id = s->queue.front();
-            s->queue.pop_front();
-            Request &r = s->reqs[id];
-            s->mem_in_use += r.mem;
-            r.t_start = Clock::now();
-            rq = r;
-            sa = s->sets[r.a];
-            sb = s->sets[r.b];
+            // the head, then followers of the same dtype while they fit the budget
+            int dtype = 0;
+            while (!s->queue.empty() && (int)ids.size() < batch_max) {
+                Request &r = s->reqs[s->queue.front()];
+                const DevSet &a = s->sets[r.a];
+                if (!ids.empty() && (a.dtype_bytes != dtype || s->mem_in_use + r.mem > s->opts.memory_budget_bytes))
+                    break;
+                dtype = a.dtype_bytes;
+                ids.push_back(r.id);
+                s->queue.pop_front();
+                s->mem_in_use += r.mem;
+                r.t_start = Clock::now();
+                rqs.push_back(r);
+                sa.push_back(a);
+                sb.push_back(s->sets[r.b]);
+            }
             s->cv_work.notify_all();
         }
         hj_opts o;
         hj_opts_init(&o);
         o.form = s->opts.form;
         o.device = s->device;
-        uint64_t count = 0;
-        hj_stats st;
-        int status;
-        if (rq.a == rq.b)
-            status = hj_self_join_count_device(sa.ptr, sa.dtype_bytes, sa.n, sa.d, rq.eps, &o, &count, &st);
-        else
-            status = hj_join_count_device(sa.ptr, sa.n, sb.ptr, sb.n, sa.dtype_bytes, sa.d, rq.eps, &o, &count, &st);
+        o.stream = stream;
+        const size_t k = ids.size();
+        std::vector<int> status(k, HJ_OK);
+        std::vector<uint64_t> count(k, 0), cand(k, 0), band(k, 0);
+        std::vector<int> form_used(k, s->opts.form);
+        bool batched = false;
+        if (k > 1) {
+            std::vector<hj_batch_job> jobs(k);
+            for (size_t i = 0; i < k; ++i) {
+                std::memset(&jobs[i], 0, sizeof(jobs[i]));
+                jobs[i].a = sa[i].ptr;
+                jobs[i].na = sa[i].n;
+                jobs[i].d = sa[i].d;
+                jobs[i].eps = rqs[i].eps;
+                if (rqs[i].a != rqs[i].b) {
+                    jobs[i].b = sb[i].ptr;
+                    jobs[i].nb = sb[i].n;
+                }
+            }
+            hj_batch *b = nullptr;
+            if (hj_batch_create(jobs.data(), (uint32_t)k, sa[0].dtype_bytes, &o, &b) == HJ_OK) {
+                hj_stats st;
+                if (hj_batch_counts(b, count.data(), &st) == HJ_OK) {
+                    batched = true;
+                    hj::batch_job_candidates(b, cand.data());
+                    for (size_t i = 0; i < k; ++i) form_used[i] = st.form_used;
+                }
+                hj_batch_destroy(b);
+            }
+        }
+        if (!batched) {
+            for (size_t i = 0; i < k; ++i) {
+                hj_stats st;
+                if (rqs[i].a == rqs[i].b)
+                    status[i] = hj_self_join_count_device(sa[i].ptr, sa[i].dtype_bytes, sa[i].n, sa[i].d, rqs[i].eps,
+                                                          &o, &count[i], &st);
+                else
+                    status[i] = hj_join_count_device(sa[i].ptr, sa[i].n, sb[i].ptr, sb[i].n, sa[i].dtype_bytes,
+                                                     sa[i].d, rqs[i].eps, &o, &count[i], &st);
+                if (status[i] == HJ_OK) {
+                    form_used[i] = st.form_used;
+                    cand[i] = st.candidate_pairs;
+                    band[i] = st.band_pairs;
+                }
+            }
+        }
         {
             std::lock_guard<std::mutex> lk(s->mu);
-            Request &r = s->reqs[id];
-            r.t_end = Clock::now();
-            r.done = true;
-            r.res.count = count;
-            r.res.status = status;
-            r.res.form_used = status == HJ_OK ? st.form_used : -1;
-            r.res.queue_ms = std::chrono::duration<double, std::milli>(r.t_start - r.t_submit).count();
-            r.res.run_ms = std::chrono::duration<double, std::milli>(r.t_end - r.t_start).count();
-            r.res.latency_ms = std::chrono::duration<double, std::milli>(r.t_end - r.t_submit).count();
-            r.res.candidate_pairs = status == HJ_OK ? st.candidate_pairs : 0;
-            r.res.band_pairs = status == HJ_OK ? st.band_pairs : 0;
-            s->mem_in_use -= r.mem;
-            for (uint64_t sid : {r.a, r.b}) {
-                auto it = s->sets.find(sid);
-                if (it != s->sets.end()) {
-                    if (--it->second.users == 0 && it->second.released) {
-                        cudaFree(it->second.ptr);
-                        s->sets.erase(it);
-                    }
-                }
-                if (r.a == r.b) break;
-            }
+            for (size_t i = 0; i < k; ++i) finish_request(s, ids[i], status[i], count[i], form_used[i], cand[i], band[i]);
         }
         s->cv_done.notify_all();
         s->cv_work.notify_all();

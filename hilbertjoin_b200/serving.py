@@ -54,12 +54,16 @@ def _result_dict(r: Result) -> dict:
 
 
 class Server:
-    def __init__(self, form="fp16", memory_budget_bytes: int = 40 << 30, max_inflight: int = 8, device=None):
+    def __init__(self, form="fp16", memory_budget_bytes: int = 40 << 30, max_inflight: int = 8, device=None,
+                 batch_max: int = 1):
+        """batch_max > 1 (tensor-core forms): a free worker runs up to batch_max
+        queued requests as one batch (one persistent launch)."""
         L = _bind()
         o = ServerOpts()
         L.hj_server_opts_init(ctypes.byref(o))
         o.memory_budget_bytes = int(memory_budget_bytes)
         o.max_inflight = int(max_inflight)
+        o.batch_max = int(batch_max)
         o.device = -1 if device is None else int(device)
         o.form = FORMS[form] if isinstance(form, str) else int(form)
         h = ctypes.c_void_p()
@@ -198,7 +202,7 @@ def _summary(res, wall):
 
 
 def run_benchmark(n_requests: int = 2000, form: str = "fp16", max_inflight: int = 8, baseline_requests: int = 200,
-                  seed: int = 5, budget: int = 40 << 30, n_hi: int = 500_000) -> dict:
+                  seed: int = 5, budget: int = 40 << 30, n_hi: int = 500_000, batch_max: int = 8) -> dict:
     sets, reqs = make_workload(n_requests, seed=seed, n_hi=n_hi)
     out = {"workload": f"{n_requests} requests, 70% self / 30% A x B, n log-U[1e3, {n_hi:.0e}], d in {DIMS}, "
                        "uniform or 16-GMM FP32, eps for 8-128 neighbours, sets resident", "form": form}
@@ -209,6 +213,14 @@ def run_benchmark(n_requests: int = 2000, form: str = "fp16", max_inflight: int 
         cap = _summary(res, wall)
         out["saturated"] = cap
         counts = [r["count"] for r in res]
+    if batch_max > 1:  # the same stream with queued requests grouped into batches
+        with Server(form=form, memory_budget_bytes=budget, max_inflight=max_inflight, batch_max=batch_max) as srv:
+            ids = [srv.upload(s["x"]) for s in sets]
+            _replay(srv, ids, reqs[:16], 0)
+            res_bt, wall_bt = _replay(srv, ids, reqs, 0)
+            if [r["count"] for r in res_bt] != counts:
+                raise RuntimeError("batched and unbatched servers disagree")
+            out[f"saturated_batch_max_{batch_max}"] = _summary(res_bt, wall_bt)
     with Server(form="plain", memory_budget_bytes=budget, max_inflight=1) as srv:
         ids = [srv.upload(s["x"]) for s in sets]
         _replay(srv, ids, reqs[:4], 0)

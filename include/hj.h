@@ -277,6 +277,8 @@ HJ_API int hj_batch_create(const hj_batch_job *jobs, uint32_t n_jobs, int dtype_
                            hj_batch **out);
 HJ_API int hj_batch_run(hj_batch *batch, void *stream);
 HJ_API int hj_batch_counts(hj_batch *batch, uint64_t *counts, hj_stats *stats);
+/* Frees the batch; its runs must have finished (hj_batch_counts, or a
+ * synchronisation of the streams and graphs that ran it). */
 HJ_API int hj_batch_destroy(hj_batch *batch);
 /* create + counts + destroy. */
 HJ_API int hj_batch_count_device(const hj_batch_job *jobs, uint32_t n_jobs, int dtype_bytes, const hj_opts *opts,
@@ -294,7 +296,10 @@ typedef struct {
     int32_t max_inflight;         /* concurrent requests on the device (0 = 8) */
     int32_t device;               /* -1 = current */
     int32_t form;                 /* hj_form for every request */
-    int32_t reserved_i;
+    int32_t batch_max;            /* tensor-core forms: a free worker takes up to batch_max queued
+                                     requests (same dtype, within the budget) and runs them as one
+                                     batch (hj_batch_*: one persistent launch); 0 or 1 = one
+                                     request per worker */
     uint64_t reserved[4];
 } hj_server_opts;
 

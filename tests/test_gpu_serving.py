@@ -16,8 +16,8 @@ def hj():
     return hilbertjoin_b200
 
 
-@pytest.mark.parametrize("form", ["tf32", "plain"])
-def test_results_alone_equal_results_in_the_mix(hj, form):
+@pytest.mark.parametrize("form,batch_max", [("tf32", 1), ("plain", 1), ("fp16", 8)])
+def test_results_alone_equal_results_in_the_mix(hj, form, batch_max):
     from hilbertjoin_b200 import serving
     sets, reqs = serving.make_workload(n_requests=60, n_sets=10, seed=11, n_hi=40_000)
     alone = []
@@ -27,7 +27,7 @@ def test_results_alone_equal_results_in_the_mix(hj, form):
             alone.append(hj.self_join_count(a, r["eps"], form=form))
         else:
             alone.append(hj.join_count(a, sets[r["b"]]["x"], r["eps"], form=form))
-    with serving.Server(form=form, max_inflight=6) as srv:
+    with serving.Server(form=form, max_inflight=6, batch_max=batch_max) as srv:
         ids = [srv.upload(s["x"]) for s in sets]
         rids = [srv.submit(ids[r["a"]], None if r["b"] is None else ids[r["b"]], r["eps"]) for r in reqs]
         mix = [srv.wait(i) for i in rids]
