@@ -50,12 +50,9 @@
 
 namespace hj {
 
-#ifndef HJ_EPI_WARPS
-#define HJ_EPI_WARPS 8
-#endif
 // Epilogue warps: kEpiWarps / 4 per TMEM lane quadrant, each on kEpiCols of the
 // 256 accumulator columns, in two chunks of kChunkCols (one TMEM load each).
-constexpr int kEpiWarps = HJ_EPI_WARPS;
+constexpr int kEpiWarps = 8;
 constexpr int kEpiCols = 4 * kTcTileB / kEpiWarps;
 // 8 warps: two 64-column chunks each; 16 warps: one 64-column chunk each
 constexpr int kChunkCols = 64;
@@ -138,23 +135,6 @@ __device__ __forceinline__ void mma_issue(uint32_t tmem_d, uint64_t adesc, uint6
     }
 }
 
-// 32 consecutive accumulator columns of this thread's TMEM lane.
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-}
-
 // 64 consecutive accumulator columns of this thread's TMEM lane (two x32
 // loads, one wait).
 __device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
@@ -178,31 +158,6 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-// 128 consecutive accumulator columns of this thread's TMEM lane (four x32
-// loads, one wait).
-__device__ __forceinline__ void tmem_ld128(uint32_t taddr, float (&v)[128]) {
-    uint32_t r[128];
-#pragma unroll
-    for (int h = 0; h < 4; ++h) {
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-            "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-            "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-            : "=r"(r[32 * h + 0]), "=r"(r[32 * h + 1]), "=r"(r[32 * h + 2]), "=r"(r[32 * h + 3]),
-              "=r"(r[32 * h + 4]), "=r"(r[32 * h + 5]), "=r"(r[32 * h + 6]), "=r"(r[32 * h + 7]),
-              "=r"(r[32 * h + 8]), "=r"(r[32 * h + 9]), "=r"(r[32 * h + 10]), "=r"(r[32 * h + 11]),
-              "=r"(r[32 * h + 12]), "=r"(r[32 * h + 13]), "=r"(r[32 * h + 14]), "=r"(r[32 * h + 15]),
-              "=r"(r[32 * h + 16]), "=r"(r[32 * h + 17]), "=r"(r[32 * h + 18]), "=r"(r[32 * h + 19]),
-              "=r"(r[32 * h + 20]), "=r"(r[32 * h + 21]), "=r"(r[32 * h + 22]), "=r"(r[32 * h + 23]),
-              "=r"(r[32 * h + 24]), "=r"(r[32 * h + 25]), "=r"(r[32 * h + 26]), "=r"(r[32 * h + 27]),
-              "=r"(r[32 * h + 28]), "=r"(r[32 * h + 29]), "=r"(r[32 * h + 30]), "=r"(r[32 * h + 31])
-            : "r"(taddr + 32 * h));
-    }
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 128; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // max(a, b, c) in one instruction (three-input max.f32, sm_100).
@@ -422,13 +377,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         float pf_gmin[kEpiVec];
         auto prefetch = [&](uint32_t b) {
             const uint64_t g = (uint64_t)b * kTcTileB + half * kEpiCols;
-            if constexpr (kEpiVec == 4) {
-                const float4 m = __ldg(reinterpret_cast<const float4 *>(p.gmin_b + g / 32));
-                pf_gmin[0] = m.x, pf_gmin[1] = m.y, pf_gmin[2] = m.z, pf_gmin[3] = m.w;
-            } else {
-                const float2 m = __ldg(reinterpret_cast<const float2 *>(p.gmin_b + g / 32));
-                pf_gmin[0] = m.x, pf_gmin[1] = m.y;
-            }
+            const float4 m = __ldg(reinterpret_cast<const float4 *>(p.gmin_b + g / 32));
+            pf_gmin[0] = m.x, pf_gmin[1] = m.y, pf_gmin[2] = m.z, pf_gmin[3] = m.w;
         };
 #pragma unroll
         for (int q = 0; q < kEpiVec; ++q) pf_gmin[q] = 0.f;
@@ -498,10 +448,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 for (uint32_t c = 0; c < kEpiChunks; ++c) {
                     float v[kChunkCols];
                     const uint32_t taddr = tmem + lane_base + acc * kTcTileB + half * kEpiCols + c * kChunkCols;
-                    if constexpr (kChunkCols == 64)
-                        tmem_ld64(taddr, *reinterpret_cast<float(*)[64]>(v));
-                    else
-                        tmem_ld32(taddr, *reinterpret_cast<float(*)[32]>(v));
+                    tmem_ld64(taddr, v);
                     if (c + 1 == kEpiChunks) {
                         // the last chunk is in registers (its slow path too works from
                         // them): the accumulator goes back to the MMA warp before the
