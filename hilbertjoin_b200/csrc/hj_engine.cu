@@ -347,6 +347,7 @@ struct Prepared {
     int launches = 0;
     double reorder_ms = 0;
     double op_scale = 1.0;  // FP16 form: operand scale 2^s
+    std::vector<double> center_host;
 };
 
 static int prepare_join(Ctx *c, cudaStream_t st, const JoinIn &in, const hj_opts *opts, int form_override,
@@ -442,8 +443,8 @@ static int prepare_join(Ctx *c, cudaStream_t st, const JoinIn &in, const hj_opts
             rmax = std::fmax(rmax, std::fmax(hi - hc[t], hc[t] - lo));
         }
         P->op_scale = rmax > 0 ? std::ldexp(1.0, 14 - std::ilogb(rmax)) : 1.0;
-        cudaMemcpyAsync(center, hc.data(), d * 8, cudaMemcpyHostToDevice, st);
-        cudaStreamSynchronize(st);  // hc goes out of scope
+        P->center_host = hc;  // outlives the asynchronous copy (the join synchronises later)
+        cudaMemcpyAsync(center, P->center_host.data(), d * 8, cudaMemcpyHostToDevice, st);
     }
 
     // 2. EGO sort + layouts
