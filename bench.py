@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="fp16", choices=["fp16", "tf32", "bf16x3", "plain"])
+    ap.add_argument("--form", default=None, choices=["fp16", "tf32", "bf16x3", "plain", "auto"],
+                    help="distance form (default: fp16 for the self-join line, auto for serving and batch)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison step")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--n", type=int, default=N_POINTS, help=argparse.SUPPRESS)
@@ -212,7 +213,7 @@ def run_serving(args):
     import torch
     torch.cuda.set_device(0)
     from hilbertjoin_b200 import serving
-    r = serving.run_benchmark(n_requests=args.requests, form=args.form if args.form != "plain" else "fp16",
+    r = serving.run_benchmark(n_requests=args.requests, form=args.form or "auto",
                               baseline_requests=args.baseline_requests)
     line = {"metric": "join-serving requests/s (p50/p99 latency)", "value": r["saturated"]["requests_per_s"],
             "unit": "requests/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
@@ -226,7 +227,7 @@ def run_batch(args):
     import torch
     torch.cuda.set_device(0)
     from hilbertjoin_b200 import batching
-    r = batching.run_benchmark(form=args.form if args.form != "plain" else "fp16")
+    r = batching.run_benchmark(form=args.form if args.form not in (None, "plain", "auto") else "fp16")
     line = {"metric": "batched joins/s (one persistent launch, graph replay)",
             "value": r["batch_replay"]["jobs_per_s"], "unit": "joins/s", "n_gpus": 1, "higher_is_better": True,
             "data": "synthetic", "config": {"workload": r["workload"], "form": r["form"]}, "batch": r}
@@ -235,6 +236,11 @@ def run_batch(args):
 
 def main():
     args = parse()
+    if args.workload == "selfjoin":
+        if args.form is None:
+            args.form = "fp16"
+        if args.form == "auto":
+            args.form = "fp16"  # the 1M x 64 join is far above the small-join threshold
     if args.workload == "serving":
         return run_serving(args)
     if args.workload == "batch":

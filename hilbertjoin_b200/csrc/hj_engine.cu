@@ -387,7 +387,14 @@ static int prepare_join(Ctx *c, cudaStream_t st, const JoinIn &in, const hj_opts
         unsigned long long bits = c->h_small[0];
         std::memcpy(&maxabs, &bits, 8);
     }
-    if (form == HJ_FORM_AUTO) form = (d <= 256 && maxabs < 1e18) ? HJ_FORM_TC_FP16 : HJ_FORM_PLAIN_FP64;
+    if (form == HJ_FORM_AUTO) {
+        // small joins: the tensor-core form's extra stages (layouts, precision
+        // split, band) cost more than they save below about na * nb * d = 2e10
+        // (measured on B200: d = 16, n = 20k is the crossover)
+        const double work = (double)in.na * (double)(in.self ? in.na : in.nb) * (double)d;
+        const bool small = work <= 2e10 && d <= 128;
+        form = (d <= 256 && maxabs < 1e18 && !small) ? HJ_FORM_TC_FP16 : HJ_FORM_PLAIN_FP64;
+    }
     if (form_is_tc(form) && d > 256) return fail(HJ_ERR_UNSUPPORTED, "tensor-core forms support d <= 256");
     if (form_is_tc(form) && !(maxabs < 1e18)) return fail(HJ_ERR_UNSUPPORTED, "tensor-core forms need |x| < 1e18");
     if (form == HJ_FORM_PLAIN_FP64 && d > 128) return fail(HJ_ERR_UNSUPPORTED, "plain FP64 form supports d <= 128");

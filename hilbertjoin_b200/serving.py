@@ -2,7 +2,7 @@
 against a device-memory budget, and concurrent execution of admitted joins
 (the native loop in csrc/hj_server.cu, bound here with ctypes).
 
-    srv = Server(form="fp16", memory_budget_bytes=40 << 30, max_inflight=8)
+    srv = Server(form="auto", memory_budget_bytes=40 << 30, max_inflight=8)
     a = srv.upload(points_a)                 # stays on the device
     rid = srv.submit(a, None, eps)           # self-join; submit(a, b, eps) for A x B
     res = srv.wait(rid)                      # {"count", "status", "latency_ms", ...}
@@ -54,7 +54,7 @@ def _result_dict(r: Result) -> dict:
 
 
 class Server:
-    def __init__(self, form="fp16", memory_budget_bytes: int = 40 << 30, max_inflight: int = 8, device=None,
+    def __init__(self, form="auto", memory_budget_bytes: int = 40 << 30, max_inflight: int = 8, device=None,
                  batch_max: int = 1):
         """batch_max > 1 (tensor-core forms): a free worker runs up to batch_max
         queued requests as one batch (one persistent launch)."""
@@ -201,7 +201,7 @@ def _summary(res, wall):
             "candidate_pairs_per_s": pairs / wall}
 
 
-def run_benchmark(n_requests: int = 2000, form: str = "fp16", max_inflight: int = 8, baseline_requests: int = 200,
+def run_benchmark(n_requests: int = 2000, form: str = "auto", max_inflight: int = 8, baseline_requests: int = 200,
                   seed: int = 5, budget: int = 40 << 30, n_hi: int = 500_000, batch_max: int = 8) -> dict:
     sets, reqs = make_workload(n_requests, seed=seed, n_hi=n_hi)
     out = {"workload": f"{n_requests} requests, 70% self / 30% A x B, n log-U[1e3, {n_hi:.0e}], d in {DIMS}, "

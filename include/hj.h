@@ -68,7 +68,8 @@ typedef enum {
      * a_hi.b_hi + a_hi.b_lo + a_lo.b_hi (a = a_hi + a_lo), FP32 accumulation. */
     HJ_FORM_TC_BF16X3 = 2,
     /* HJ_FORM_TC_FP16 when the input allows it (d <= 256, coordinates within
-     * +-1e18), else HJ_FORM_PLAIN_FP64. */
+     * +-1e18) and the join is not small (na * nb * d > 2e10, where the plain
+     * form's fewer stages measured faster), else HJ_FORM_PLAIN_FP64. */
     HJ_FORM_AUTO = 3,
     /* As TF32 with FP16 operands at twice the tensor-core rate: the centred
      * coordinates are scaled by a power of two 2^s (exact) so that the largest

@@ -105,3 +105,21 @@ def test_fp16_scaling_extremes(hj):
     z = rng.standard_normal((3000, 40)) * 1e-9
     eps = 4e-9
     assert hj.self_join_count(z, eps, form="fp16") == oracle.self_count_brute(z, eps)
+
+
+def test_auto_form_picks_by_size_and_stays_exact(hj):
+    """auto: the plain FP64 form for small joins (na * nb * d <= 2e10, where its
+    fewer stages are faster), FP16 above; the count is the plain form's."""
+    from hilbertjoin_b200 import workloads as W
+    small = W.uniform(5000, 16, 61, dtype=np.float32)
+    eps_s = W.calibrate_eps(small, 5000, 16)
+    c, st = hj.self_join_count(small, eps_s, form="auto", return_stats=True)
+    assert st["form_used"] == "plain_fp64" and c == hj.self_join_count(small, eps_s)
+    big = W.uniform(60000, 16, 62, dtype=np.float32)
+    eps_b = W.calibrate_eps(big, 60000, 16)
+    c, st = hj.self_join_count(big, eps_b, form="auto", return_stats=True)
+    assert st["form_used"] == "tc_fp16" and c == hj.self_join_count(big, eps_b)
+    wide = W.uniform(3000, 200, 63, dtype=np.float32)  # d > 128: the plain form does not apply
+    eps_w = W.calibrate_eps(wide, 3000, 16)
+    c, st = hj.self_join_count(wide, eps_w, form="auto", return_stats=True)
+    assert st["form_used"] == "tc_fp16" and c == hj.self_join_count(wide, eps_w, form="bf16x3")
