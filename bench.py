@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--form", default=None, choices=["fp16", "tf32", "bf16x3", "plain", "auto"],
-                    help="distance form (default: fp16 for the self-join line, auto for serving and batch)")
+                    help="distance form (default: fp16 for the self-join and batch lines, auto for serving)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison step")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--n", type=int, default=N_POINTS, help=argparse.SUPPRESS)
