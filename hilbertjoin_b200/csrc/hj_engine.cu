@@ -397,7 +397,7 @@ static int prepare_join(Ctx *c, cudaStream_t st, const JoinIn &in, const hj_opts
     }
     if (form_is_tc(form) && d > 256) return fail(HJ_ERR_UNSUPPORTED, "tensor-core forms support d <= 256");
     if (form_is_tc(form) && !(maxabs < 1e18)) return fail(HJ_ERR_UNSUPPORTED, "tensor-core forms need |x| < 1e18");
-    if (form == HJ_FORM_PLAIN_FP64 && d > 128) return fail(HJ_ERR_UNSUPPORTED, "plain FP64 form supports d <= 128");
+    if (form == HJ_FORM_PLAIN_FP64 && d > 256) return fail(HJ_ERR_UNSUPPORTED, "plain FP64 form supports d <= 256");
     std::vector<uint32_t> ord;
     if (opts && opts->reorder_dims && d > 1) {
         auto t0 = std::chrono::steady_clock::now();
@@ -812,7 +812,7 @@ static int pairs_host(const void *a, uint64_t na, const void *b, uint64_t nb, in
     if (!n_pairs || (capacity && !pairs) || (na && !a) || (!self && nb && !b))
         return fail(HJ_ERR_INVALID_ARG, "null pointer");
     if (int r = validate(na, nb, d, eps)) return r;
-    if (d > 128) return fail(HJ_ERR_UNSUPPORTED, "pair output supports d <= 128 (plain FP64 form)");
+    if (d > 256) return fail(HJ_ERR_UNSUPPORTED, "pair output supports d <= 256 (plain FP64 form)");
     Ctx *c;
     if (int r = get_ctx(opts ? opts->device : -1, &c)) return r;
     cudaStream_t st = (opts && opts->stream) ? (cudaStream_t)opts->stream : c->stream;

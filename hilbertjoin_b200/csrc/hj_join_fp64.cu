@@ -10,7 +10,8 @@
 // ranks against a run of B tiles of 64 ranks) in Hilbert order. The A tile is
 // staged once per item and the B tiles are double-buffered, each by one 1D
 // bulk copy (cp.async.bulk, the non-tensor TMA) of its [d][64] FP64 block into
-// shared memory, completion tracked by mbarriers. Each thread owns a 4 x 4
+// shared memory (above d = 128 by 64-dim chunks, which keeps d <= 256 within
+// 192 KB), completion tracked by mbarriers. Each thread owns a 4 x 4
 // block of pairs and evaluates the pair test exactly as the oracle defines it:
 // acc = fma(a_k - b_k, a_k - b_k, acc) in IEEE FP64, k = 0..d-1 in order,
 // count iff acc <= eps*eps. The partial sums never decrease, so a warp whose
@@ -51,6 +52,15 @@ enum PlainMode { kModeCount = 0, kModeItemCounts = 1, kModeEmit = 2 };
 constexpr int kPlainThreads = 256;
 constexpr int kPlainWarps = kPlainThreads / 32;
 
+// Dims per B stage: the whole tile up to d = 128; above, 64-dim chunks, so that
+// the A tile (d <= 256: at most 128 KB) and two B stages fit one CTA's smem.
+__host__ __device__ constexpr uint32_t plain_chunk_dims(uint32_t d) { return d <= 128 ? d : 64; }
+constexpr uint32_t kPlainMaxDims = 256;
+
+__host__ __device__ constexpr size_t plain_smem_bytes(uint32_t d) {
+    return ((size_t)d + 2 * plain_chunk_dims(d)) * kPlainTile * sizeof(double);
+}
+
 // Waits for a bulk copy to land regardless of the error word, bounded in time:
 // used only to drain copies still in flight before the CTA exits.
 __device__ __forceinline__ void drain_wait(uint64_t *bar, uint32_t parity) {
@@ -60,15 +70,33 @@ __device__ __forceinline__ void drain_wait(uint64_t *bar, uint32_t parity) {
     }
 }
 
+// One dimension of a thread's 4 x 4 pair block: acc[i][j] += (a_i - b_j)^2,
+// rounded as the pair test defines it (one FP64 subtract, one FMA).
+__device__ __forceinline__ void fma_dim(const double *pa, const double *pb, double (&acc)[4][4]) {
+    const double2 a01 = *reinterpret_cast<const double2 *>(pa);
+    const double2 a23 = *reinterpret_cast<const double2 *>(pa + 2);
+    const double2 b01 = *reinterpret_cast<const double2 *>(pb);
+    const double2 b23 = *reinterpret_cast<const double2 *>(pb + 2);
+    const double av[4] = {a01.x, a01.y, a23.x, a23.y};
+    const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double df = __dsub_rn(av[i], bv[j]);
+            acc[i][j] = __fma_rn(df, df, acc[i][j]);
+        }
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(kPlainThreads, 2) k_join_fp64(PlainArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar_a, bar_full[2], bar_empty[2];
     const uint32_t d = a.d;
+    const uint32_t kc = plain_chunk_dims(d);  // dims per B stage
     const uint32_t tile_elems = d * kPlainTile;
-    const uint32_t tile_bytes = tile_elems * 8u;
     double *sA = reinterpret_cast<double *>(smem_raw);
-    double *sB[2] = {sA + tile_elems, sA + 2 * tile_elems};
+    double *sB[2] = {sA + tile_elems, sA + tile_elems + kc * kPlainTile};
     const uint32_t tid = threadIdx.x, lane = tid & 31u;
     const uint32_t ty = tid >> 4, tx = tid & 15u;
     volatile uint32_t *err = a.err;
@@ -83,9 +111,11 @@ __global__ void __launch_bounds__(kPlainThreads, 2) k_join_fp64(PlainArgs a) {
     }
     __syncthreads();
 
-    // Producer state (thread 0): the next B tile to load in this CTA's sequence.
+    // Producer state (thread 0): the next (B tile, dim chunk) to load in this
+    // CTA's sequence; the chunk at dim k0 of a tile is the contiguous [kc][64]
+    // block at row k0 of the tile's [d][64] layout.
     uint64_t p_item = blockIdx.x;
-    uint32_t p_bt = 0, p_end = 0;
+    uint32_t p_bt = 0, p_end = 0, p_k0 = 0;
     uint32_t issued = 0;
     if (tid == 0 && p_item < a.n_items) {
         WorkItem w = a.items[p_item];
@@ -98,9 +128,12 @@ __global__ void __launch_bounds__(kPlainThreads, 2) k_join_fp64(PlainArgs a) {
         while (p_item < a.n_items && issued < consumed + 2) {
             const uint32_t s = issued & 1u, u = issued >> 1;
             if (u >= 1) mbar_wait(&bar_empty[s], (u - 1) & 1u, err);
-            mbar_arrive_expect_tx(&bar_full[s], tile_bytes);
-            bulk_g2s(sB[s], a.B + (uint64_t)p_bt * tile_elems, tile_bytes, &bar_full[s]);
+            const uint32_t bytes = (d - p_k0 < kc ? d - p_k0 : kc) * kPlainTile * 8u;
+            mbar_arrive_expect_tx(&bar_full[s], bytes);
+            bulk_g2s(sB[s], a.B + (uint64_t)p_bt * tile_elems + p_k0 * kPlainTile, bytes, &bar_full[s]);
             ++issued;
+            if ((p_k0 += kc) < d) continue;
+            p_k0 = 0;
             if (++p_bt >= p_end) {
                 p_item += gridDim.x;
                 if (p_item < a.n_items) {
@@ -120,69 +153,50 @@ __global__ void __launch_bounds__(kPlainThreads, 2) k_join_fp64(PlainArgs a) {
         const WorkItem w = a.items[it];
         __syncthreads();  // all warps are done with the previous A tile
         if (tid == 0) {
-            mbar_arrive_expect_tx(&bar_a, tile_bytes);
-            bulk_g2s(sA, a.A + (uint64_t)w.a * tile_elems, tile_bytes, &bar_a);
+            mbar_arrive_expect_tx(&bar_a, tile_elems * 8u);
+            bulk_g2s(sA, a.A + (uint64_t)w.a * tile_elems, tile_elems * 8u, &bar_a);
         }
         mbar_wait(&bar_a, a_phase, err);
         a_phase ^= 1u;
         const uint64_t ia0 = (uint64_t)w.a * kPlainTile + ty * 4;
         for (uint32_t bt = w.b0; bt < w.b1; ++bt) {
-            const uint32_t s = consumed & 1u;
-            if (tid == 0) issue_next(consumed);
-            mbar_wait(&bar_full[s], (consumed >> 1) & 1u, err);
-            const double *pa = sA + ty * 4;
-            const double *pb = sB[s] + tx * 4;
             double acc[4][4];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-            uint32_t k = 0;
-            while (k < d) {
-                const uint32_t kend = k + 8 <= d ? k + 8 : d;
-                if (kend - k == 8) {
+            bool live = true;  // some pair of this warp may still qualify
+            for (uint32_t c0 = 0; c0 < d; c0 += kc) {
+                const uint32_t s = consumed & 1u;
+                if (tid == 0) issue_next(consumed);
+                mbar_wait(&bar_full[s], (consumed >> 1) & 1u, err);
+                const uint32_t c1 = c0 + kc < d ? c0 + kc : d;
+                const double *pa = sA + ty * 4;
+                const double *pb = sB[s] + tx * 4;
+                for (uint32_t k = c0; live && k < c1;) {
+                    const uint32_t kend = k + 8 <= c1 ? k + 8 : c1;
+                    const double *pak = pa + k * kPlainTile, *pbk = pb + (k - c0) * kPlainTile;
+                    if (kend - k == 8) {
 #pragma unroll
-                    for (int kk = 0; kk < 8; ++kk) {
-                        const double2 a01 = *reinterpret_cast<const double2 *>(pa + (k + kk) * kPlainTile);
-                        const double2 a23 = *reinterpret_cast<const double2 *>(pa + (k + kk) * kPlainTile + 2);
-                        const double2 b01 = *reinterpret_cast<const double2 *>(pb + (k + kk) * kPlainTile);
-                        const double2 b23 = *reinterpret_cast<const double2 *>(pb + (k + kk) * kPlainTile + 2);
-                        const double av[4] = {a01.x, a01.y, a23.x, a23.y};
-                        const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+                        for (int kk = 0; kk < 8; ++kk) fma_dim(pak + kk * kPlainTile, pbk + kk * kPlainTile, acc);
+                    } else {
+                        for (uint32_t kk = 0; kk < kend - k; ++kk) fma_dim(pak + kk * kPlainTile, pbk + kk * kPlainTile, acc);
+                    }
+                    k = kend;
+                    if (k < d) {
+                        bool any = false;
 #pragma unroll
                         for (int i = 0; i < 4; ++i)
 #pragma unroll
-                            for (int j = 0; j < 4; ++j) {
-                                const double df = __dsub_rn(av[i], bv[j]);
-                                acc[i][j] = __fma_rn(df, df, acc[i][j]);
-                            }
-                    }
-                } else {
-                    for (uint32_t kk = k; kk < kend; ++kk) {
-                        const double2 a01 = *reinterpret_cast<const double2 *>(pa + kk * kPlainTile);
-                        const double2 a23 = *reinterpret_cast<const double2 *>(pa + kk * kPlainTile + 2);
-                        const double2 b01 = *reinterpret_cast<const double2 *>(pb + kk * kPlainTile);
-                        const double2 b23 = *reinterpret_cast<const double2 *>(pb + kk * kPlainTile + 2);
-                        const double av[4] = {a01.x, a01.y, a23.x, a23.y};
-                        const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
-#pragma unroll
-                        for (int i = 0; i < 4; ++i)
-#pragma unroll
-                            for (int j = 0; j < 4; ++j) {
-                                const double df = __dsub_rn(av[i], bv[j]);
-                                acc[i][j] = __fma_rn(df, df, acc[i][j]);
-                            }
+                            for (int j = 0; j < 4; ++j) any |= acc[i][j] <= T;
+                        live = __any_sync(0xffffffffu, any);
                     }
                 }
-                k = kend;
-                if (k < d) {
-                    bool live = false;
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) live |= acc[i][j] <= T;
-                    if (!__any_sync(0xffffffffu, live)) break;
-                }
+                // a warp that stopped early still waits for and releases every
+                // chunk of this tile, so the stage sequence stays in step
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bar_empty[s]);
+                ++consumed;
             }
             const uint64_t jb0 = (uint64_t)bt * kPlainTile + tx * 4;
             uint32_t hits = 0;  // bit 4i+j: pair (i, j) of this thread's block qualifies
@@ -194,9 +208,6 @@ __global__ void __launch_bounds__(kPlainThreads, 2) k_join_fp64(PlainArgs a) {
                     const bool valid = pi < a.na && pj < a.nb && (!a.self || pj > pi);
                     hits |= (valid && acc[i][j] <= T) ? 1u << (4 * i + j) : 0u;
                 }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&bar_empty[s]);
-            ++consumed;
             const uint32_t nh = __popc(hits);
             if (MODE != kModeEmit) {
                 cnt += nh;
@@ -245,9 +256,10 @@ __global__ void __launch_bounds__(kPlainThreads, 2) k_join_fp64(PlainArgs a) {
 
 template <int MODE>
 static void launch_plain(const PlainArgs &a, uint64_t n_items, int num_sms, cudaStream_t st) {
-    const size_t smem = (size_t)3 * a.d * kPlainTile * sizeof(double);
-    // the largest this kernel ever needs (d <= 128), set once
-    ensure_max_dynamic_smem((const void *)k_join_fp64<MODE>, 3 * 128 * kPlainTile * (int)sizeof(double));
+    const size_t smem = plain_smem_bytes(a.d);
+    // the largest this kernel ever needs (d = 128 and d = 256 both take 192 KB), set once
+    static_assert(plain_smem_bytes(128) == plain_smem_bytes(kPlainMaxDims), "plain smem maximum");
+    ensure_max_dynamic_smem((const void *)k_join_fp64<MODE>, (int)plain_smem_bytes(kPlainMaxDims));
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_join_fp64<MODE>, kPlainThreads, smem);
     if (per_sm < 1) per_sm = 1;

@@ -58,7 +58,7 @@ typedef enum {
 typedef enum {
     /* FP64 direct difference on CUDA cores, early exit every 8 dims once all
      * pairs of a warp exceed eps^2 (the reference's KBLOCK early exit,
-     * hilbertjoin/egojoin.h:350-359). The drop-in form. */
+     * hilbertjoin/egojoin.h:350-359). The drop-in form; d <= 256. */
     HJ_FORM_PLAIN_FP64 = 0,
     /* dist^2 = |a|^2 + |b|^2 - 2 a.b with a.b on tcgen05 tensor cores in TF32
      * (operands rounded to TF32, FP32 accumulation); every pair within a
@@ -167,7 +167,7 @@ HJ_API int hj_join_count_f32(const float *A, uint64_t nA, const float *B, uint64
  * i < j; two-set joins list (index in A, index in B). Sorted by (i, j).
  * The reference pushes indices into its EGO-sorted array; these are indices
  * into the caller's unsorted input. Always computed by the plain FP64 form
- * (d <= 128; opts->form is ignored), so the pairs are exactly the ones the
+ * (d <= 256; opts->form is ignored), so the pairs are exactly the ones the
  * count functions count. If more than `capacity` pairs qualify nothing is
  * written, *n_pairs is set to the number and HJ_ERR_CAPACITY is returned
  * (capacity 0 with pairs NULL asks for the number alone). */

@@ -43,11 +43,8 @@ def make_jobs(torch, seed=0, dtype=np.float32):
 
 
 def alone(hj, job, form):
-    """The job run on its own; "plain" means the FP64 form where it applies
-    (d <= 128) and the BF16x3 form above that (exact as well)."""
+    """The job run on its own in the given form ("plain": the FP64 form)."""
     a, b, eps = job
-    if form == "plain" and a.shape[1] > 128:
-        form = "bf16x3"
     return hj.self_join_count(a, eps, form=form) if b is None else hj.join_count(a, b, eps, form=form)
 
 

@@ -33,6 +33,8 @@ SELF_CASES = [  # n, d, target neighbours, dtype, seed
     (4099, 33, 24, np.float64, 6),
     (6000, 64, 64, np.float32, 7),
     (2500, 128, 16, np.float64, 8),
+    (2100, 129, 16, np.float32, 9),   # above 128: B tiles in 64-dim chunks
+    (1900, 256, 16, np.float64, 10),
 ]
 
 
@@ -54,6 +56,7 @@ JOIN_CASES = [  # nA, nB, d, target, dtype, seed
     (2000, 3333, 12, 16, np.float64, 13),
     (4100, 900, 40, 32, np.float32, 14),
     (1500, 1500, 100, 16, np.float64, 15),
+    (1200, 1700, 200, 16, np.float32, 16),
 ]
 
 
@@ -173,5 +176,8 @@ def test_pairs_medium_size_properties(hj):
 
 
 def test_pairs_reject_large_d(hj):
+    """The plain FP64 kernel, which lists the pairs, covers d <= 256."""
     with pytest.raises(hj.HJError):
-        hj.self_join_pairs(np.zeros((10, 129)), 0.1)
+        hj.self_join_pairs(np.zeros((10, 257)), 0.1)
+    with pytest.raises(hj.HJError):
+        hj.self_join_count(np.zeros((10, 257)), 0.1, form="plain")

@@ -88,6 +88,31 @@ def test_forms_agree_dense(hj):
         assert hj.self_join_count(x, eps, form=form) == want, form
 
 
+@pytest.mark.parametrize("d", [160, 256])
+def test_wide_ill_conditioned_routes_to_fp64(hj, d):
+    """Two unit-variance clusters 1000 apart in every dim, at d > 128: the
+    centred squared norms (~d * 500^2) dwarf eps^2 (~2d), so the tensor-core
+    bound is far too wide and the work items are routed to the plain FP64
+    kernel, which runs d > 128 by 64-dim chunks of the B tiles. Counts stay the
+    FP64 counts."""
+    rng = np.random.default_rng(1017)
+
+    def pts(n):
+        return (1000.0 * rng.integers(0, 2, n)[:, None] + rng.standard_normal((n, d))).astype(np.float32)
+
+    a, b = pts(2939), pts(2917)
+    s = a[:400].astype(np.float64)
+    eps = float(np.sqrt(np.quantile(exact_dist2(s, s)[np.triu_indices(400, 1)], 0.1)))
+    want_j = oracle.join_count_brute(a.astype(np.float64), b.astype(np.float64), eps)
+    want_s = oracle.self_count_brute(a.astype(np.float64), eps)
+    for form in ("fp16", "tf32", "bf16x3", "plain"):
+        got, st = hj.join_count(a, b, eps, form=form, return_stats=True)
+        assert got == want_j, form
+        if form != "plain":
+            assert st["fp64_items"] > 0, form
+        assert hj.self_join_count(a, eps, form=form) == want_s, form
+
+
 def test_fp16_scaling_extremes(hj):
     """FP16 operands are scaled so the largest centred coordinate lands in
     [2^14, 2^15): a dim whose range dwarfs the others drives the small ones
@@ -119,7 +144,7 @@ def test_auto_form_picks_by_size_and_stays_exact(hj):
     eps_b = W.calibrate_eps(big, 60000, 16)
     c, st = hj.self_join_count(big, eps_b, form="auto", return_stats=True)
     assert st["form_used"] == "tc_fp16" and c == hj.self_join_count(big, eps_b)
-    wide = W.uniform(3000, 200, 63, dtype=np.float32)  # d > 128: the plain form does not apply
+    wide = W.uniform(3000, 200, 63, dtype=np.float32)  # d > 128: auto takes FP16 at any size
     eps_w = W.calibrate_eps(wide, 3000, 16)
     c, st = hj.self_join_count(wide, eps_w, form="auto", return_stats=True)
-    assert st["form_used"] == "tc_fp16" and c == hj.self_join_count(wide, eps_w, form="bf16x3")
+    assert st["form_used"] == "tc_fp16" and c == hj.self_join_count(wide, eps_w)
