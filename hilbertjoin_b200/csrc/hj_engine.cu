@@ -129,7 +129,9 @@ static int get_ctx(int device, Ctx **out) {
     return HJ_OK;
 }
 
-// Slot ids (index-stage slots 40..49 live in hj_index.cu).
+// Slot ids. The index stage's slots (hj_index.cu) start at kSlotIndexFirst;
+// the two ranges must not meet, or a buffer of one stage is freed while the
+// other still reads it.
 enum {
     kSlotInA = 1, kSlotInB, kSlotDimStats, kSlotGridOff, kSlotGridBits, kSlotGridWord, kSlotGridShift,
     kSlotKeysWmA, kSlotKeysWmB, kSlotPermA, kSlotPermB, kSlotPermTmp, kSlotHist,
@@ -138,7 +140,9 @@ enum {
     kSlotTmaxAA, kSlotTmaxAB, kSlotTmaxBA, kSlotTmaxBB, kSlotBand, kSlotCenter, kSlotGminA, kSlotGminB,
     kSlotItemCnt, kSlotPairKeys, kSlotPairPerm, kSlotPairTmp, kSlotPairHist, kSlotPairOut, kSlotDimCost,
     kSlotGridOrd,
+    kSlotEngineEnd
 };
+static_assert(kSlotEngineEnd <= kSlotIndexFirst, "engine slots overlap the index stage's");
 
 static int bitwidth(unsigned long long v) {
     int b = 0;
@@ -560,6 +564,18 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
             launches += 2;
             fp_items = idx_fp.n_items;
             cudaMemsetAsync(c->d_small + 2, 0, 5 * sizeof(unsigned long long), st);
+            if (attempt == 0 && idx_tc.n_items == 0 && idx_fp.n_items && !(opts && opts->shard_count > 1)) {
+                // Every item is routed to FP64: the plain form's own work list
+                // (64 x 64 tiles, stripes per 64-rank tile) holds fewer candidate
+                // pairs than the tensor-core one, so it replaces it.
+                const uint32_t chunk = (opts && opts->item_chunk > 0) ? (uint32_t)opts->item_chunk : 16u;
+                std::string ierr;
+                int ir = build_index(A, B, P.g, P.gd, in.self, na_eff, nb_eff, kPlainTile, kPlainTile, active_dims,
+                                     chunk, slot_alloc_cb, &actx, st, &idx, &launches, &ierr);
+                if (ir == 2) return fail(HJ_ERR_OOM, ierr);
+                if (ir) return fail(HJ_ERR_CUDA, ierr);
+                idx_fp = idx;
+            }
             if (idx_fp.n_items) {
                 if (int rr = ensure_plain_tiles(c, st, &A, false, &launches)) return rr;
                 if (in.self)

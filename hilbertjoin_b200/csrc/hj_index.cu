@@ -306,9 +306,10 @@ __global__ void k_permute_items(const WorkItem *__restrict__ in, const uint32_t 
 }
 
 // Scratch slots requested through the caller's allocator.
-enum { kSlotRuns = 40, kSlotNruns, kSlotCounts, kSlotItemsTmp, kSlotItems, kSlotItemKeys, kSlotItemPerm,
+enum { kSlotRuns = kSlotIndexFirst, kSlotNruns, kSlotCounts, kSlotItemsTmp, kSlotItems, kSlotItemKeys, kSlotItemPerm,
        kSlotItemPermTmp, kSlotItemHist, kSlotIdxStats, kSlotSplitFlags, kSlotSplitTc, kSlotSplitFp, kSlotSplitStats,
-       kSlotShardLoad, kSlotShardCut };
+       kSlotShardLoad, kSlotShardCut, kSlotIndexEnd };
+static_assert(kSlotIndexEnd <= kSlotIndexFirst + 32, "index-stage slots");
 
 __global__ void k_item_loads(const WorkItem *__restrict__ items, uint64_t n, uint32_t *load) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;

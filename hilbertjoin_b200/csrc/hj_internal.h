@@ -119,6 +119,10 @@ struct WorkItem {
 // error bound c_rel * (max |a|^2 + max |b|^2) + c_abs exceeds `limit` go, as
 // 64 x 64 items, to the plain FP64 kernel. Order (Hilbert) is preserved in both
 // lists. Synchronises once on `st`.
+// First scratch-slot id of the index stage (build_index, the precision split,
+// sharding); the engine's own slot ids stay below it.
+constexpr int kSlotIndexFirst = 64;
+
 struct IndexResult;
 int split_items_by_precision(const IndexResult &tc_in, const SortedSet &A, const SortedSet &B, double c_rel,
                              double c_abs, double limit, void *(*alloc)(void *ctx, int slot, size_t bytes),

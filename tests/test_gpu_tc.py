@@ -105,12 +105,18 @@ def test_wide_ill_conditioned_routes_to_fp64(hj, d):
     eps = float(np.sqrt(np.quantile(exact_dist2(s, s)[np.triu_indices(400, 1)], 0.1)))
     want_j = oracle.join_count_brute(a.astype(np.float64), b.astype(np.float64), eps)
     want_s = oracle.self_count_brute(a.astype(np.float64), eps)
+    _, plain_j = hj.join_count(a, b, eps, form="plain", return_stats=True)
+    _, plain_s = hj.self_join_count(a, eps, form="plain", return_stats=True)
     for form in ("fp16", "tf32", "bf16x3", "plain"):
         got, st = hj.join_count(a, b, eps, form=form, return_stats=True)
         assert got == want_j, form
+        got_s, st_s = hj.self_join_count(a, eps, form=form, return_stats=True)
+        assert got_s == want_s, form
         if form != "plain":
-            assert st["fp64_items"] > 0, form
-        assert hj.self_join_count(a, eps, form=form) == want_s, form
+            # every item routed: the join runs on the plain form's finer work list
+            assert st["fp64_items"] > 0 and st_s["fp64_items"] > 0, form
+            assert st["candidate_pairs"] == plain_j["candidate_pairs"], form
+            assert st_s["candidate_pairs"] == plain_s["candidate_pairs"], form
 
 
 def test_fp16_scaling_extremes(hj):
