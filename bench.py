@@ -321,7 +321,7 @@ def main():
         e2e_ms = float(t.item())
     assert ce == counts[0]
 
-    # the plain FP64 form on the same input (the north star's comparison)
+    # the plain FP64 form on the same input: the tensor-core form's speed-up over it
     plain = None
     if not args.no_plain and args.form != "plain" and rank == 0:
         step_dev("plain")
