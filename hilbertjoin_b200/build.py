@@ -38,13 +38,31 @@ def _newer(target: str, deps) -> bool:
 
 
 def build_lib(verbose: bool = False, force: bool = False) -> str:
+    """Compiles every CUDA source to an object (in parallel; a source is
+    recompiled when it, a header or the C ABI changed) and links libhj.so."""
+    from concurrent.futures import ThreadPoolExecutor
     srcs = [os.path.join(CSRC, s) for s in CU_SOURCES if os.path.exists(os.path.join(CSRC, s))]
-    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    deps.append(os.path.join(ROOT, "include", "hj.h"))
-    if not force and not _newer(LIB, deps):
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    headers.append(os.path.join(ROOT, "include", "hj.h"))
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs = [os.path.join(objdir, os.path.basename(s)[:-3] + ".o") for s in srcs]
+    todo = [(s, o) for s, o in zip(srcs, objs) if force or _newer(o, [s, *headers])]
+    if not todo and not _newer(LIB, objs):
         return LIB
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
-    cmd = [_nvcc(), *GENCODE, *NVCC_FLAGS, "-shared", "-o", LIB + ".tmp", *srcs, "-lpthread"]
+
+    def compile_one(so):
+        s, o = so
+        cmd = [_nvcc(), *GENCODE, *NVCC_FLAGS, "-c", "-o", o + ".tmp", s]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        os.replace(o + ".tmp", o)
+
+    with ThreadPoolExecutor(max_workers=min(8, max(1, len(todo)))) as ex:
+        list(ex.map(compile_one, todo))
+    cmd = [_nvcc(), *GENCODE, "-shared", "-o", LIB + ".tmp", *objs, "-lpthread"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -944,6 +944,8 @@ static int dim_order_host(const double *pts, uint64_t n, uint32_t d, double eps,
 
 int engine_fail(int code, const std::string &msg) { return fail(code, msg); }
 
+void engine_clear_error() { tl_error.clear(); }
+
 int engine_prepare_job(cudaStream_t st_in, const void *a, const void *b, uint64_t na, uint64_t nb, int dtype_bytes,
                        uint32_t d, double eps, bool self, const hj_opts *opts, int form, PreparedJob *out) {
     if (!form_is_tc(form)) return fail(HJ_ERR_INVALID_ARG, "a batch runs a tensor-core form");

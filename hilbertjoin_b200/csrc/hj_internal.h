@@ -276,6 +276,8 @@ int engine_prepare_job(cudaStream_t st, const void *a, const void *b, uint64_t n
 int batch_job_candidates(const hj_batch *b, uint64_t *out);
 // Sets the calling thread's last error text and returns code.
 int engine_fail(int code, const std::string &msg);
+// Clears this host thread's error text (hj_last_error) at the start of a call.
+void engine_clear_error();
 // Norm summaries over a row-major norm array of npad rows (padding rows hold
 // kPadNorm): per 128-row and per 256-row tile maxima, per 32-row minima.
 void launch_norm_summaries(const float *norms, uint64_t npad, float *tmax128, float *tmax256, float *gmin32,

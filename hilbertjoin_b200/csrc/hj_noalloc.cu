@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <string>
 
 #include "../../include/hj.h"
 #include "hj_common.cuh"
@@ -45,7 +46,8 @@ int scratch_address(int dev, unsigned char **out) {
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
             cudaGetLastError();
-            return HJ_ERR_CUDA;
+            return engine_fail(HJ_ERR_CUDA, std::string("cudaGetSymbolAddress of the scratch array failed: ") +
+                                                cudaGetErrorString(e));
         }
         g_addr[dev] = static_cast<unsigned char *>(p);
     }
@@ -68,9 +70,12 @@ using namespace hj;
 
 extern "C" int hj_ego_sort_device_noalloc(const void *pts, int dtype_bytes, uint64_t n, uint32_t d, double eps,
                                           uint32_t *perm, void *stream) {
-    if (!perm || (n && !pts) || (dtype_bytes != 4 && dtype_bytes != 8) || d == 0 || d > kMaxDim ||
-        n >= (1ull << 31) || !(eps > 0.0) || !std::isfinite(eps))
-        return HJ_ERR_INVALID_ARG;
+    engine_clear_error();
+    if (!perm || (n && !pts)) return engine_fail(HJ_ERR_INVALID_ARG, "null pointer");
+    if (dtype_bytes != 4 && dtype_bytes != 8) return engine_fail(HJ_ERR_INVALID_ARG, "dtype_bytes must be 4 or 8");
+    if (d == 0 || d > kMaxDim) return engine_fail(HJ_ERR_INVALID_ARG, "d out of range");
+    if (n >= (1ull << 31)) return engine_fail(HJ_ERR_INVALID_ARG, "n must be below 2^31");
+    if (!(eps > 0.0) || !std::isfinite(eps)) return engine_fail(HJ_ERR_INVALID_ARG, "eps must be finite and > 0");
     if (n == 0) return HJ_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // scratch layout: stats | maxabs, bad | off | bits | word | shift | keys [W][n] | perm2 [n] | hist
@@ -83,11 +88,12 @@ extern "C" int hj_ego_sort_device_noalloc(const void *pts, int dtype_bytes, uint
     const size_t o_keys = align256(o_shift + (size_t)d * 4);
     const size_t hist_bytes = radix_hist_entries(n) * 4;
     // at least one key word: reject before touching the device when even that does not fit
-    if (o_keys + align256(n * 4) + align256(n * 4) + hist_bytes > kScratchBytes) return HJ_ERR_INVALID_ARG;
+    if (o_keys + align256(n * 4) + align256(n * 4) + hist_bytes > kScratchBytes)
+        return engine_fail(HJ_ERR_INVALID_ARG, "n too large for the fixed 32 MiB scratch array");
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         cudaGetLastError();
-        return HJ_ERR_NO_DEVICE;
+        return engine_fail(HJ_ERR_NO_DEVICE, "no usable CUDA device");
     }
     unsigned char *base = nullptr;
     if (int r = scratch_address(dev, &base)) return r;
@@ -102,11 +108,12 @@ extern "C" int hj_ego_sort_device_noalloc(const void *pts, int dtype_bytes, uint
     uint32_t hbad = 0;
     cudaMemcpyAsync(hds, ds, d * sizeof(DimStats), cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(&hbad, d_bad, 4, cudaMemcpyDeviceToHost, st);
-    if (cudaStreamSynchronize(st) != cudaSuccess) {
+    if (cudaError_t e = cudaStreamSynchronize(st)) {
         cudaGetLastError();
-        return HJ_ERR_CUDA;
+        return engine_fail(HJ_ERR_CUDA, std::string("cell statistics: ") + cudaGetErrorString(e));
     }
-    if (hbad) return HJ_ERR_INVALID_ARG;
+    if (hbad & 1u) return engine_fail(HJ_ERR_INVALID_ARG, "input holds a non-finite coordinate");
+    if (hbad) return engine_fail(HJ_ERR_INVALID_ARG, "a cell index floor(x/eps) exceeds 2^62");
 
     // 2. packed key layout (same rule as the allocating path)
     long long off[kMaxDim];
@@ -117,7 +124,8 @@ extern "C" int hj_ego_sort_device_noalloc(const void *pts, int dtype_bytes, uint
         long long lo = hds[t].cmin, hi = hds[t].cmax;
         if (lo > hi) lo = hi = 0;
         range[t] = hi - lo;
-        if (range[t] < 0 || range[t] > (1ll << 30)) return HJ_ERR_INVALID_ARG;
+        if (range[t] < 0 || range[t] > (1ll << 30))
+            return engine_fail(HJ_ERR_INVALID_ARG, "a dimension spans more than 2^30 cells");
         const uint32_t b = (uint32_t)bits_of((unsigned long long)range[t] + 4);
         if (b > left) {
             ++w;
@@ -132,7 +140,8 @@ extern "C" int hj_ego_sort_device_noalloc(const void *pts, int dtype_bytes, uint
     const uint32_t W = w + 1;
     const size_t o_perm2 = align256(o_keys + (size_t)W * n * 4);
     const size_t o_hist = align256(o_perm2 + n * 4);
-    if (o_hist + hist_bytes > kScratchBytes) return HJ_ERR_INVALID_ARG;
+    if (o_hist + hist_bytes > kScratchBytes)
+        return engine_fail(HJ_ERR_INVALID_ARG, "packed keys of this input exceed the fixed 32 MiB scratch array");
     GridDev gd;
     gd.off = reinterpret_cast<long long *>(base + o_off);
     gd.bits = reinterpret_cast<uint32_t *>(base + o_bits);
@@ -176,6 +185,6 @@ extern "C" int hj_ego_sort_device_noalloc(const void *pts, int dtype_bytes, uint
             src = dst;
         }
     }
-    if (cudaGetLastError() != cudaSuccess) return HJ_ERR_CUDA;
+    if (cudaError_t e = cudaGetLastError()) return engine_fail(HJ_ERR_CUDA, cudaGetErrorString(e));
     return HJ_OK;
 }

@@ -57,6 +57,25 @@ def sharded_join_count(a, b, eps: float, form: str = "fp16", group=None,
     return _reduce_sum(part, group)
 
 
+def equal_load_cut(loads, shard: Tuple[int, int]) -> Tuple[int, int]:
+    """[a, b) of the items that shard (k, K) takes from a work list with the
+    given per-item loads: the first item whose exclusive load prefix reaches
+    floor(L k / K) up to the first that reaches floor(L (k+1) / K), L the total
+    load; the last shard runs to the end. This is the rule the device applies
+    to the Hilbert-ordered list (shard_items in csrc/hj_index.cu), stated here
+    so that orchestration can be tested without a GPU."""
+    import bisect
+    k, K = shard
+    prefix, run = [], 0
+    for w in loads:
+        prefix.append(run)
+        run += int(w)
+    lo, hi = run * k // K, run * (k + 1) // K
+    a = bisect.bisect_left(prefix, lo)
+    b = len(prefix) if k + 1 == K else bisect.bisect_left(prefix, hi)
+    return a, max(a, b)
+
+
 def row_shard(n: int, shard: Tuple[int, int]) -> Tuple[int, int]:
     """[lo, hi) of an even split of n rows into shard[1] parts (used by tests and
     by callers that shard by rows instead of by work-list load)."""

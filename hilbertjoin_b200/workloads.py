@@ -84,3 +84,37 @@ def calibrate_eps_join(a: np.ndarray, b: np.ndarray, nb_total: int, mean_neighbo
     k = max(0, min(d2.size - 1, int(np.floor(q * d2.size))))
     v = np.partition(d2, k)[k]
     return float(f"{np.sqrt(v):.7g}")
+
+
+# The benchmark configurations at their stated sizes. Every set is regenerated
+# from its seed; `eps` is either the configuration's stated value or calibrated
+# (and rounded to 7 digits) from the first points of the same set.
+CONFIGS = {
+    "cfg1_self_200k_d64": dict(kind="self", gen="uniform", dtype="f64", n=200_000, d=64, seed=1, eps=0.2),
+    "cfg2_join_200k_d20": dict(kind="join", gen="uniform", dtype="f32", n=200_000, m=200_000, d=20, seed=2,
+                               seed_b=3, eps=0.2),
+    "cfg2_join_200k_d20_nbrs20": dict(kind="join", gen="uniform", dtype="f32", n=200_000, m=200_000, d=20, seed=2,
+                                      seed_b=3, nbrs=20),
+    "cfg3_self_1M_d64_nbrs32": dict(kind="self", gen="uniform", dtype="f32", n=1_000_000, d=64, seed=22, nbrs=32),
+    "cfg4_self_4M_d28_gmm64_nbrs100": dict(kind="self", gen="gmm", dtype="f32", n=4_000_000, d=28, seed=4,
+                                           components=64, nbrs=100),
+}
+
+
+def config_sets(name: str):
+    """(A, B or None, eps) of a benchmark configuration; A and B in the
+    configuration's storage type (float32 or float64)."""
+    c = CONFIGS[name]
+    dt = np.float32 if c["dtype"] == "f32" else np.float64
+    if c["gen"] == "uniform":
+        a = uniform(c["n"], c["d"], c["seed"], dtype=dt)
+    else:
+        a = gmm(c["n"], c["d"], c["seed"], components=c["components"], dtype=dt)
+    b = uniform(c["m"], c["d"], c["seed_b"], dtype=dt) if c["kind"] == "join" else None
+    if "eps" in c:
+        eps = c["eps"]
+    elif b is None:
+        eps = calibrate_eps(a, c["n"], c["nbrs"])
+    else:
+        eps = calibrate_eps_join(a, b, c["m"], c["nbrs"])
+    return a, b, eps

@@ -170,7 +170,10 @@ HJ_API int hj_join_count_f32(const float *A, uint64_t nA, const float *B, uint64
  * (d <= 256; opts->form is ignored), so the pairs are exactly the ones the
  * count functions count. If more than `capacity` pairs qualify nothing is
  * written, *n_pairs is set to the number and HJ_ERR_CAPACITY is returned
- * (capacity 0 with pairs NULL asks for the number alone). */
+ * (capacity 0 with pairs NULL asks for the number alone). At most 2^32 - 1
+ * pairs can be listed (the device pair buffer is indexed with 32-bit
+ * offsets): a join with more returns HJ_ERR_UNSUPPORTED with *n_pairs set to
+ * the count. */
 HJ_API int hj_self_join_pairs(const double *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts,
                               uint64_t *pairs, uint64_t capacity, uint64_t *n_pairs, hj_stats *stats);
 HJ_API int hj_self_join_pairs_f32(const float *pts, uint64_t n, uint32_t d, double eps, const hj_opts *opts,
@@ -201,10 +204,13 @@ HJ_API int hj_ego_sort(const double *pts, uint64_t n, uint32_t d, double eps, co
  * are rejected with HJ_ERR_INVALID_ARG. pts: device rows [n][d], dtype_bytes 8
  * or 4; perm: device uint32 [n] output, the same stable order as hj_ego_sort.
  * The first call on a device looks up the array's address
- * (cudaGetSymbolAddress); make it before any stream capture. Calls share the
- * array and it keeps the last call's contents: calls that overlap on the GPU
- * race, calls on one stream are ordered. Returns once the work is queued on
- * `stream` (NULL = default stream), after one small read-back.
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Calls share the array and it keeps the last call's contents: calls that
+ * overlap on the GPU race, calls on one stream are ordered. Each call blocks
+ * the calling host thread until the cell-statistics kernels on `stream`
+ * (NULL = default stream) have finished -- it reads 16 d + 4 bytes back and
+ * synchronises `stream` -- then queues the key packing and the sort passes on
+ * `stream` and returns without waiting for them. Failures set hj_last_error().
  * This entry point has no counterpart in the reference. */
 HJ_API int hj_ego_sort_device_noalloc(const void *pts, int dtype_bytes, uint64_t n, uint32_t d, double eps,
                                       uint32_t *perm, void *stream);

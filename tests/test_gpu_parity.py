@@ -210,13 +210,16 @@ def test_medium_sparse_config_shape(hj):
 @pytest.mark.parametrize("form", ["plain", "tf32"])
 @pytest.mark.parametrize("K", [2, 3, 4])
 def test_shards_sum_to_full_count(hj, form, K):
-    """The device shard selection (equal-load ranges of the work list) partitions the work."""
+    """The device shard selection (equal-load ranges of the work list) partitions the
+    work: the shard counts sum to the oracle's brute-force count."""
+    import oracle
     from hilbertjoin_b200 import workloads as W
     x = W.gmm(20000, 16, 5)
     eps = 0.08
-    full = hj.self_join_count(x, eps, form=form)
+    want = oracle.self_count_brute(x, eps)
     parts = [hj.self_join_count(x, eps, form=form, shard=(k, K)) for k in range(K)]
-    assert sum(parts) == full
+    assert sum(parts) == want
+    assert sum(1 for p in parts if p > 0) >= 2  # the work really is split
     a, b = W.uniform(6000, 8, 1), W.uniform(5000, 8, 2)
-    fj = hj.join_count(a, b, 0.3, form=form)
-    assert sum(hj.join_count(a, b, 0.3, form=form, shard=(k, K)) for k in range(K)) == fj
+    want_j = oracle.join_count_brute(a, b, 0.3)
+    assert sum(hj.join_count(a, b, 0.3, form=form, shard=(k, K)) for k in range(K)) == want_j
