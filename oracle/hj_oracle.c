@@ -72,74 +72,109 @@ static void set_threads(int nthreads) {
 #endif
 }
 
-/* Brute-force self-join over all i < j. The inner loop runs over 8 partners j at
- * a time against a transposed copy, so each pair keeps the exact sequential
- * fma order while the compiler vectorises across pairs. */
-HJO_EXPORT uint64_t hjo_self_count_brute(const double *X, uint64_t n, uint32_t d, double eps, int nthreads) {
-    const double T = eps * eps;
-    set_threads(nthreads);
-    uint64_t npad = (n + 7) / 8 * 8;
-    double *XT = (double *)calloc((size_t)npad * d + 8, sizeof(double));
-    for (uint64_t i = 0; i < n; ++i)
-        for (uint32_t k = 0; k < d; ++k) XT[(size_t)k * npad + i] = X[(size_t)i * d + k];
-    uint64_t total = 0;
-#pragma omp parallel for schedule(dynamic, 16) reduction(+ : total)
-    for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
-        uint64_t i = (uint64_t)ii, cnt = 0;
-        const double *a = X + (size_t)i * d;
-        uint64_t j0 = (i + 1) / 8 * 8;
-        for (uint64_t jb = j0; jb < n; jb += 8) {
-            double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+/* Brute-force count over all pairs (i in A, j in B), restricted to j > i for a
+ * self-join (A == B). Cache-blocked so that it stays compute-bound at a
+ * million points: B is cut into chunks of kJC partners, each thread copies one
+ * chunk transposed ([d][kJC], about 0.5 MB at d = 64) and streams every A row
+ * past it, 4 rows x 8 partners at a time. Each pair keeps the exact sequential
+ * FMA order of dist2 (the vector lanes are different pairs), so the count is
+ * the pair test's, bit for bit. */
+#define kJC 1024
+#ifdef __AVX2__
+#include <immintrin.h>
+#endif
+
+static uint64_t brute_chunk(const double *A, uint64_t ilim, const double *bt, uint64_t j0, uint64_t w, uint32_t d,
+                            double T, int self) {
+    uint64_t cnt = 0;
+    for (uint64_t i = 0; i < ilim; i += 4) {
+        const uint64_t nr = ilim - i < 4 ? ilim - i : 4;
+        const double *a[4];
+        for (int r = 0; r < 4; ++r) a[r] = A + (size_t)(i + ((uint64_t)r < nr ? (uint64_t)r : 0)) * d;
+        uint64_t lstart = 0;
+        if (self && i + 1 > j0) lstart = (i + 1 - j0) / 8 * 8;
+        for (uint64_t lb = lstart; lb < w; lb += 8) {
+            double acc[4][8];
+#ifdef __AVX2__
+            __m256d c00 = _mm256_setzero_pd(), c01 = c00, c10 = c00, c11 = c00, c20 = c00, c21 = c00, c30 = c00,
+                    c31 = c00;
             for (uint32_t k = 0; k < d; ++k) {
-                const double ak = a[k];
-                const double *bt = XT + (size_t)k * npad + jb;
-                for (int l = 0; l < 8; ++l) {
-                    double df = ak - bt[l];
-                    acc[l] = fma(df, df, acc[l]);
+                const double *b = bt + (size_t)k * kJC + lb;
+                const __m256d b0 = _mm256_loadu_pd(b), b1 = _mm256_loadu_pd(b + 4);
+                __m256d x = _mm256_set1_pd(a[0][k]), d0 = _mm256_sub_pd(x, b0), d1 = _mm256_sub_pd(x, b1);
+                c00 = _mm256_fmadd_pd(d0, d0, c00);
+                c01 = _mm256_fmadd_pd(d1, d1, c01);
+                x = _mm256_set1_pd(a[1][k]), d0 = _mm256_sub_pd(x, b0), d1 = _mm256_sub_pd(x, b1);
+                c10 = _mm256_fmadd_pd(d0, d0, c10);
+                c11 = _mm256_fmadd_pd(d1, d1, c11);
+                x = _mm256_set1_pd(a[2][k]), d0 = _mm256_sub_pd(x, b0), d1 = _mm256_sub_pd(x, b1);
+                c20 = _mm256_fmadd_pd(d0, d0, c20);
+                c21 = _mm256_fmadd_pd(d1, d1, c21);
+                x = _mm256_set1_pd(a[3][k]), d0 = _mm256_sub_pd(x, b0), d1 = _mm256_sub_pd(x, b1);
+                c30 = _mm256_fmadd_pd(d0, d0, c30);
+                c31 = _mm256_fmadd_pd(d1, d1, c31);
+            }
+            _mm256_storeu_pd(acc[0], c00);
+            _mm256_storeu_pd(acc[0] + 4, c01);
+            _mm256_storeu_pd(acc[1], c10);
+            _mm256_storeu_pd(acc[1] + 4, c11);
+            _mm256_storeu_pd(acc[2], c20);
+            _mm256_storeu_pd(acc[2] + 4, c21);
+            _mm256_storeu_pd(acc[3], c30);
+            _mm256_storeu_pd(acc[3] + 4, c31);
+#else
+            for (int r = 0; r < 4; ++r)
+                for (int l = 0; l < 8; ++l) acc[r][l] = 0.0;
+            for (uint32_t k = 0; k < d; ++k) {
+                const double *b = bt + (size_t)k * kJC + lb;
+                for (int r = 0; r < 4; ++r)
+                    for (int l = 0; l < 8; ++l) {
+                        const double df = a[r][k] - b[l];
+                        acc[r][l] = fma(df, df, acc[r][l]);
+                    }
+            }
+#endif
+            for (uint64_t r = 0; r < nr; ++r)
+                for (uint64_t l = 0; l < 8; ++l) {
+                    const uint64_t j = j0 + lb + l;
+                    if (lb + l < w && (!self || j > i + r) && acc[r][l] <= T) ++cnt;
                 }
-            }
-            for (int l = 0; l < 8; ++l) {
-                uint64_t j = jb + (uint64_t)l;
-                if (j > i && j < n && acc[l] <= T) ++cnt;
-            }
         }
-        total += cnt;
     }
-    free(XT);
+    return cnt;
+}
+
+static uint64_t brute_count(const double *A, uint64_t nA, const double *B, uint64_t nB, uint32_t d, double eps,
+                            int self) {
+    const double T = eps * eps;
+    const uint64_t nch = (nB + kJC - 1) / kJC;
+    uint64_t total = 0;
+#pragma omp parallel reduction(+ : total)
+    {
+        double *bt = (double *)malloc(sizeof(double) * (size_t)kJC * d + 64);
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t c = (int64_t)nch - 1; c >= 0; --c) { /* largest self-join chunks first */
+            const uint64_t j0 = (uint64_t)c * kJC, w = nB - j0 < kJC ? nB - j0 : kJC;
+            for (uint32_t k = 0; k < d; ++k)
+                for (uint64_t l = 0; l < kJC; ++l) bt[(size_t)k * kJC + l] = l < w ? B[(size_t)(j0 + l) * d + k] : 0.0;
+            const uint64_t ilim = self ? (j0 + w < nA ? j0 + w : nA) : nA;
+            total += brute_chunk(A, ilim, bt, j0, w, d, T, self);
+        }
+        free(bt);
+    }
     return total;
+}
+
+HJO_EXPORT uint64_t hjo_self_count_brute(const double *X, uint64_t n, uint32_t d, double eps, int nthreads) {
+    set_threads(nthreads);
+    return brute_count(X, n, X, n, d, eps, 1);
 }
 
 /* Brute-force two-set join: ordered pairs (a in A, b in B). */
 HJO_EXPORT uint64_t hjo_join_count_brute(const double *A, uint64_t nA, const double *B, uint64_t nB, uint32_t d,
                                         double eps, int nthreads) {
-    const double T = eps * eps;
     set_threads(nthreads);
-    uint64_t npad = (nB + 7) / 8 * 8;
-    double *BT = (double *)calloc((size_t)npad * d + 8, sizeof(double));
-    for (uint64_t i = 0; i < nB; ++i)
-        for (uint32_t k = 0; k < d; ++k) BT[(size_t)k * npad + i] = B[(size_t)i * d + k];
-    uint64_t total = 0;
-#pragma omp parallel for schedule(dynamic, 16) reduction(+ : total)
-    for (int64_t ii = 0; ii < (int64_t)nA; ++ii) {
-        uint64_t cnt = 0;
-        const double *a = A + (size_t)ii * d;
-        for (uint64_t jb = 0; jb < nB; jb += 8) {
-            double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-            for (uint32_t k = 0; k < d; ++k) {
-                const double ak = a[k];
-                const double *bt = BT + (size_t)k * npad + jb;
-                for (int l = 0; l < 8; ++l) {
-                    double df = ak - bt[l];
-                    acc[l] = fma(df, df, acc[l]);
-                }
-            }
-            for (int l = 0; l < 8; ++l)
-                if (jb + (uint64_t)l < nB && acc[l] <= T) ++cnt;
-        }
-        total += cnt;
-    }
-    free(BT);
-    return total;
+    return brute_count(A, nA, B, nB, d, eps, 0);
 }
 
 /* Per-row neighbour counts (all partners j != i in the same set) for a list of
