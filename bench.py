@@ -61,8 +61,11 @@ def parse():
     ap.add_argument("--no-variants", action="store_true", help="skip the other tensor-core forms")
     ap.add_argument("--no-serving", action="store_true", help="skip the shortened serving stream")
     ap.add_argument("--n", type=int, default=N_POINTS, help=argparse.SUPPRESS)
-    ap.add_argument("--workload", default="selfjoin", choices=["selfjoin", "serving", "batch"],
-                    help="serving: the join-serving stream (not the headline line)")
+    ap.add_argument("--workload", default="selfjoin", choices=["selfjoin", "serving", "batch", "config"],
+                    help="serving: the join-serving stream; config: one benchmark configuration "
+                         "(--config) in every form (not the headline line)")
+    ap.add_argument("--config", default="cfg4_self_4M_d28_gmm64_nbrs100",
+                    help="configuration name for --workload config (hilbertjoin_b200.workloads.CONFIGS)")
     ap.add_argument("--requests", type=int, default=2000)
     ap.add_argument("--baseline-requests", type=int, default=200)
     return ap.parse_args()
@@ -354,6 +357,50 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def run_config(args):
+    """One benchmark configuration at its stated size, device-resident input:
+    per form (--form, else all four) the whole-join time over --steps steps and
+    the stage times, with the count checked against the oracle's fixture."""
+    import torch
+    torch.cuda.set_device(0)
+    import hilbertjoin_b200 as hj
+    from hilbertjoin_b200 import workloads as W
+    a, b, eps = W.config_sets(args.config)
+    p = os.path.join(ROOT, "tests", "golden", "config_counts.json")
+    want = None
+    if os.path.exists(p):
+        with open(p) as f:
+            fx = json.load(f)["configs"].get(args.config)
+        want = None if fx is None else int(fx["oracle_count"])
+    ad = torch.from_numpy(a).cuda()
+    bd = None if b is None else torch.from_numpy(b).cuda()
+    stream = torch.cuda.current_stream()
+    out = {}
+    forms = [args.form] if args.form not in (None, "auto") else ["plain", "fp16", "tf32", "bf16x3"]
+    for form in forms:
+        def step():
+            if bd is None:
+                return hj.self_join_count(ad, eps, form=form, return_stats=True)
+            return hj.join_count(ad, bd, eps, form=form, return_stats=True)
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = [step() for _ in range(args.steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        counts = {c for c, _ in res}
+        st = res[-1][1]
+        if want is not None and counts != {want}:
+            raise SystemExit(f"{args.config} {form}: count {counts} differs from the oracle's {want}")
+        out[form] = {"ms_per_step": e0.elapsed_time(e1) / args.steps, "count": res[-1][0],
+                     **{k: st[k] for k in ("sort_ms", "index_ms", "join_ms", "kernel_ms", "recheck_ms",
+                                           "candidate_pairs", "work_items", "fp64_items", "band_pairs",
+                                           "form_used", "kernel_launches")}}
+    print(json.dumps({"workload": args.config, "eps": eps, "oracle_count_fixture": want, "forms": out}), flush=True)
+
+
 def main():
     args = parse()
     if args.workload == "selfjoin":
@@ -365,6 +412,8 @@ def main():
         return run_serving(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "config":
+        return run_config(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch

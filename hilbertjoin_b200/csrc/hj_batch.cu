@@ -8,7 +8,7 @@
 //   * one operand matrix holding every set's rows (row blocks of 256, in the
 //     order A0, B0, A1, B1, ...; a self-join has one block), padded to the
 //     largest K of the batch with zeros, which add nothing to a dot product;
-//   * the sets' norms, with their 128/256-row maxima and 32-row minima;
+//   * the sets' norms, with their per-tile maxima and 32-row minima;
 //   * the sorted rows in input precision (for the FP64 recheck);
 //   * one work list: each job's items, tile indices rebased onto the matrix,
 //     the job index in WorkItem.pad;
@@ -216,8 +216,8 @@ static int batch_plan(const hj_batch_job *jobs, uint32_t n_jobs, int dtype_bytes
     void *hi = b->alloc(rows * kpad * esz);
     void *lo = bf ? b->alloc(rows * kpad * esz) : nullptr;
     O.norms = (float *)b->alloc(rows * 4);
-    O.tile_maxnorm_a = (float *)b->alloc((rows / 128) * 4);
-    O.tile_maxnorm_b = (float *)b->alloc((rows / 256) * 4);
+    O.tile_maxnorm_a = (float *)b->alloc((rows / kTcTileA) * 4);
+    O.tile_maxnorm_b = (float *)b->alloc((rows / kTcTileB) * 4);
     O.group_minnorm = (float *)b->alloc((rows / 32) * 4);
     char *srows = (char *)b->alloc(row_bytes);
     b->d_jobs = (TcJob *)b->alloc(n_jobs * sizeof(TcJob));

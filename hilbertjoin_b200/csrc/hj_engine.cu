@@ -248,11 +248,10 @@ static int prepare_set(Ctx *c, cudaStream_t st, const void *x, uint64_t n, int d
     uint32_t *keys_wm = (uint32_t *)slot_alloc_impl(c, st, is_b ? kSlotKeysWmB : kSlotKeysWmA,
                                                     n * (W + (norm_order ? 1 : 0)) * 4);
     uint32_t *perm = (uint32_t *)slot_alloc_impl(c, st, is_b ? kSlotPermB : kSlotPermA, n * 4);
-    uint32_t *ptmp = (uint32_t *)slot_alloc_impl(c, st, kSlotPermTmp, n * 4);
-    uint32_t *hist = (uint32_t *)slot_alloc_impl(c, st, kSlotHist, radix_hist_entries(n) * 4);
+    void *rs = slot_alloc_impl(c, st, kSlotHist, radix_scratch_bytes(n));
     s.keys = (uint32_t *)slot_alloc_impl(c, st, is_b ? kSlotKeysB : kSlotKeysA, n * W * 4);
     s.rows = slot_alloc_impl(c, st, is_b ? kSlotRowsB : kSlotRowsA, n * g.d * dtype_bytes);
-    if (!keys_wm || !perm || !ptmp || !hist || !s.keys || !s.rows) return fail(HJ_ERR_OOM, "out of device memory");
+    if (!keys_wm || !perm || !rs || !s.keys || !s.rows) return fail(HJ_ERR_OOM, "out of device memory");
     s.perm = perm;
     uint32_t flags = kGatherKeys | kGatherRows;
     if (form == HJ_FORM_PLAIN_FP64) {
@@ -289,17 +288,18 @@ static int prepare_set(Ctx *c, cudaStream_t st, const void *x, uint64_t n, int d
             return fail(HJ_ERR_OOM, "out of device memory");
         flags |= kGatherNorms;
     }
-    launch_pack_keys(x, dtype_bytes, n, g.d, g.eps, gd, W, keys_wm, st);
+    // the tensor-core forms' least significant key: the quantised norm (ties
+    // within a cell by norm), packed in the same pass
+    launch_pack_keys(x, dtype_bytes, n, g.d, g.eps, gd, W, keys_wm, st, center, norm_scale,
+                     norm_order ? keys_wm + (size_t)W * n : nullptr);
     *launches += 1;
     if (norm_order) {
-        // least significant key: the quantised norm (ties within a cell by norm)
-        launch_norm_key(x, dtype_bytes, n, g.d, center, norm_scale, keys_wm + (size_t)W * n, st);
         std::vector<std::pair<uint32_t, uint32_t>> passes = {{W, 0u}, {W, 8u}};
         passes.insert(passes.end(), g.passes.begin(), g.passes.end());
-        radix_sort_perm(keys_wm, n, passes, perm, ptmp, hist, st, launches);
+        radix_sort_perm(keys_wm, n, passes, perm, rs, st, launches);
         *launches += 1;
     } else {
-        radix_sort_perm(keys_wm, n, g.passes, perm, ptmp, hist, st, launches);
+        radix_sort_perm(keys_wm, n, g.passes, perm, rs, st, launches);
     }
     launch_gather(x, dtype_bytes, n, g.d, perm, keys_wm, W, s, flags, st, launches);
     *out = s;
@@ -723,10 +723,9 @@ static int run_pairs(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *pa
         // keys word-major: word 0 = i (most significant), word 1 = j
         uint32_t *keys = (uint32_t *)slot_alloc_impl(c, st, kSlotPairKeys, total * 8);
         uint32_t *perm = (uint32_t *)slot_alloc_impl(c, st, kSlotPairPerm, total * 4);
-        uint32_t *ptmp = (uint32_t *)slot_alloc_impl(c, st, kSlotPairTmp, total * 4);
-        uint32_t *hist = (uint32_t *)slot_alloc_impl(c, st, kSlotPairHist, radix_hist_entries(total) * 4);
+        void *rs = slot_alloc_impl(c, st, kSlotPairHist, radix_scratch_bytes(total));
         unsigned long long *out = (unsigned long long *)slot_alloc_impl(c, st, kSlotPairOut, total * 16);
-        if (!keys || !perm || !ptmp || !hist || !out) return fail(HJ_ERR_OOM, "out of device memory (pairs)");
+        if (!keys || !perm || !rs || !out) return fail(HJ_ERR_OOM, "out of device memory (pairs)");
         launch_pairs_fp64(A, B, in.self, P.na_eff, P.nb_eff, T, idx, item_cnt, keys, keys + total, d_err,
                           c->num_sms, st);
         ++launches;
@@ -734,7 +733,7 @@ static int run_pairs(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *pa
         const int bj = bitwidth(in.nb ? in.nb - 1 : 0), bi = bitwidth(in.na ? in.na - 1 : 0);
         for (int b = 0; b < bj; b += 8) passes.push_back({1u, (uint32_t)b});
         for (int b = 0; b < bi; b += 8) passes.push_back({0u, (uint32_t)b});
-        radix_sort_perm(keys, total, passes, perm, ptmp, hist, st, &launches);
+        radix_sort_perm(keys, total, passes, perm, rs, st, &launches);
         k_pairs_gather<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(keys, keys + total, perm, total, out);
         ++launches;
         cudaEventRecord(c->ev[4], st);
@@ -882,10 +881,9 @@ static int ego_sort_host(const double *pts, uint64_t n, uint32_t d, double eps, 
     gd.shift = (uint32_t *)slot_alloc_impl(c, st, kSlotGridShift, d * 4);
     uint32_t *keys_wm = (uint32_t *)slot_alloc_impl(c, st, kSlotKeysWmA, n * g.W * 4);
     uint32_t *dperm = (uint32_t *)slot_alloc_impl(c, st, kSlotPermA, n * 4);
-    uint32_t *ptmp = (uint32_t *)slot_alloc_impl(c, st, kSlotPermTmp, n * 4);
-    uint32_t *hist = (uint32_t *)slot_alloc_impl(c, st, kSlotHist, radix_hist_entries(n) * 4);
+    void *rs = slot_alloc_impl(c, st, kSlotHist, radix_scratch_bytes(n));
     void *rows = sorted ? slot_alloc_impl(c, st, kSlotRowsA, n * d * 8) : nullptr;
-    if (!gd.off || !gd.bits || !gd.word || !gd.shift || !keys_wm || !dperm || !ptmp || !hist || (sorted && !rows))
+    if (!gd.off || !gd.bits || !gd.word || !gd.shift || !keys_wm || !dperm || !rs || (sorted && !rows))
         return fail(HJ_ERR_OOM, "out of device memory");
     cudaMemcpyAsync(gd.off, g.off.data(), d * 8, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(gd.bits, g.bits.data(), d * 4, cudaMemcpyHostToDevice, st);
@@ -893,7 +891,7 @@ static int ego_sort_host(const double *pts, uint64_t n, uint32_t d, double eps, 
     cudaMemcpyAsync(gd.shift, g.shift.data(), d * 4, cudaMemcpyHostToDevice, st);
     int launches = 0;
     launch_pack_keys(dx, 8, n, d, eps, gd, g.W, keys_wm, st);
-    radix_sort_perm(keys_wm, n, g.passes, dperm, ptmp, hist, st, &launches);
+    radix_sort_perm(keys_wm, n, g.passes, dperm, rs, st, &launches);
     if (sorted) {
         SortedSet s;
         s.rows = rows;
@@ -945,6 +943,57 @@ static int dim_order_host(const double *pts, uint64_t n, uint32_t d, double eps,
 int engine_fail(int code, const std::string &msg) { return fail(code, msg); }
 
 void engine_clear_error() { tl_error.clear(); }
+
+uint64_t engine_ctx_bytes(int device) {
+    auto it = tl_ctx.find(device);
+    if (it == tl_ctx.end()) return 0;
+    uint64_t b = 0;
+    for (const auto &s : it->second->slots) b += s.second;
+    return b;
+}
+
+void engine_ctx_trim(int device, cudaStream_t st) {
+    auto it = tl_ctx.find(device);
+    if (it == tl_ctx.end()) return;
+    Ctx *c = it->second;
+    cudaSetDevice(device);
+    if (st) cudaStreamSynchronize(st);
+    cudaStreamSynchronize(c->stream);
+    for (auto &s : c->slots) {
+        if (s.first) cudaFree(s.first);
+        s = {nullptr, 0};
+    }
+    cudaGetLastError();
+}
+
+// Device memory one join takes in the calling thread's context, from the
+// buffers prepare_set, the index and run_join allocate, with the key width
+// bounded by 6 bits per dim (cell ranges up to 60 cells per dim; wider key
+// words are rare and are measured after the join) and the band queue at its
+// first size (a larger band regrows it; the server measures that too).
+uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dtype_bytes, int form, bool self) {
+    const uint64_t W = (6ull * d + 31) / 32 + 1;
+    const bool tc = form_is_tc(form) || form == HJ_FORM_AUTO;
+    auto per_set = [&](uint64_t n) -> uint64_t {
+        const uint64_t npad = hj_ceil_div(std::max<uint64_t>(n, 1), kTcTileB) * kTcTileB;
+        uint64_t b = n * d * (uint64_t)dtype_bytes;          // sorted rows
+        b += n * (2 * W + 1) * 4 + n * 8;                     // packed keys (both layouts), permutation
+        b += npad * d * 8;                                    // plain FP64 tiles (plain form or routed items)
+        if (tc) b += npad * (hj_ceil_div(d, 64) * 64) * 4 + npad * 8;  // operands (widest form), norms
+        return b;
+    };
+    uint64_t b = per_set(na) + (self ? 0 : per_set(nb));
+    const uint64_t nmax = std::max(na, nb);
+    b += radix_scratch_bytes(nmax) + 2 * radix_scratch_bytes(1);
+    // work list: per A tile up to kMaxCombos runs, items of a few B tiles
+    const uint64_t tiles = hj_ceil_div(std::max<uint64_t>(na, 1), kPlainTile);
+    b += tiles * (uint64_t)kMaxCombos * 8 + tiles * 64 * 16;
+    if (tc) {
+        const double cand = (double)na * (double)nb;
+        b += (uint64_t)std::max(1048576.0, cand / 4096.0) * kBandEntryBytes;
+    }
+    return b + (16ull << 20);
+}
 
 int engine_prepare_job(cudaStream_t st_in, const void *a, const void *b, uint64_t na, uint64_t nb, int dtype_bytes,
                        uint32_t d, double eps, bool self, const hj_opts *opts, int form, PreparedJob *out) {
@@ -1122,6 +1171,13 @@ int hj_debug_tc_estimates(const float *A, uint64_t nA, const float *B, uint64_t 
         r = check_cuda("debug copy");
     cudaFree(dbg);
     return r;
+}
+
+int hj_debug_set_wait_gate(uint64_t gate_ns) {
+    tl_error.clear();
+    if (gate_ns > kWaitLimitNs) return fail(HJ_ERR_INVALID_ARG, "gate longer than the wait limit");
+    set_tc_wait_gate(gate_ns);
+    return HJ_OK;
 }
 
 int hj_self_join_count_device(const void *pts, int dtype_bytes, uint64_t n, uint32_t d, double eps,

@@ -377,11 +377,11 @@ __global__ void k_item_split(const WorkItem *__restrict__ items, uint64_t n, con
     const uint32_t before = flags_scan[i];
     const uint32_t next = i + 1 < n ? flags_scan[i + 1] : (uint32_t)n_tc;
     const WorkItem w = items[i];
+    constexpr uint32_t r = kTcTileA / kPlainTile, c = kTcTileB / kPlainTile;
     if (next != before) {
         tc_out[before] = w;
     } else {
-        const uint64_t k = 2 * (i - before);
-        const uint32_t r = kTcTileA / kPlainTile, c = kTcTileB / kPlainTile;
+        const uint64_t k = (uint64_t)r * (i - before);
         for (uint32_t h = 0; h < r; ++h) {
             WorkItem p;
             p.a = w.a * r + h;
@@ -414,14 +414,15 @@ int split_items_by_precision(const IndexResult &in, const SortedSet &A, const So
     const uint64_t n_tc = h[0], n_fp = n - n_tc;
     if (n_fp == 0) return 0;
     WorkItem *tc = (WorkItem *)alloc(actx, kSlotSplitTc, (n_tc + 1) * sizeof(WorkItem));
-    WorkItem *fp = (WorkItem *)alloc(actx, kSlotSplitFp, 2 * n_fp * sizeof(WorkItem));
+    constexpr uint32_t rows_per_tc = kTcTileA / kPlainTile;  // FP64 items per routed tensor-core item
+    WorkItem *fp = (WorkItem *)alloc(actx, kSlotSplitFp, rows_per_tc * n_fp * sizeof(WorkItem));
     if (!tc || !fp) return 2;
     k_item_split<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(in.items, n, flags, n_tc, tc, fp);
     tc_out->items = tc;
     tc_out->n_items = n_tc;
     tc_out->tile_pairs = in.tile_pairs - h[1];
     fp_out->items = fp;
-    fp_out->n_items = 2 * n_fp;
+    fp_out->n_items = rows_per_tc * n_fp;
     fp_out->tile_pairs = h[1] * (kTcTileA / kPlainTile) * (kTcTileB / kPlainTile);
     return 0;
 }
@@ -495,9 +496,8 @@ int build_index(const SortedSet &A, const SortedSet &B, const Grid &grid, const 
     WorkItem *items = (WorkItem *)alloc(actx, kSlotItems, n_items * sizeof(WorkItem));
     uint32_t *keys = (uint32_t *)alloc(actx, kSlotItemKeys, n_items * key_words * sizeof(uint32_t));
     uint32_t *perm = (uint32_t *)alloc(actx, kSlotItemPerm, n_items * sizeof(uint32_t));
-    uint32_t *ptmp = (uint32_t *)alloc(actx, kSlotItemPermTmp, n_items * sizeof(uint32_t));
-    uint32_t *hist = (uint32_t *)alloc(actx, kSlotItemHist, radix_hist_entries(n_items) * sizeof(uint32_t));
-    if (!tmp || !items || !keys || !perm || !ptmp || !hist) {
+    void *rs = alloc(actx, kSlotItemHist, radix_scratch_bytes(n_items));
+    if (!tmp || !items || !keys || !perm || !rs) {
         *err = "out of device memory (work list)";
         return 2;
     }
@@ -510,7 +510,7 @@ int build_index(const SortedSet &A, const SortedSet &B, const Grid &grid, const 
         for (int b = 0; b < 32; b += 8) passes.push_back({1u, (uint32_t)b});
         for (int b = 0; b < hbits - 32; b += 8) passes.push_back({0u, (uint32_t)b});
     }
-    radix_sort_perm(keys, n_items, passes, perm, ptmp, hist, st, launches);
+    radix_sort_perm(keys, n_items, passes, perm, rs, st, launches);
     k_permute_items<<<(unsigned)hj_ceil_div(n_items, 256), 256, 0, st>>>(tmp, perm, n_items, items);
     if (launches) *launches += 2;
     out->items = items;

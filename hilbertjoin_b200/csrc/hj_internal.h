@@ -16,7 +16,7 @@ namespace hj {
 
 // Point-tile sizes of the two distance kernels.
 constexpr int kPlainTile = 64;   // plain FP64 kernel: 64 x 64 point tiles
-constexpr int kTcTileA = 128;    // tensor-core kernel: 128 A rows (UMMA M) ...
+constexpr int kTcTileA = 256;    // tensor-core kernel: 256 A rows (UMMA M of a CTA pair) ...
 constexpr int kTcTileB = 256;    // ... against 256 B rows (UMMA N)
 constexpr int kMaxActiveDims = 5;
 constexpr int kMaxCombos = 243;  // 3^kMaxActiveDims
@@ -100,7 +100,7 @@ struct SortedSet {
     const double *center = nullptr;  // per-dim shift of the tensor-core operands (shared by A and B)
     double op_scale = 1.0;       // FP16 form: power of two applied to operands (norms: its square)
     float *norms = nullptr;      // FP32(|x - center|^2 in FP64); padding rows hold kPadNorm
-    float *tile_maxnorm_a = nullptr;  // per 128-row tile
+    float *tile_maxnorm_a = nullptr;  // per kTcTileA-row tile
     float *tile_maxnorm_b = nullptr;  // per 256-row tile
     float *group_minnorm = nullptr;   // per 32-row group: min |x - center|^2
     uint64_t npad_tc = 0;
@@ -157,8 +157,11 @@ void launch_dim_stats_init(DimStats *dstats, uint32_t d, unsigned long long *d_m
                            cudaStream_t st);
 
 // Packed keys, word-major [W][n].
+// With norm_key non-null, the quantised norm key (launch_norm_key) of every
+// point is written in the same pass.
 void launch_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, const GridDev &g,
-                      uint32_t W, uint32_t *keys_wm, cudaStream_t st);
+                      uint32_t W, uint32_t *keys_wm, cudaStream_t st, const double *center = nullptr,
+                      double norm_scale = 0.0, uint32_t *norm_key = nullptr);
 
 // Quantised |x - center|^2 (16 bits, key = min(65535, floor(norm * scale))),
 // the least significant sort key of the tensor-core forms: points of one cell
@@ -166,15 +169,15 @@ void launch_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t d, do
 void launch_norm_key(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const double *center, double scale,
                      uint32_t *key_out, cudaStream_t st);
 
-// Stable LSD radix sort of a permutation by 8-bit windows of word-major keys.
-// `passes` in order (least significant first). Needs scratch: perm_tmp[n],
-// hist[256 * ceil(n/4096)]. Result in perm_out.
+// Stable LSD radix sort of a permutation by 8-bit windows of word-major keys
+// ([word][n]); `passes` = (word, shift) in order, least significant first.
+// Needs radix_scratch_bytes(n) of 16-byte aligned device scratch. Result:
+// perm_out[r] = input index of rank r (identity when there is no pass).
+size_t radix_scratch_bytes(uint64_t n);
+void radix_sort_perm(const uint32_t *keys_wm, uint64_t n, const std::pair<uint32_t, uint32_t> *passes, size_t np,
+                     uint32_t *perm_out, void *scratch, cudaStream_t st, int *launches);
 void radix_sort_perm(const uint32_t *keys_wm, uint64_t n, const std::vector<std::pair<uint32_t, uint32_t>> &passes,
-                     uint32_t *perm_out, uint32_t *perm_tmp, uint32_t *hist, cudaStream_t st, int *launches);
-size_t radix_hist_entries(uint64_t n);
-// One stable pass of the above (perm_in null = identity), and an iota.
-void radix_sort_pass(const uint32_t *keyw, uint64_t n, uint32_t shift, const uint32_t *perm_in,
-                     uint32_t *perm_out, uint32_t *hist, cudaStream_t st);
+                     uint32_t *perm_out, void *scratch, cudaStream_t st, int *launches);
 void launch_iota(uint32_t *p, uint64_t n, cudaStream_t st);
 // Exclusive scan of u32 entries in place (one block); total into *total if non-null.
 void launch_scan_u32(uint32_t *a, uint64_t count, unsigned long long *total, cudaStream_t st);
@@ -249,6 +252,9 @@ void launch_recheck(const TcJob *d_jobs, int dtype_bytes, const uint2 *band, con
 // Test hook: when non-null, the tensor-core kernel writes its dist^2 estimate
 // of every pair to dbg[ia * nb + jb] (EGO ranks). Not thread-safe.
 void set_tc_debug_output(float *dbg);
+// Test hook: with ns > 0 the tensor-core kernel's epilogue first waits ns on a
+// barrier that nothing arrives on, then raises kErrTimeout (0 = off).
+void set_tc_wait_gate(uint64_t ns);
 // Error-bound constant of a tensor-core form for dimension d.
 void tc_band_constants(int form, uint32_t d, double maxabs, double *c_rel, double *c_abs);
 
@@ -278,9 +284,16 @@ int batch_job_candidates(const hj_batch *b, uint64_t *out);
 int engine_fail(int code, const std::string &msg);
 // Clears this host thread's error text (hj_last_error) at the start of a call.
 void engine_clear_error();
+// Device memory held by the calling thread's engine context on `device`
+// (its reusable buffers), and their release once `st` and the context's own
+// stream have drained.
+uint64_t engine_ctx_bytes(int device);
+void engine_ctx_trim(int device, cudaStream_t st);
+// Upper estimate of the device memory one join takes in a context.
+uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dtype_bytes, int form, bool self);
 // Norm summaries over a row-major norm array of npad rows (padding rows hold
-// kPadNorm): per 128-row and per 256-row tile maxima, per 32-row minima.
-void launch_norm_summaries(const float *norms, uint64_t npad, float *tmax128, float *tmax256, float *gmin32,
+// kPadNorm): per A-tile and per B-tile maxima, per 32-row minima.
+void launch_norm_summaries(const float *norms, uint64_t npad, float *tmax_a, float *tmax_b, float *gmin32,
                            cudaStream_t st);
 
 }  // namespace hj

@@ -78,7 +78,7 @@ extern "C" int hj_ego_sort_device_noalloc(const void *pts, int dtype_bytes, uint
     if (!(eps > 0.0) || !std::isfinite(eps)) return engine_fail(HJ_ERR_INVALID_ARG, "eps must be finite and > 0");
     if (n == 0) return HJ_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    // scratch layout: stats | maxabs, bad | off | bits | word | shift | keys [W][n] | perm2 [n] | hist
+    // scratch layout: stats | maxabs, bad | off | bits | word | shift | keys [W][n] | radix sort scratch
     const size_t o_stats = 0;
     const size_t o_small = align256(o_stats + (size_t)d * sizeof(DimStats));
     const size_t o_off = align256(o_small + 16);
@@ -86,9 +86,9 @@ extern "C" int hj_ego_sort_device_noalloc(const void *pts, int dtype_bytes, uint
     const size_t o_word = align256(o_bits + (size_t)d * 4);
     const size_t o_shift = align256(o_word + (size_t)d * 4);
     const size_t o_keys = align256(o_shift + (size_t)d * 4);
-    const size_t hist_bytes = radix_hist_entries(n) * 4;
+    const size_t rs_bytes = radix_scratch_bytes(n);
     // at least one key word: reject before touching the device when even that does not fit
-    if (o_keys + align256(n * 4) + align256(n * 4) + hist_bytes > kScratchBytes)
+    if (o_keys + align256(n * 4) + rs_bytes > kScratchBytes)
         return engine_fail(HJ_ERR_INVALID_ARG, "n too large for the fixed 32 MiB scratch array");
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
@@ -138,9 +138,8 @@ extern "C" int hj_ego_sort_device_noalloc(const void *pts, int dtype_bytes, uint
         left -= b;
     }
     const uint32_t W = w + 1;
-    const size_t o_perm2 = align256(o_keys + (size_t)W * n * 4);
-    const size_t o_hist = align256(o_perm2 + n * 4);
-    if (o_hist + hist_bytes > kScratchBytes)
+    const size_t o_rs = align256(o_keys + (size_t)W * n * 4);
+    if (o_rs + rs_bytes > kScratchBytes)
         return engine_fail(HJ_ERR_INVALID_ARG, "packed keys of this input exceed the fixed 32 MiB scratch array");
     GridDev gd;
     gd.off = reinterpret_cast<long long *>(base + o_off);
@@ -152,13 +151,12 @@ extern "C" int hj_ego_sort_device_noalloc(const void *pts, int dtype_bytes, uint
     cudaMemcpyAsync(gd.word, word, d * 4, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(gd.shift, shift, d * 4, cudaMemcpyHostToDevice, st);
     uint32_t *keys = reinterpret_cast<uint32_t *>(base + o_keys);
-    uint32_t *perm2 = reinterpret_cast<uint32_t *>(base + o_perm2);
-    uint32_t *hist = reinterpret_cast<uint32_t *>(base + o_hist);
+    void *rs = base + o_rs;
     launch_pack_keys(pts, dtype_bytes, n, d, eps, gd, W, keys, st);
 
-    // 3. stable LSD passes over the digit windows that can vary; the last pass
-    //    writes the caller's buffer
-    uint32_t pw[4 * kMaxDim], ps[4 * kMaxDim];
+    // 3. stable LSD passes over the digit windows that can vary (the same
+    //    rule as the allocating path), into the caller's buffer
+    static thread_local std::pair<uint32_t, uint32_t> passes[4 * kMaxDim];
     uint32_t np = 0;
     for (int ww = (int)W - 1; ww >= 0; --ww)
         for (uint32_t lowbit = 0; lowbit < 32; lowbit += 8) {
@@ -169,22 +167,9 @@ extern "C" int hj_ego_sort_device_noalloc(const void *pts, int dtype_bytes, uint
                 const uint32_t f0 = shift[t], f1 = shift[t] + (vb < bits[t] ? vb : bits[t]);
                 if (f0 < lowbit + 8 && f1 > lowbit) active = true;
             }
-            if (active) {
-                pw[np] = (uint32_t)ww;
-                ps[np] = lowbit;
-                ++np;
-            }
+            if (active) passes[np++] = {(uint32_t)ww, lowbit};
         }
-    if (np == 0) {
-        launch_iota(perm, n, st);
-    } else {
-        const uint32_t *src = nullptr;
-        for (uint32_t k = 0; k < np; ++k) {
-            uint32_t *dst = ((np - 1 - k) & 1u) ? perm2 : perm;
-            radix_sort_pass(keys + (size_t)pw[k] * n, n, ps[k], src, dst, hist, st);
-            src = dst;
-        }
-    }
+    radix_sort_perm(keys, n, passes, np, perm, rs, st, nullptr);
     if (cudaError_t e = cudaGetLastError()) return engine_fail(HJ_ERR_CUDA, cudaGetErrorString(e));
     return HJ_OK;
 }

@@ -14,6 +14,7 @@
 
 #include <map>
 #include <mutex>
+#include <type_traits>
 
 #include "hj_common.cuh"
 #include "hj_internal.h"
@@ -44,65 +45,67 @@ __global__ void k_dim_stats_init(DimStats *s, uint32_t d, unsigned long long *ma
     }
 }
 
-// Cells beyond +-2^62 cannot be represented; such inputs are rejected.
-constexpr double kCellLimit = 4.611686018427388e18;
 
-// Thread k handles dim t = k % d of rows k / d, k / d + R, ... (R = threads /
-// d): consecutive threads read consecutive coordinates of a row (coalesced),
-// and every thread keeps its dim's minima and maxima in registers; one
-// shared-memory atomic per thread and statistic at the end.
-__global__ void k_dim_stats(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, DimStats *s,
-                            unsigned long long *maxabs_bits, uint32_t *bad) {
-    extern __shared__ long long sh[];  // [4][d]
-    long long *smin = sh, *smax = sh + d;
-    unsigned long long *sxmin = reinterpret_cast<unsigned long long *>(sh + 2 * d), *sxmax = sxmin + d;
+// Per-dim coordinate range, maximum |x| and the non-finite check, reading the
+// rows as one flat array of n*d coordinates with 128-bit loads (V = 4 FP32 or
+// 2 FP64 coordinates per load; V = 1 when the array is not 16-byte aligned).
+// The grid is sized so that threads * V is a multiple of d: thread k then sees
+// the same V dims (k*V + j) % d at every step and keeps their minima and
+// maxima in registers. The cells need no division per coordinate: floor(x/eps)
+// is monotone in x (IEEE division by a positive eps rounds monotonically), so
+// a dim's smallest and largest cells are those of its smallest and largest
+// coordinate; k_dim_stats_cells computes them once per dim.
+template <typename T, int V>
+__global__ void __launch_bounds__(256) k_dim_stats(const T *__restrict__ x, uint64_t total, uint32_t d,
+                                                   DimStats *s, unsigned long long *maxabs_bits, uint32_t *bad) {
+    extern __shared__ unsigned long long shx[];  // [2][d]
+    unsigned long long *sxmin = shx, *sxmax = shx + d;
     for (uint32_t t = threadIdx.x; t < d; t += blockDim.x) {
-        smin[t] = LLONG_MAX;
-        smax[t] = LLONG_MIN;
         sxmin[t] = ~0ull;
         sxmax[t] = 0ull;
     }
     __syncthreads();
     const uint64_t threads = (uint64_t)gridDim.x * blockDim.x;
     const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t rows_per_step = threads / d;  // >= 1 (the launch ensures threads >= d)
-    const uint32_t t = (uint32_t)(k % d);
-    long long cmin = LLONG_MAX, cmax = LLONG_MIN;
-    unsigned long long xmin = ~0ull, xmax = 0ull;
+    unsigned long long xmin[V], xmax[V];
+#pragma unroll
+    for (int j = 0; j < V; ++j) xmin[j] = ~0ull, xmax[j] = 0ull;
     double amax = 0.0;
     uint32_t lbad = 0;
-    if (k < rows_per_step * d) {
-        for (uint64_t r = k / d; r < n; r += rows_per_step) {
-            const double v = coord(x, dtype_bytes, r * d + t);
-            if (!isfinite(v)) {
+    using Vec = typename std::conditional<V == 4, float4, typename std::conditional<V == 2, double2, T>::type>::type;
+    for (uint64_t e = k * V; e < total; e += threads * V) {
+        T v[V];
+        if (e + V <= total) {
+            const Vec q = __ldg(reinterpret_cast<const Vec *>(x + e));
+            memcpy(v, &q, sizeof(v));
+        } else {
+#pragma unroll
+            for (int j = 0; j < V; ++j) v[j] = e + j < total ? x[e + j] : T(0);
+        }
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+            if (e + j >= total) continue;
+            const double w = (double)v[j];
+            if (!isfinite(w)) {
                 lbad |= 1u;
                 continue;
             }
-            const double c = floor(v / eps);
-            if (!(fabs(c) < kCellLimit)) {
-                lbad |= 2u;
-                continue;
-            }
-            amax = fmax(amax, fabs(v));
-            const long long ci = (long long)c;
-            cmin = min(cmin, ci);
-            cmax = max(cmax, ci);
-            const unsigned long long ov = ordered_from_double(v);
-            xmin = min(xmin, ov);
-            xmax = max(xmax, ov);
+            amax = fmax(amax, fabs(w));
+            const unsigned long long o = ordered_from_double(w);
+            xmin[j] = min(xmin[j], o);
+            xmax[j] = max(xmax[j], o);
         }
     }
-    if (cmin != LLONG_MAX) {
-        atomicMin(&smin[t], cmin);
-        atomicMax(&smax[t], cmax);
-        atomicMin(&sxmin[t], xmin);
-        atomicMax(&sxmax[t], xmax);
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+        if (xmin[j] == ~0ull) continue;
+        const uint32_t t = (uint32_t)((k * V + j) % d);
+        atomicMin(&sxmin[t], xmin[j]);
+        atomicMax(&sxmax[t], xmax[j]);
     }
     __syncthreads();
     for (uint32_t u = threadIdx.x; u < d; u += blockDim.x) {
-        if (smin[u] != LLONG_MAX) {
-            atomicMin(&s[u].cmin, smin[u]);
-            atomicMax(&s[u].cmax, smax[u]);
+        if (sxmin[u] != ~0ull) {
             atomicMin(&s[u].xmin, sxmin[u]);
             atomicMax(&s[u].xmax, sxmax[u]);
         }
@@ -112,19 +115,67 @@ __global__ void k_dim_stats(const void *x, int dtype_bytes, uint64_t n, uint32_t
     if (lbad) atomicOr(bad, lbad);
 }
 
+// Cells beyond +-2^62 cannot be represented; such inputs are rejected.
+constexpr double kCellLimit = 4.611686018427388e18;
+
+// Per dim: the cells of its smallest and largest coordinate.
+__global__ void k_dim_stats_cells(DimStats *s, uint32_t d, double eps, uint32_t *bad) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d || s[t].xmin == ~0ull) return;
+    const double lo = floor(double_from_ordered(s[t].xmin) / eps), hi = floor(double_from_ordered(s[t].xmax) / eps);
+    if (!(fabs(lo) < kCellLimit) || !(fabs(hi) < kCellLimit)) {
+        atomicOr(bad, 2u);
+        return;
+    }
+    s[t].cmin = (long long)lo;
+    s[t].cmax = (long long)hi;
+}
+
 void launch_dim_stats_init(DimStats *dstats, uint32_t d, unsigned long long *d_maxabs_bits, uint32_t *d_bad,
                            cudaStream_t st) {
     k_dim_stats_init<<<(d + 255) / 256, 256, 0, st>>>(dstats, d, d_maxabs_bits, d_bad);
 }
 
+static uint64_t gcd_u64(uint64_t a, uint64_t b) {
+    while (b) {
+        const uint64_t r = a % b;
+        a = b;
+        b = r;
+    }
+    return a;
+}
+
+template <typename T, int V>
+static void dim_stats_launch(const T *x, uint64_t n, uint32_t d, DimStats *dstats, unsigned long long *maxabs,
+                             uint32_t *bad, cudaStream_t st) {
+    const uint64_t total = n * d;
+    // threads * V must be a multiple of d: blocks a multiple of L
+    const uint64_t dv = d / gcd_u64(d, V);
+    const uint64_t L = dv / gcd_u64(dv, 256);
+    uint64_t want = std::min<uint64_t>(hj_ceil_div(total, 256 * V * 8), 148 * 8);
+    if (want < 1) want = 1;
+    const uint64_t blocks = hj_ceil_div(want, L) * L;
+    k_dim_stats<T, V><<<(unsigned)blocks, 256, 2 * d * sizeof(unsigned long long), st>>>(x, total, d, dstats, maxabs,
+                                                                                         bad);
+}
+
 void launch_dim_stats(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, DimStats *dstats,
                       unsigned long long *d_maxabs_bits, uint32_t *d_bad, cudaStream_t st) {
-    uint64_t total = n * d;
-    int blocks = (int)std::min<uint64_t>(hj_ceil_div(total, 256 * 8), 148 * 8);
-    if (blocks < 1) blocks = 1;
-    if ((uint64_t)blocks * 256 < d) blocks = (int)hj_ceil_div(d, 256);  // every dim gets a thread
-    k_dim_stats<<<blocks, 256, 4 * d * sizeof(long long), st>>>(x, dtype_bytes, n, d, eps, dstats, d_maxabs_bits,
-                                                                 d_bad);
+    const bool vec = ((uintptr_t)x & 15u) == 0;
+    if (n) {
+        if (dtype_bytes == 8) {
+            if (vec)
+                dim_stats_launch<double, 2>(static_cast<const double *>(x), n, d, dstats, d_maxabs_bits, d_bad, st);
+            else
+                dim_stats_launch<double, 1>(static_cast<const double *>(x), n, d, dstats, d_maxabs_bits, d_bad, st);
+        } else {
+            if (vec)
+                dim_stats_launch<float, 4>(static_cast<const float *>(x), n, d, dstats, d_maxabs_bits, d_bad, st);
+            else
+                dim_stats_launch<float, 1>(static_cast<const float *>(x), n, d, dstats, d_maxabs_bits, d_bad, st);
+        }
+    }
+    k_dim_stats_cells<<<(d + 255) / 256, 256, 0, st>>>(dstats, d, eps, d_bad);
 }
 
 // ------------------------------------------------------------ key packing
@@ -245,41 +296,106 @@ void launch_dim_cost(const void *x, int dtype_bytes, uint64_t n, uint32_t d, dou
     k_dim_cost<<<d, 1024, 0, st>>>(x, dtype_bytes, n, d, eps, ds, cost);
 }
 
-void launch_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, const GridDev &g,
-                      uint32_t W, uint32_t *keys_wm, cudaStream_t st) {
-    if (n == 0) return;
-    k_pack_keys<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(x, dtype_bytes, n, d, eps, g, W, keys_wm);
-}
+// Packing with the rows staged in shared memory: a block of kPkRows threads
+// packs kPkRows consecutive points, whose rows form one contiguous range of
+// kPkRows * d coordinates. The block loads it with 128-bit loads (coalesced)
+// into a [d][kPkRows] layout, so that thread t then reads its own row with
+// consecutive threads on consecutive banks. The quantised norm key of the
+// tensor-core forms comes out of the same pass (norm_key != null): the rows
+// are read from memory once for both. Rows of up to 512 bytes (d <= 128 FP32,
+// d <= 64 FP64) take this path.
+constexpr int kPkRows = 128;
+constexpr uint32_t kPkMaxRowBytes = 512;
 
-// ------------------------------------------------------------ radix sort
-//
-// Stable LSD radix sort of a permutation. Each pass orders by one 8-bit window
-// of one key word, read through the current permutation. Three kernels per
-// pass: per-tile digit histograms, one exclusive scan over (digit, tile), and a
-// stable scatter that ranks equal digits in index order (warp match + per-warp
-// prefix), so ties keep their previous order and the sort is stable overall.
-
-constexpr int kRsThreads = 256;
-constexpr int kRsTile = 4096;  // items per block
-constexpr int kRsWarps = kRsThreads / 32;
-
-size_t radix_hist_entries(uint64_t n) { return 256 * (size_t)hj_ceil_div(n, kRsTile); }
-
-__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const uint32_t *__restrict__ keyw,
-                                                       const uint32_t *__restrict__ perm_in, uint64_t n,
-                                                       uint32_t shift, uint32_t *__restrict__ hist,
-                                                       uint32_t nblocks) {
-    __shared__ uint32_t h[256];
-    h[threadIdx.x] = 0;
-    __syncthreads();
-    uint64_t base = (uint64_t)blockIdx.x * kRsTile;
-    uint64_t end = base + kRsTile < n ? base + kRsTile : n;
-    for (uint64_t i = base + threadIdx.x; i < end; i += kRsThreads) {
-        uint32_t src = perm_in ? perm_in[i] : (uint32_t)i;
-        atomicAdd(&h[(keyw[src] >> shift) & 255u], 1u);
+template <typename T>
+__global__ void __launch_bounds__(kPkRows) k_pack_keys_staged(const T *__restrict__ x, uint64_t n, uint32_t d,
+                                                              double eps, GridDev g, uint32_t W,
+                                                              uint32_t *__restrict__ keys_wm,
+                                                              const double *__restrict__ center, double nscale,
+                                                              uint32_t *__restrict__ norm_key, bool vec) {
+    extern __shared__ __align__(16) unsigned char pk_smem[];
+    T *cols = reinterpret_cast<T *>(pk_smem);  // [d][kPkRows]
+    const uint64_t r0 = (uint64_t)blockIdx.x * kPkRows;
+    const uint32_t m = (uint32_t)(n - r0 < (uint64_t)kPkRows ? n - r0 : kPkRows);
+    const uint32_t ne = m * d;
+    const T *src = x + r0 * d;
+    const float inv_d = 1.0f / (float)d;
+    // element e of the block's range -> (row e / d, col e % d); e < 2^17, so
+    // the FP32 quotient is off by at most one and one correction step fixes it
+    auto put = [&](uint32_t e, T v) {
+        uint32_t r = (uint32_t)((float)e * inv_d);
+        int c = (int)e - (int)(r * d);
+        if (c < 0) c += (int)d, --r;
+        if (c >= (int)d) c -= (int)d, ++r;
+        cols[(uint32_t)c * kPkRows + r] = v;
+    };
+    constexpr uint32_t V = 16 / sizeof(T);
+    if (vec) {
+        const uint32_t nv = ne / V;
+        const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
+        for (uint32_t u = threadIdx.x; u < nv; u += kPkRows) {
+            const uint4 q = __ldg(s4 + u);
+            T v[V];
+            memcpy(v, &q, 16);
+#pragma unroll
+            for (uint32_t j = 0; j < V; ++j) put(u * V + j, v[j]);
+        }
+        for (uint32_t e = nv * V + threadIdx.x; e < ne; e += kPkRows) put(e, __ldg(src + e));
+    } else {
+        for (uint32_t e = threadIdx.x; e < ne; e += kPkRows) put(e, __ldg(src + e));
     }
     __syncthreads();
-    hist[(size_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+    const uint32_t t = threadIdx.x;
+    if (t >= m) return;
+    const uint64_t i = r0 + t;
+    uint32_t cur_word = 0, acc = 0;
+    for (uint32_t pos = 0; pos < d; ++pos) {
+        const uint32_t dim = grid_dim_at(g, pos);
+        const uint32_t w = g.word[dim];
+        if (w != cur_word) {
+            keys_wm[(uint64_t)cur_word * n + i] = acc;
+            for (uint32_t z = cur_word + 1; z < w; ++z) keys_wm[(uint64_t)z * n + i] = 0u;
+            cur_word = w;
+            acc = 0;
+        }
+        const double c = floor((double)cols[dim * kPkRows + t] / eps);
+        const long long dig = (long long)c - g.off[dim];
+        acc |= (uint32_t)dig << g.shift[dim];
+    }
+    keys_wm[(uint64_t)cur_word * n + i] = acc;
+    for (uint32_t z = cur_word + 1; z < W; ++z) keys_wm[(uint64_t)z * n + i] = 0u;
+    if (norm_key) {
+        double sum = 0.0;
+        for (uint32_t k = 0; k < d; ++k) {
+            const double v = (double)cols[k * kPkRows + t] - center[k];
+            sum = fma(v, v, sum);
+        }
+        const double q = floor(sum * nscale);
+        norm_key[i] = q < 65535.0 ? (uint32_t)q : 65535u;
+    }
+}
+
+void launch_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, const GridDev &g,
+                      uint32_t W, uint32_t *keys_wm, cudaStream_t st, const double *center, double norm_scale,
+                      uint32_t *norm_key) {
+    if (n == 0) return;
+    const bool vec = ((uintptr_t)x & 15u) == 0;
+    if ((uint64_t)d * dtype_bytes <= kPkMaxRowBytes) {
+        const unsigned blocks = (unsigned)hj_ceil_div(n, kPkRows);
+        const size_t smem = (size_t)kPkRows * d * dtype_bytes;  // <= 64 KB
+        if (dtype_bytes == 8) {
+            ensure_max_dynamic_smem((const void *)k_pack_keys_staged<double>, 64 * 1024);
+            k_pack_keys_staged<double><<<blocks, kPkRows, smem, st>>>(static_cast<const double *>(x), n, d, eps, g,
+                                                                      W, keys_wm, center, norm_scale, norm_key, vec);
+        } else {
+            ensure_max_dynamic_smem((const void *)k_pack_keys_staged<float>, 64 * 1024);
+            k_pack_keys_staged<float><<<blocks, kPkRows, smem, st>>>(static_cast<const float *>(x), n, d, eps, g, W,
+                                                                     keys_wm, center, norm_scale, norm_key, vec);
+        }
+        return;
+    }
+    k_pack_keys<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(x, dtype_bytes, n, d, eps, g, W, keys_wm);
+    if (norm_key) launch_norm_key(x, dtype_bytes, n, d, center, norm_scale, norm_key, st);
 }
 
 // Exclusive scan of `count` u32 entries in place, one block of 1024 threads.
@@ -306,45 +422,272 @@ __global__ void __launch_bounds__(1024) k_scan_u32(uint32_t *a, uint64_t count, 
     if (total_out && threadIdx.x == 1023) *total_out = part[1023];
 }
 
-__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint32_t *__restrict__ keyw,
-                                                          const uint32_t *__restrict__ perm_in, uint64_t n,
-                                                          uint32_t shift, const uint32_t *__restrict__ hist,
-                                                          uint32_t nblocks, uint32_t *__restrict__ perm_out) {
-    __shared__ uint32_t s_base[256];
-    __shared__ uint32_t s_wcnt[kRsWarps][256];
-    const uint32_t t = threadIdx.x, warp = t >> 5, lane = t & 31u;
-    s_base[t] = hist[(size_t)t * nblocks + blockIdx.x];
-    const uint32_t lt_mask = (1u << lane) - 1u;
-    const uint64_t base = (uint64_t)blockIdx.x * kRsTile;
-    for (int r = 0; r < kRsTile / kRsThreads; ++r) {
-        uint64_t i = base + (uint64_t)r * kRsThreads + t;
-        bool valid = i < n;
-        uint32_t src = 0, dig = 256u;
-        if (valid) {
-            src = perm_in ? perm_in[i] : (uint32_t)i;
-            dig = (keyw[src] >> shift) & 255u;
-        }
+// ------------------------------------------------------------ radix sort
+//
+// Stable LSD radix sort of a permutation by 8-bit windows of word-major keys.
+// Every pass moves (key, index) pairs: the index (the permutation) and the
+// current key word in the current order, so that a pass reads both with
+// coalesced 128-bit loads. Per pass:
+//   k_rs_count      per 4096-item tile, the 256 digit counts;
+//   k_rs_scan_rows  one block per digit: exclusive scan of that digit's tile
+//                   counts, and the digit's total;
+//   k_rs_scatter    per tile, a stable local sort by digit in shared memory
+//                   (warp match + per-warp running counts, warps in order),
+//                   then coalesced stores of each digit's run at its global
+//                   offset (digit base + the tile's prefix within the digit).
+// The next pass's key word travels with the pair: the current word when the
+// next pass reads the same word, else the next word gathered once by index
+// (4-byte reads from an array that stays in L2 at the engine's sizes).
+
+constexpr int kRsThreads = 256;
+constexpr int kRsIpt = 16;                      // items per thread
+constexpr int kRsTile = kRsThreads * kRsIpt;    // 4096 items per tile
+constexpr int kRsWarps = kRsThreads / 32;
+constexpr int kRsWarpItems = kRsTile / kRsWarps;  // 512 consecutive items per warp
+
+static uint64_t rs_round4(uint64_t n) { return hj_ceil_div(n, 4) * 4; }
+
+size_t radix_scratch_bytes(uint64_t n) {
+    // index and key ping-pong buffers (16-byte aligned), tile counts, digit totals
+    return (3 * rs_round4(n) + 256 * hj_ceil_div(std::max<uint64_t>(n, 1), kRsTile) + 256) * 4;
+}
+
+// Tile items [base, base + 4096) of a u32 array into s[0 .. 4096): 128-bit
+// loads when the array is 16-byte aligned, 32-bit loads otherwise; items past
+// n are not loaded.
+__device__ __forceinline__ void rs_load_tile(const uint32_t *__restrict__ a, uint64_t base, uint64_t n, bool vec,
+                                             uint32_t *s) {
+    const uint32_t t = threadIdx.x;
+    if (vec && base + kRsTile <= n) {
+        const uint4 *a4 = reinterpret_cast<const uint4 *>(a + base);
 #pragma unroll
-        for (int w = 0; w < kRsWarps; ++w) s_wcnt[w][t] = 0;
-        __syncthreads();
-        uint32_t peers = __match_any_sync(0xffffffffu, dig);
-        uint32_t rank = __popc(peers & lt_mask);
-        if (valid && rank == 0) s_wcnt[warp][dig] = __popc(peers);
-        __syncthreads();
-        {
-            uint32_t run = s_base[t];
-#pragma unroll
-            for (int w = 0; w < kRsWarps; ++w) {
-                uint32_t c = s_wcnt[w][t];
-                s_wcnt[w][t] = run;
-                run += c;
-            }
-            s_base[t] = run;
+        for (int k = 0; k < kRsIpt / 4; ++k) {
+            const uint4 v = __ldg(a4 + t + k * kRsThreads);
+            reinterpret_cast<uint4 *>(s)[t + k * kRsThreads] = v;
         }
-        __syncthreads();
-        if (valid) perm_out[s_wcnt[warp][dig] + rank] = src;
-        __syncthreads();
+    } else {
+        for (uint32_t i = t; i < kRsTile; i += kRsThreads)
+            if (base + i < n) s[i] = __ldg(a + base + i);
     }
+}
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_count(const uint32_t *__restrict__ key, uint64_t n, uint32_t shift,
+                                                        uint32_t nb, bool vec, uint32_t *__restrict__ counts) {
+    __shared__ uint32_t h[256];
+    __shared__ __align__(16) uint32_t s_key[kRsTile];
+    const uint32_t t = threadIdx.x, lane = t & 31u;
+    h[t] = 0;
+    const uint64_t base = (uint64_t)blockIdx.x * kRsTile;
+    rs_load_tile(key, base, n, vec, s_key);
+    __syncthreads();
+    const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll 4
+    for (int k = 0; k < kRsIpt; ++k) {
+        const uint32_t i = t + k * kRsThreads;
+        const uint32_t dg = base + i < n ? (s_key[i] >> shift) & 255u : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+        if (dg < 256u && (peers & lt) == 0) atomicAdd(&h[dg], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    counts[(size_t)t * nb + blockIdx.x] = h[t];
+}
+
+// Exclusive scan of 1024 values held one per thread; returns the thread's
+// exclusive prefix, *total gets the sum (all threads).
+__device__ __forceinline__ unsigned long long rs_block_scan1024(unsigned long long v, unsigned long long *sh,
+                                                                unsigned long long *total) {
+    const uint32_t t = threadIdx.x, lane = t & 31u, w = t >> 5;
+    unsigned long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) sh[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        unsigned long long s = sh[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= (uint32_t)o) s += y;
+        }
+        sh[lane] = s;  // inclusive over warps
+    }
+    __syncthreads();
+    const unsigned long long before = (w ? sh[w - 1] : 0ull) + x - v;
+    *total = sh[31];
+    __syncthreads();
+    return before;
+}
+
+// One block (1024 threads) per digit: counts[dg][0 .. nb) becomes its
+// exclusive scan; totals[dg] = the digit's count over all tiles.
+__global__ void __launch_bounds__(1024) k_rs_scan_rows(uint32_t *__restrict__ counts, uint32_t nb,
+                                                      uint32_t *__restrict__ totals) {
+    __shared__ unsigned long long sh[32];
+    uint32_t *row = counts + (size_t)blockIdx.x * nb;
+    const uint32_t per = (nb + 1023) / 1024;
+    const uint32_t b = threadIdx.x * per, e = min(b + per, nb);
+    unsigned long long s = 0;
+    for (uint32_t i = b; i < e; ++i) s += row[i];
+    unsigned long long total;
+    unsigned long long run = rs_block_scan1024(s, sh, &total);
+    for (uint32_t i = b; i < e; ++i) {
+        const uint32_t v = row[i];
+        row[i] = (uint32_t)run;
+        run += v;
+    }
+    if (threadIdx.x == 0) totals[blockIdx.x] = (uint32_t)total;
+}
+
+// val_in null: the identity (first pass). key_out null: no next pass.
+// next_word non-null: key_out receives next_word[index] (the next pass reads
+// another word), else the current key. Dynamic shared memory: two tiles of
+// (key, index), the loaded one and the locally sorted one (64 KB).
+constexpr int kRsScatterSmem = 4 * kRsTile * 4;
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint32_t *__restrict__ key_in,
+                                                          const uint32_t *__restrict__ val_in, uint64_t n,
+                                                          uint32_t shift, uint32_t nb, bool vec_key,
+                                                          const uint32_t *__restrict__ counts,
+                                                          const uint32_t *__restrict__ totals,
+                                                          uint32_t *__restrict__ val_out, uint32_t *__restrict__ key_out,
+                                                          const uint32_t *__restrict__ next_word) {
+    extern __shared__ __align__(16) uint32_t rs_smem[];
+    uint32_t *s_key = rs_smem, *s_val = rs_smem + kRsTile;              // loaded tile
+    uint32_t *o_key = rs_smem + 2 * kRsTile, *o_val = rs_smem + 3 * kRsTile;  // sorted tile
+    __shared__ uint32_t s_cnt[kRsWarps][256];
+    __shared__ uint32_t s_dstart[256], s_gbase[256];
+    __shared__ unsigned long long sh[16];
+    const uint32_t t = threadIdx.x, warp = t >> 5, lane = t & 31u;
+    const uint64_t base = (uint64_t)blockIdx.x * kRsTile;
+    const uint32_t m = (uint32_t)(n - base < (uint64_t)kRsTile ? n - base : kRsTile);  // items in this tile
+    rs_load_tile(key_in, base, n, vec_key, s_key);
+    if (val_in) {
+        rs_load_tile(val_in, base, n, ((uintptr_t)val_in & 15u) == 0, s_val);
+    } else {
+        for (uint32_t i = t; i < m; i += kRsThreads) s_val[i] = (uint32_t)(base + i);
+    }
+#pragma unroll
+    for (int w = 0; w < kRsWarps; ++w) s_cnt[w][t] = 0;
+    __syncthreads();
+    // 1. ranks within each warp's 512 items, in item order (stable): warp-local
+    //    rank of item j of this lane, 0xffff for items past the tile's end
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t r_reg[kRsIpt / 2];
+#pragma unroll
+    for (int j = 0; j < kRsIpt; ++j) {
+        const uint32_t i = warp * kRsWarpItems + j * 32 + lane;
+        const bool ok = i < m;
+        const uint32_t dg = ok ? (s_key[i] >> shift) & 255u : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+        const uint32_t before = dg < 256u ? s_cnt[warp][dg] : 0u;
+        __syncwarp();
+        if (dg < 256u && (peers & lt) == 0) s_cnt[warp][dg] = before + __popc(peers);
+        __syncwarp();
+        const uint32_t r = ok ? before + __popc(peers & lt) : 0xffffu;  // < 512 for real items
+        if (j & 1)
+            r_reg[j >> 1] |= r << 16;
+        else
+            r_reg[j >> 1] = r;
+    }
+    __syncthreads();
+    // 2. per digit (thread t = digit t): warp offsets in warp order, the tile's
+    //    local digit starts, and the digit's global base for this tile
+    {
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kRsWarps; ++w) {
+            const uint32_t c = s_cnt[w][t];
+            s_cnt[w][t] = run;
+            run += c;
+        }
+        // exclusive scans over the 256 digits of the tile's digit counts (x0)
+        // and of the digits' totals over all tiles (x1)
+        const unsigned long long x0 = run, x1 = totals[t];
+        unsigned long long a = x0, b = x1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long ya = __shfl_up_sync(0xffffffffu, a, o);
+            const unsigned long long yb = __shfl_up_sync(0xffffffffu, b, o);
+            if (lane >= (uint32_t)o) a += ya, b += yb;
+        }
+        if (lane == 31) sh[warp] = a, sh[8 + warp] = b;
+        __syncthreads();
+        unsigned long long pa = 0, pb = 0;
+        for (uint32_t w = 0; w < warp; ++w) pa += sh[w], pb += sh[8 + w];
+        s_dstart[t] = (uint32_t)(pa + a - x0);
+        s_gbase[t] = (uint32_t)(pb + b - x1) + counts[(size_t)t * nb + blockIdx.x];
+    }
+    __syncthreads();
+    // 3. the tile sorted by digit into the second buffer
+#pragma unroll
+    for (int j = 0; j < kRsIpt; ++j) {
+        const uint32_t r = (r_reg[j >> 1] >> ((j & 1) * 16)) & 0xffffu;
+        if (r == 0xffffu) continue;
+        const uint32_t i = warp * kRsWarpItems + j * 32 + lane;
+        const uint32_t key = s_key[i];
+        const uint32_t dg = (key >> shift) & 255u;
+        const uint32_t pos = s_dstart[dg] + s_cnt[warp][dg] + r;
+        o_key[pos] = key;
+        o_val[pos] = s_val[i];
+    }
+    __syncthreads();
+    // 4. each digit's run to its global offset: consecutive positions of a run
+    //    go to consecutive addresses
+    for (uint32_t p = t; p < m; p += kRsThreads) {
+        const uint32_t key = o_key[p], val = o_val[p];
+        const uint32_t dg = (key >> shift) & 255u;
+        const uint32_t g = s_gbase[dg] + (p - s_dstart[dg]);
+        val_out[g] = val;
+        if (key_out) key_out[g] = next_word ? __ldg(next_word + val) : key;
+    }
+}
+
+__global__ void k_iota(uint32_t *p, uint64_t n) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = (uint32_t)i;
+}
+
+void radix_sort_perm(const uint32_t *keys_wm, uint64_t n, const std::pair<uint32_t, uint32_t> *passes, size_t np,
+                     uint32_t *perm_out, void *scratch, cudaStream_t st, int *launches) {
+    if (n == 0) return;
+    if (np == 0) {
+        k_iota<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(perm_out, n);
+        if (launches) *launches += 1;
+        return;
+    }
+    const uint64_t nn = rs_round4(n);
+    uint32_t *vtmp = static_cast<uint32_t *>(scratch);
+    uint32_t *kb[2] = {vtmp + nn, vtmp + 2 * nn};
+    const uint32_t nb = (uint32_t)hj_ceil_div(n, kRsTile);
+    uint32_t *counts = vtmp + 3 * nn;
+    uint32_t *totals = counts + (size_t)256 * nb;
+    ensure_max_dynamic_smem((const void *)k_rs_scatter, kRsScatterSmem);
+    const uint32_t *val_in = nullptr;
+    for (size_t p = 0; p < np; ++p) {
+        const uint32_t shift = passes[p].second;
+        // pass 0 reads its word of the input keys (identity order); later
+        // passes read the key that the previous pass carried
+        const uint32_t *key_in = p == 0 ? keys_wm + (size_t)passes[0].first * n : kb[p & 1];
+        const bool vec_key = ((uintptr_t)key_in & 15u) == 0;
+        uint32_t *val_out = ((np - 1 - p) & 1) ? vtmp : perm_out;
+        uint32_t *key_out = p + 1 < np ? kb[(p + 1) & 1] : nullptr;
+        const uint32_t *next_word = nullptr;
+        if (key_out && passes[p + 1].first != passes[p].first) next_word = keys_wm + (size_t)passes[p + 1].first * n;
+        k_rs_count<<<nb, kRsThreads, 0, st>>>(key_in, n, shift, nb, vec_key, counts);
+        k_rs_scan_rows<<<256, 1024, 0, st>>>(counts, nb, totals);
+        k_rs_scatter<<<nb, kRsThreads, kRsScatterSmem, st>>>(key_in, val_in, n, shift, nb, vec_key, counts, totals,
+                                                             val_out, key_out, next_word);
+        if (launches) *launches += 3;
+        val_in = val_out;
+    }
+}
+
+void radix_sort_perm(const uint32_t *keys_wm, uint64_t n, const std::vector<std::pair<uint32_t, uint32_t>> &passes,
+                     uint32_t *perm_out, void *scratch, cudaStream_t st, int *launches) {
+    radix_sort_perm(keys_wm, n, passes.data(), passes.size(), perm_out, scratch, st, launches);
 }
 
 void ensure_max_dynamic_smem(const void *func, int bytes) {
@@ -374,92 +717,56 @@ void launch_scan_u32(uint32_t *a, uint64_t count, unsigned long long *total, cud
     k_scan_u32<<<1, 1024, 0, st>>>(a, count, total);
 }
 
-__global__ void k_iota(uint32_t *p, uint64_t n) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) p[i] = (uint32_t)i;
-}
-
-void radix_sort_perm(const uint32_t *keys_wm, uint64_t n, const std::vector<std::pair<uint32_t, uint32_t>> &passes,
-                     uint32_t *perm_out, uint32_t *perm_tmp, uint32_t *hist, cudaStream_t st, int *launches) {
-    if (n == 0) return;
-    const uint32_t nb = (uint32_t)hj_ceil_div(n, kRsTile);
-    if (passes.empty()) {
-        k_iota<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(perm_out, n);
-        if (launches) *launches += 1;
-        return;
-    }
-    // ping-pong so that the last pass writes perm_out
-    const size_t np = passes.size();
-    uint32_t *bufs[2] = {perm_out, perm_tmp};
-    const uint32_t *src = nullptr;
-    for (size_t p = 0; p < np; ++p) {
-        uint32_t *dst = bufs[(np - 1 - p) & 1];
-        const uint32_t *kw = keys_wm + (size_t)passes[p].first * n;
-        const uint32_t shift = passes[p].second;
-        k_rs_hist<<<nb, kRsThreads, 0, st>>>(kw, src, n, shift, hist, nb);
-        k_scan_u32<<<1, 1024, 0, st>>>(hist, (uint64_t)nb * 256, nullptr);
-        k_rs_scatter<<<nb, kRsThreads, 0, st>>>(kw, src, n, shift, hist, nb, dst);
-        if (launches) *launches += 3;
-        src = dst;
-    }
-}
-
-// One radix pass (histogram, scan, stable scatter) and a plain iota, for
-// callers that drive the passes themselves (hj_noalloc.cu).
-void radix_sort_pass(const uint32_t *keyw, uint64_t n, uint32_t shift, const uint32_t *perm_in,
-                     uint32_t *perm_out, uint32_t *hist, cudaStream_t st) {
-    const uint32_t nb = (uint32_t)hj_ceil_div(n, kRsTile);
-    k_rs_hist<<<nb, kRsThreads, 0, st>>>(keyw, perm_in, n, shift, hist, nb);
-    k_scan_u32<<<1, 1024, 0, st>>>(hist, (uint64_t)nb * 256, nullptr);
-    k_rs_scatter<<<nb, kRsThreads, 0, st>>>(keyw, perm_in, n, shift, hist, nb, perm_out);
-}
-
 void launch_iota(uint32_t *p, uint64_t n, cudaStream_t st) {
     if (n) k_iota<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(p, n);
 }
 
-// ------------------------------------------------------------ gather
+// ------------------------------------------------------------ fused gathers
+//
+// One pass over the sorted ranks writes every layout a form reads, so each
+// input row is read from memory once. A group of 8 threads handles one sorted
+// rank; thread j of the group covers the 8-coordinate chunks j, j + 8, ... of
+// the padded width, reading the row's coordinates with 128-bit loads when
+// rows are 16-byte aligned (d * dtype_bytes a multiple of 16) and writing the
+// chunk of each layout with 128-bit stores.
 
-// Sorted keys row-major [n][W] (for binary searches) and sorted rows.
-// One warp per sorted rank: the key words and the row of input index perm[r]
-// (lanes over words and coordinates: coalesced reads and writes).
-__global__ void k_gather_keys_rows(const void *x, int dtype_bytes, uint64_t n, uint32_t d,
-                                   const uint32_t *__restrict__ perm, const uint32_t *__restrict__ keys_wm,
-                                   uint32_t W, uint32_t *__restrict__ keys_rm, void *rows_out) {
-    const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t lane = threadIdx.x & 31u;
-    if (r >= n) return;
-    const uint32_t src = perm[r];
-    if (keys_rm)
-        for (uint32_t w = lane; w < W; w += 32) keys_rm[r * W + w] = keys_wm[(uint64_t)w * n + src];
-    if (rows_out) {
-        if (dtype_bytes == 8) {
-            const double *xs = static_cast<const double *>(x) + (uint64_t)src * d;
-            double *o = static_cast<double *>(rows_out) + r * d;
-            for (uint32_t k = lane; k < d; k += 32) o[k] = xs[k];
+constexpr int kGrpRows = 32;  // ranks per 256-thread block
+
+template <typename T>
+__device__ __forceinline__ void load_chunk8(const T *row, uint32_t k0, uint32_t d, bool vec, double (&v)[8]) {
+    if (vec && k0 + 8 <= d) {
+        if (sizeof(T) == 4) {
+            const float4 a = __ldg(reinterpret_cast<const float4 *>(row + k0));
+            const float4 b = __ldg(reinterpret_cast<const float4 *>(row + k0 + 4));
+            v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
         } else {
-            const float *xs = static_cast<const float *>(x) + (uint64_t)src * d;
-            float *o = static_cast<float *>(rows_out) + r * d;
-            for (uint32_t k = lane; k < d; k += 32) o[k] = xs[k];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double2 a = __ldg(reinterpret_cast<const double2 *>(row + k0) + q);
+                v[2 * q] = a.x, v[2 * q + 1] = a.y;
+            }
         }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = k0 + q < d ? (double)__ldg(row + k0 + q) : 0.0;
     }
 }
 
-// Plain layout [tile][d][64]: element (rank r, dim k) at ((r/64)*d + k)*64 + r%64.
-// One thread per output element, so the writes are coalesced.
-__global__ void k_gather_plain(const void *x, int dtype_bytes, uint64_t n, uint32_t d,
-                               const uint32_t *__restrict__ perm, double *__restrict__ out, uint64_t n_tiles) {
-    uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    uint64_t total = n_tiles * d * 64;
-    if (e >= total) return;
-    uint32_t lane = (uint32_t)(e & 63u);
-    uint64_t q = e >> 6;
-    uint32_t k = (uint32_t)(q % d);
-    uint64_t tile = q / d;
-    uint64_t r = tile * 64 + lane;
-    double v = 0.0;
-    if (r < n) v = coord(x, dtype_bytes, (uint64_t)perm[r] * d + k);
-    out[e] = v;
+template <typename T>
+__device__ __forceinline__ void store_row_chunk(T *row, uint32_t k0, uint32_t d, bool vec, const double (&v)[8]) {
+    if (vec && k0 + 8 <= d) {
+        if (sizeof(T) == 4) {
+            reinterpret_cast<float4 *>(row + k0)[0] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+            reinterpret_cast<float4 *>(row + k0)[1] = make_float4((float)v[4], (float)v[5], (float)v[6], (float)v[7]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) reinterpret_cast<double2 *>(row + k0)[q] = make_double2(v[2 * q], v[2 * q + 1]);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            if (k0 + q < d) row[k0 + q] = (T)v[q];
+    }
 }
 
 __device__ __forceinline__ float to_tf32_rn(float v) {
@@ -468,59 +775,126 @@ __device__ __forceinline__ float to_tf32_rn(float v) {
     return __uint_as_float(u);
 }
 
-// Tensor-core layouts, one thread per (row, k) element of the padded matrix:
-// TF32 rows [npad][kp32], BF16 hi/lo rows [npad][kp16]. The operands are the
-// coordinates minus `center` (per dim): distances are shift invariant, and the
-// smaller norms narrow the error band of the norm expansion.
-// FP16 (f16 != nullptr): (x - center) * scale rounded once from FP64 to FP16
-// (round to nearest even); scale is a power of two, so the scaling is exact.
-__global__ void k_gather_tc(const void *x, int dtype_bytes, uint64_t n, uint32_t d,
-                            const uint32_t *__restrict__ perm, const double *__restrict__ center, uint64_t npad,
-                            uint32_t kp, float *tf32, uint16_t *bf_hi, uint16_t *bf_lo, uint16_t *f16,
-                            double scale) {
-    uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= npad * kp) return;
-    uint64_t r = e / kp;
-    uint32_t k = (uint32_t)(e % kp);
-    if (f16) {
-        double w = 0.0;
-        if (r < n && k < d) w = (coord(x, dtype_bytes, (uint64_t)perm[r] * d + k) - center[k]) * scale;
-        f16[e] = __half_as_ushort(__double2half(w));
-        return;
+// Tensor-core forms: sorted keys (row-major [n][W]), sorted rows (input
+// precision), the operand matrix ([npad][kp]: TF32, BF16 hi/lo, or FP16) of
+// the centred coordinates, and the FP64 centred norm of every rank (FP32,
+// padding ranks kPadNorm). FP16 operands are (x - center) * scale rounded once
+// from FP64 (scale a power of two: exact); TF32 and BF16 from the FP32 value
+// of x - center, BF16 as hi + lo with lo the BF16 of the exact remainder.
+template <typename T, int OP>  // OP: 0 TF32, 1 BF16 hi/lo, 2 FP16
+__global__ void __launch_bounds__(256) k_gather_tc_fused(const T *__restrict__ x, uint64_t n, uint32_t d,
+                                                         const uint32_t *__restrict__ perm,
+                                                         const uint32_t *__restrict__ keys_wm, uint32_t W,
+                                                         const double *__restrict__ center, uint64_t npad, uint32_t kp,
+                                                         double scale, double scale2, bool vec,
+                                                         uint32_t *__restrict__ keys_rm, T *__restrict__ rows_out,
+                                                         void *__restrict__ op_hi, uint16_t *__restrict__ op_lo,
+                                                         float *__restrict__ norms) {
+    const uint64_t r = (uint64_t)blockIdx.x * kGrpRows + (threadIdx.x >> 3);
+    const uint32_t j = threadIdx.x & 7u;
+    const bool in = r < npad;  // npad is a multiple of kGrpRows: always true at the engine's launches
+    const bool real = r < n;
+    const uint32_t src = real ? perm[r] : 0u;
+    const T *row = x + (uint64_t)src * d;
+    double part = 0.0;
+    for (uint32_t k0 = 8 * j; in && k0 < kp; k0 += 64) {
+        double v[8];
+        if (real) {
+            load_chunk8(row, k0, d, vec, v);
+            if (rows_out && k0 < d) store_row_chunk(rows_out + r * d, k0, d, vec, v);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const double c = k0 + q < d ? v[q] - center[k0 + q] : 0.0;
+                part = fma(c, c, part);
+                v[q] = c;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v[q] = 0.0;
+        }
+        if (OP == 2) {
+            uint32_t h[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                h[q] = (uint32_t)__half_as_ushort(__double2half(v[2 * q] * scale)) |
+                       ((uint32_t)__half_as_ushort(__double2half(v[2 * q + 1] * scale)) << 16);
+            reinterpret_cast<uint4 *>(static_cast<uint16_t *>(op_hi) + r * kp + k0)[0] = make_uint4(h[0], h[1], h[2], h[3]);
+        } else if (OP == 0) {
+            float f[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) f[q] = to_tf32_rn((float)v[q]);
+            float4 *o = reinterpret_cast<float4 *>(static_cast<float *>(op_hi) + r * kp + k0);
+            o[0] = make_float4(f[0], f[1], f[2], f[3]);
+            o[1] = make_float4(f[4], f[5], f[6], f[7]);
+        } else {
+            uint32_t hi[4], lo[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                uint32_t hh[2], ll[2];
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const float f = (float)v[2 * q + e];
+                    const __nv_bfloat16 b = __float2bfloat16_rn(f);
+                    const float rem = f - __bfloat162float(b);  // exact: b holds the leading bits of f
+                    hh[e] = __bfloat16_as_ushort(b);
+                    ll[e] = __bfloat16_as_ushort(__float2bfloat16_rn(rem));
+                }
+                hi[q] = hh[0] | (hh[1] << 16);
+                lo[q] = ll[0] | (ll[1] << 16);
+            }
+            reinterpret_cast<uint4 *>(static_cast<uint16_t *>(op_hi) + r * kp + k0)[0] = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+            reinterpret_cast<uint4 *>(op_lo + r * kp + k0)[0] = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        }
     }
-    float v = 0.0f;
-    if (r < n && k < d) v = (float)(coord(x, dtype_bytes, (uint64_t)perm[r] * d + k) - center[k]);
-    if (tf32) tf32[e] = to_tf32_rn(v);
-    if (bf_hi) {
-        __nv_bfloat16 h = __float2bfloat16_rn(v);
-        float rem = v - __bfloat162float(h);  // exact: h holds the leading bits of v
-        __nv_bfloat16 l = __float2bfloat16_rn(rem);
-        bf_hi[e] = __bfloat16_as_ushort(h);
-        bf_lo[e] = __bfloat16_as_ushort(l);
-    }
+    // norm of the rank: sum over the group's 8 lanes
+    part += __shfl_xor_sync(0xffffffffu, part, 4);
+    part += __shfl_xor_sync(0xffffffffu, part, 2);
+    part += __shfl_xor_sync(0xffffffffu, part, 1);
+    if (in && j == 0) norms[r] = real ? (float)(part * scale2) : kPadNorm;
+    if (real && keys_rm)
+        for (uint32_t w = j; w < W; w += 8) keys_rm[r * W + w] = keys_wm[(uint64_t)w * n + src];
 }
 
-// |x - center|^2 per sorted row in FP64 (input precision widened exactly),
-// stored as FP32; padding rows get kPadNorm so that they never pass a threshold.
-__global__ void k_norms(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const uint32_t *__restrict__ perm,
-                        const double *__restrict__ center, uint64_t npad, double scale2, float *norms) {
-    const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t lane = threadIdx.x & 31u;
-    if (r >= npad) return;
-    if (r >= n) {
-        if (lane == 0) norms[r] = kPadNorm;
-        return;
+// Plain form and row-only gathers: sorted keys and sorted rows, a group of 8
+// threads per rank as above (no padding ranks).
+template <typename T>
+__global__ void __launch_bounds__(256) k_gather_rows_fused(const T *__restrict__ x, uint64_t n, uint32_t d,
+                                                           const uint32_t *__restrict__ perm,
+                                                           const uint32_t *__restrict__ keys_wm, uint32_t W, bool vec,
+                                                           uint32_t *__restrict__ keys_rm, T *__restrict__ rows_out) {
+    const uint64_t r = (uint64_t)blockIdx.x * kGrpRows + (threadIdx.x >> 3);
+    const uint32_t j = threadIdx.x & 7u;
+    if (r >= n) return;
+    const uint32_t src = perm[r];
+    if (rows_out) {
+        const T *row = x + (uint64_t)src * d;
+        for (uint32_t k0 = 8 * j; k0 < d; k0 += 64) {
+            double v[8];
+            load_chunk8(row, k0, d, vec, v);
+            store_row_chunk(rows_out + r * d, k0, d, vec, v);
+        }
     }
-    const uint64_t src = perm[r];
-    double s = 0.0;
-    for (uint32_t k = lane; k < d; k += 32) {
-        const double v = coord(x, dtype_bytes, src * d + k) - center[k];
-        s = fma(v, v, s);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) norms[r] = (float)(s * scale2);
+    if (keys_rm)
+        for (uint32_t w = j; w < W; w += 8) keys_rm[r * W + w] = keys_wm[(uint64_t)w * n + src];
 }
+
+// Plain layout [tile][d][64]: element (rank r, dim k) at ((r/64)*d + k)*64 + r%64.
+// One block per 64-rank tile; thread (k4 = t / 64, lane = t % 64) writes dims
+// k4, k4 + 4, ... of rank lane: each store instruction writes 64 consecutive
+// doubles, and the tile's rows are re-read from L1.
+template <typename T>
+__global__ void __launch_bounds__(256) k_gather_plain_tiles(const T *__restrict__ x, uint64_t n, uint32_t d,
+                                                            const uint32_t *__restrict__ perm,
+                                                            double *__restrict__ out) {
+    const uint64_t tile = blockIdx.x;
+    const uint32_t lane = threadIdx.x & 63u, k4 = threadIdx.x >> 6;
+    const uint64_t r = tile * 64 + lane;
+    const T *row = r < n ? x + (uint64_t)perm[r] * d : nullptr;
+    double *o = out + tile * d * 64 + lane;
+    for (uint32_t k = k4; k < d; k += 4) o[(uint64_t)k * 64] = row ? (double)__ldg(row + k) : 0.0;
+}
+
+// ------------------------------------------------------------ norm summaries
 
 // Per-tile maximum norm over real rows (padding rows excluded).
 __global__ void k_tile_max(const float *__restrict__ v, uint64_t npad, int tile, float *out) {
@@ -548,59 +922,56 @@ void launch_gather(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const
                    int *launches) {
     int L = 0;
     if (n == 0) return;
-    if (flags & (kGatherKeys | kGatherRows)) {
-        k_gather_keys_rows<<<(unsigned)hj_ceil_div(n, 8), 256, 0, st>>>(  // a warp per rank
-            x, dtype_bytes, n, d, perm, keys_wm, W, (flags & kGatherKeys) ? o.keys : nullptr,
-            (flags & kGatherRows) ? const_cast<void *>(o.rows) : nullptr);
+    const bool vec = ((uintptr_t)x & 15u) == 0 && ((uint64_t)d * dtype_bytes) % 16 == 0;
+    uint32_t *keys_rm = (flags & kGatherKeys) ? o.keys : nullptr;
+    void *rows_out = (flags & kGatherRows) ? const_cast<void *>(o.rows) : nullptr;
+    const int op = (flags & kGatherTf32) ? 0 : (flags & kGatherBf16) ? 1 : (flags & kGatherF16) ? 2 : -1;
+    if (op >= 0) {
+        // every tensor-core layout in one pass (operands, norms, keys, rows)
+        const uint32_t kp = op == 0 ? o.kpad_tf32 : o.kpad_bf16;
+        void *hi = op == 0 ? (void *)o.tf32 : (void *)o.bf_hi;
+        const double scale = op == 2 ? o.op_scale : 1.0;
+        const double scale2 = op == 2 ? o.op_scale * o.op_scale : 1.0;
+        const unsigned blocks = (unsigned)hj_ceil_div(o.npad_tc, kGrpRows);
+#define HJ_GATHER_TC(T, OPV)                                                                                        \
+    k_gather_tc_fused<T, OPV><<<blocks, 256, 0, st>>>(static_cast<const T *>(x), n, d, perm, keys_wm, W, o.center,   \
+                                                      o.npad_tc, kp, scale, scale2, vec, keys_rm,                    \
+                                                      static_cast<T *>(rows_out), hi, o.bf_lo, o.norms)
+        if (dtype_bytes == 8) {
+            if (op == 0) HJ_GATHER_TC(double, 0); else if (op == 1) HJ_GATHER_TC(double, 1); else HJ_GATHER_TC(double, 2);
+        } else {
+            if (op == 0) HJ_GATHER_TC(float, 0); else if (op == 1) HJ_GATHER_TC(float, 1); else HJ_GATHER_TC(float, 2);
+        }
+#undef HJ_GATHER_TC
+        launch_norm_summaries(o.norms, o.npad_tc, o.tile_maxnorm_a, o.tile_maxnorm_b, o.group_minnorm, st);
+        L += 4;
+    } else if (keys_rm || rows_out) {
+        const unsigned blocks = (unsigned)hj_ceil_div(n, kGrpRows);
+        if (dtype_bytes == 8)
+            k_gather_rows_fused<double><<<blocks, 256, 0, st>>>(static_cast<const double *>(x), n, d, perm, keys_wm, W,
+                                                                vec, keys_rm, static_cast<double *>(rows_out));
+        else
+            k_gather_rows_fused<float><<<blocks, 256, 0, st>>>(static_cast<const float *>(x), n, d, perm, keys_wm, W,
+                                                               vec, keys_rm, static_cast<float *>(rows_out));
         ++L;
     }
     if (flags & kGatherPlain) {
-        uint64_t total = o.n_tiles64 * d * 64;
-        k_gather_plain<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.tiles64,
-                                                                         o.n_tiles64);
+        if (dtype_bytes == 8)
+            k_gather_plain_tiles<double><<<(unsigned)o.n_tiles64, 256, 0, st>>>(static_cast<const double *>(x), n, d,
+                                                                                perm, o.tiles64);
+        else
+            k_gather_plain_tiles<float><<<(unsigned)o.n_tiles64, 256, 0, st>>>(static_cast<const float *>(x), n, d,
+                                                                               perm, o.tiles64);
         ++L;
-    }
-    if (flags & kGatherTf32) {
-        uint64_t total = o.npad_tc * o.kpad_tf32;
-        k_gather_tc<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.center,
-                                                                      o.npad_tc, o.kpad_tf32, o.tf32, nullptr,
-                                                                      nullptr, nullptr, 1.0);
-        ++L;
-    }
-    if (flags & kGatherBf16) {
-        uint64_t total = o.npad_tc * o.kpad_bf16;
-        k_gather_tc<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.center,
-                                                                      o.npad_tc, o.kpad_bf16, nullptr, o.bf_hi,
-                                                                      o.bf_lo, nullptr, 1.0);
-        ++L;
-    }
-    if (flags & kGatherF16) {
-        uint64_t total = o.npad_tc * o.kpad_bf16;
-        k_gather_tc<<<(unsigned)hj_ceil_div(total, 256), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.center,
-                                                                      o.npad_tc, o.kpad_bf16, nullptr, nullptr,
-                                                                      nullptr, o.bf_hi, o.op_scale);
-        ++L;
-    }
-    if (flags & kGatherNorms) {
-        k_norms<<<(unsigned)hj_ceil_div(o.npad_tc, 8), 256, 0, st>>>(x, dtype_bytes, n, d, perm, o.center,
-                                                                      o.npad_tc, o.op_scale * o.op_scale,
-                                                                      o.norms);
-        k_tile_max<<<(unsigned)hj_ceil_div(o.npad_tc / kTcTileA, 256), 256, 0, st>>>(o.norms, o.npad_tc, kTcTileA,
-                                                                                    o.tile_maxnorm_a);
-        k_tile_max<<<(unsigned)hj_ceil_div(o.npad_tc / kTcTileB, 256), 256, 0, st>>>(o.norms, o.npad_tc, kTcTileB,
-                                                                                    o.tile_maxnorm_b);
-        k_group_min<<<(unsigned)hj_ceil_div(o.npad_tc / 32, 256), 256, 0, st>>>(o.norms, o.npad_tc, 32,
-                                                                              o.group_minnorm);
-        L += 4;
     }
     if (launches) *launches += L;
 }
 
-void launch_norm_summaries(const float *norms, uint64_t npad, float *tmax128, float *tmax256, float *gmin32,
+void launch_norm_summaries(const float *norms, uint64_t npad, float *tmax_a, float *tmax_b, float *gmin32,
                            cudaStream_t st) {
     if (npad == 0) return;
-    k_tile_max<<<(unsigned)hj_ceil_div(npad / 128, 256), 256, 0, st>>>(norms, npad, 128, tmax128);
-    k_tile_max<<<(unsigned)hj_ceil_div(npad / 256, 256), 256, 0, st>>>(norms, npad, 256, tmax256);
+    k_tile_max<<<(unsigned)hj_ceil_div(npad / kTcTileA, 256), 256, 0, st>>>(norms, npad, kTcTileA, tmax_a);
+    k_tile_max<<<(unsigned)hj_ceil_div(npad / kTcTileB, 256), 256, 0, st>>>(norms, npad, kTcTileB, tmax_b);
     k_group_min<<<(unsigned)hj_ceil_div(npad / 32, 256), 256, 0, st>>>(norms, npad, 32, gmin32);
 }
 

@@ -4,12 +4,24 @@
 // submitted from any host thread into a queue and return a request id at once.
 // A pool of `max_inflight` worker threads, each with its own device context and
 // CUDA stream, takes requests in arrival order as soon as (a) a worker is free
-// and (b) the request's working-memory estimate fits in what is left of the
-// memory budget; its kernels then run concurrently with the other admitted
-// requests' kernels on the same device (continuous batching across streams). A
-// request larger than the whole budget is rejected with HJ_ERR_BUSY. Every
-// request's count is computed by the same pipeline as a standalone call, so a
-// result does not depend on what else is in flight.
+// and (b) the request fits the memory budget; its kernels then run
+// concurrently with the other admitted requests' kernels on the same device
+// (continuous batching across streams). A request larger than the whole budget
+// is rejected with HJ_ERR_BUSY. Every request's count is computed by the same
+// pipeline as a standalone call, so a result does not depend on what else is
+// in flight.
+//
+// Memory: each worker's engine context keeps its device buffers between
+// requests (reused, grow-only). The budget is charged with what every worker
+// really holds, measured after each request, and with the estimate of each
+// running request where that is larger (engine_join_bytes_estimate). A worker
+// that holds more than its share of the budget (budget / max_inflight) when
+// it finishes frees its buffers, and every idle worker frees them when no
+// queued request fits. So the device memory of the server's requests
+// stays within the budget, up to what a request takes beyond its estimate
+// while it runs. When the head of the queue does not fit, a free worker may
+// take a later request that does (backfill), unless the head has waited
+// longer than kHeadWaitMs.
 //
 // With batch_max > 1 (tensor-core forms) a free worker takes the queue's head
 // and then further queued requests of the same dtype while they fit in the
@@ -19,6 +31,7 @@
 // run (e.g. d > 256) falls back to one call per request.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -66,19 +79,23 @@ struct hj_server {
     std::map<uint64_t, Request> reqs;
     std::map<uint64_t, DevSet> sets;
     uint64_t next_id = 1, next_set = 1;
-    uint64_t mem_in_use = 0;
+    std::vector<uint64_t> held;     // per worker: bytes its context holds (measured)
+    std::vector<uint64_t> charged;  // per worker: max(held, estimate of its running requests)
     bool stop = false;
     std::vector<std::thread> workers;
 };
 
-static uint64_t request_bytes(const DevSet &a, const DevSet &b, bool self) {
-    // sorted rows + one distance layout + keys/permutations per point, plus the
-    // work list and band queue
-    auto per_set = [](const DevSet &s) -> uint64_t {
-        return s.n * (uint64_t)s.d * 20ull + s.n * 64ull;
-    };
-    uint64_t m = per_set(a) + (self ? 0 : per_set(b));
-    return m + (64ull << 20);
+constexpr double kHeadWaitMs = 1000.0;
+
+static uint64_t request_bytes(const hj_server *s, const DevSet &a, const DevSet &b, bool self) {
+    return hj::engine_join_bytes_estimate(a.n, self ? a.n : b.n, a.d, a.dtype_bytes, s->opts.form, self);
+}
+
+static uint64_t charged_by_others(const hj_server *s, int w) {
+    uint64_t t = 0;
+    for (size_t v = 0; v < s->charged.size(); ++v)
+        if ((int)v != w) t += s->charged[v];
+    return t;
 }
 
 // Fills a finished request's result and releases its memory and sets (lock held).
@@ -95,7 +112,6 @@ static void finish_request(hj_server *s, uint64_t id, int status, uint64_t count
     r.res.latency_ms = std::chrono::duration<double, std::milli>(r.t_end - r.t_submit).count();
     r.res.candidate_pairs = status == HJ_OK ? candidate_pairs : 0;
     r.res.band_pairs = status == HJ_OK ? band_pairs : 0;
-    s->mem_in_use -= r.mem;
     for (uint64_t sid : {r.a, r.b}) {
         auto it = s->sets.find(sid);
         if (it != s->sets.end()) {
@@ -112,44 +128,77 @@ static bool tc_form(int f) {
     return f == HJ_FORM_TC_FP16 || f == HJ_FORM_TC_TF32 || f == HJ_FORM_TC_BF16X3 || f == HJ_FORM_AUTO;
 }
 
-static void worker_main(hj_server *s) {
+static void worker_main(hj_server *s, int w) {
     cudaSetDevice(s->device);
     cudaStream_t stream = nullptr;
     cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
     const int batch_max = tc_form(s->opts.form) && s->opts.batch_max > 1 ? s->opts.batch_max : 1;
+    const uint64_t budget = s->opts.memory_budget_bytes;
+    const uint64_t share = budget / (uint64_t)std::max(1, s->opts.max_inflight);
     for (;;) {
         std::vector<uint64_t> ids;
         std::vector<Request> rqs;
         std::vector<DevSet> sa, sb;
         {
             std::unique_lock<std::mutex> lk(s->mu);
+            size_t pick = 0;
             for (;;) {
                 if (s->stop) {
+                    lk.unlock();
+                    hj::engine_ctx_trim(s->device, stream);
                     if (stream) cudaStreamDestroy(stream);
                     return;
                 }
                 if (!s->queue.empty()) {
-                    Request &front = s->reqs[s->queue.front()];
-                    if (s->mem_in_use + front.mem <= s->opts.memory_budget_bytes || s->mem_in_use == 0) break;
+                    const uint64_t others = charged_by_others(s, w);
+                    auto fits = [&](const Request &r) { return others + std::max(s->held[w], r.mem) <= budget; };
+                    const Request &head = s->reqs[s->queue.front()];
+                    const double head_wait =
+                        std::chrono::duration<double, std::milli>(Clock::now() - head.t_submit).count();
+                    bool found = false;
+                    for (size_t q = 0; q < s->queue.size(); ++q) {
+                        if (q > 0 && head_wait > kHeadWaitMs) break;  // no backfill past a starving head
+                        if (fits(s->reqs[s->queue[q]])) {
+                            pick = q;
+                            found = true;
+                            break;
+                        }
+                    }
+                    if (found) break;
+                    if (s->held[w] > 0) {
+                        // nothing fits: an idle worker frees its buffers (every idle
+                        // worker does so when woken), then all check again
+                        lk.unlock();
+                        hj::engine_ctx_trim(s->device, stream);
+                        lk.lock();
+                        s->held[w] = s->charged[w] = 0;
+                        s->cv_work.notify_all();
+                        continue;
+                    }
                 }
                 s->cv_work.wait(lk);
             }
-            // the head, then followers of the same dtype while they fit the budget
+            // the picked request, then (batching) followers of the same dtype that fit
             int dtype = 0;
-            while (!s->queue.empty() && (int)ids.size() < batch_max) {
-                Request &r = s->reqs[s->queue.front()];
+            uint64_t est = 0;
+            while (pick < s->queue.size() && (int)ids.size() < batch_max) {
+                Request &r = s->reqs[s->queue[pick]];
                 const DevSet &a = s->sets[r.a];
-                if (!ids.empty() && (a.dtype_bytes != dtype || s->mem_in_use + r.mem > s->opts.memory_budget_bytes))
-                    break;
+                if (!ids.empty() && (a.dtype_bytes != dtype ||
+                                     charged_by_others(s, w) + std::max(s->held[w], est + r.mem) > budget)) {
+                    ++pick;
+                    continue;
+                }
                 dtype = a.dtype_bytes;
+                est += r.mem;
                 ids.push_back(r.id);
-                s->queue.pop_front();
-                s->mem_in_use += r.mem;
+                s->queue.erase(s->queue.begin() + (long)pick);
                 r.t_start = Clock::now();
                 rqs.push_back(r);
                 sa.push_back(a);
                 sb.push_back(s->sets[r.b]);
             }
+            s->charged[w] = std::max(s->held[w], est);
             s->cv_work.notify_all();
         }
         hj_opts o;
@@ -202,8 +251,15 @@ static void worker_main(hj_server *s) {
                 }
             }
         }
+        // what the context holds now; above this worker's share it is freed
+        uint64_t held = hj::engine_ctx_bytes(s->device);
+        if (held > share) {
+            hj::engine_ctx_trim(s->device, stream);
+            held = 0;
+        }
         {
             std::lock_guard<std::mutex> lk(s->mu);
+            s->held[w] = s->charged[w] = held;
             for (size_t i = 0; i < k; ++i) finish_request(s, ids[i], status[i], count[i], form_used[i], cand[i], band[i]);
         }
         s->cv_done.notify_all();
@@ -242,7 +298,9 @@ int hj_server_create(const hj_server_opts *opts, hj_server **out) {
     hj_server *s = new hj_server();
     s->opts = o;
     s->device = dev;
-    for (int i = 0; i < o.max_inflight; ++i) s->workers.emplace_back(worker_main, s);
+    s->held.assign(o.max_inflight, 0);
+    s->charged.assign(o.max_inflight, 0);
+    for (int i = 0; i < o.max_inflight; ++i) s->workers.emplace_back(worker_main, s, i);
     *out = s;
     return HJ_OK;
 }
@@ -316,7 +374,7 @@ int hj_submit(hj_server *s, uint64_t set_a, uint64_t set_b, double eps, uint64_t
     r.a = set_a;
     r.b = set_b;
     r.eps = eps;
-    r.mem = request_bytes(ia->second, ib->second, set_a == set_b);
+    r.mem = request_bytes(s, ia->second, ib->second, set_a == set_b);
     r.t_submit = Clock::now();
     if (r.mem > s->opts.memory_budget_bytes) return HJ_ERR_BUSY;
     ia->second.users++;

@@ -200,7 +200,7 @@ HJ_API int hj_ego_sort(const double *pts, uint64_t n, uint32_t d, double eps, co
  * cudaMalloc's implicit synchronisation. All temporaries live in one fixed
  * 32 MiB array inside libhj.so (a file-scope __device__ array that every GPU
  * loading the library holds until the process exits); sizes whose temporaries
- * exceed it (about 4 n (W + 2) bytes, W = 32-bit words of the packed cell key)
+ * exceed it (about 4 n (W + 4) bytes, W = 32-bit words of the packed cell key)
  * are rejected with HJ_ERR_INVALID_ARG. pts: device rows [n][d], dtype_bytes 8
  * or 4; perm: device uint32 [n] output, the same stable order as hj_ego_sort.
  * The first call on a device looks up the array's address
@@ -256,6 +256,15 @@ HJ_API void hj_test_ego_loop3_noself(const size_t nA, const size_t nB, const int
  * Not thread-safe; no reference counterpart. */
 HJ_API int hj_debug_tc_estimates(const float *A, uint64_t nA, const float *B, uint64_t nB, uint32_t d, int form,
                                  float *out);
+
+/* Testing hook: with gate_ns > 0, every following tensor-core kernel launch
+ * of this process makes its epilogue wait gate_ns on a device barrier that
+ * nothing arrives on; the wait runs out, the kernel raises its timeout error,
+ * drains the copies and MMAs it issued, frees its tensor memory and returns,
+ * and the call returns HJ_ERR_TIMEOUT. 0 restores normal operation. gate_ns
+ * must not exceed the engine's wait limit (2 s). Not thread-safe; no
+ * reference counterpart (the reference has no device waits). */
+HJ_API int hj_debug_set_wait_gate(uint64_t gate_ns);
 
 /* ---------------------------------------------------------------- batching
  * Many joins of uneven n, d and eps in one persistent tensor-core launch. The

@@ -66,3 +66,46 @@ def test_poll_until_done(hj):
             res = srv.poll(rid)
             time.sleep(0.001)
         assert res is not None and res["count"] == hj.self_join_count(x, 0.2)
+
+
+def test_device_memory_stays_within_budget(hj):
+    """A budget that admits only a few of these requests at a time: while 24
+    joins of uneven size run through 8 workers, the device memory the server
+    takes (free memory before the requests minus its lowest value during them)
+    stays within the budget plus 256 MB of slack (per-context counters, events
+    and the kernels' code loaded on first use). Workers' buffers are charged
+    against the budget and freed when nothing else fits."""
+    import threading
+    import time
+    import torch
+    from hilbertjoin_b200 import serving
+    from hilbertjoin_b200 import workloads as W
+    budget = 700 << 20
+    sizes = [150_000, 60_000, 100_000, 20_000, 150_000, 80_000]
+    xs = [W.uniform(n, 32, 300 + i, dtype=np.float32) for i, n in enumerate(sizes)]
+    eps = [W.calibrate_eps(x, x.shape[0], 32, sample=2000) for x in xs]
+    with serving.Server(form="fp16", memory_budget_bytes=budget, max_inflight=8) as srv:
+        ids = [srv.upload(x) for x in xs]
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        low = [free0]
+        done = threading.Event()
+
+        def sample():
+            while not done.is_set():
+                low[0] = min(low[0], torch.cuda.mem_get_info()[0])
+                time.sleep(0.002)
+
+        th = threading.Thread(target=sample)
+        th.start()
+        try:
+            rids = [srv.submit(ids[i % len(xs)], None, eps[i % len(xs)]) for i in range(24)]
+            res = [srv.wait(r) for r in rids]
+        finally:
+            done.set()
+            th.join()
+    assert all(r["status"] == 0 for r in res)
+    for i in range(len(xs)):
+        assert res[i]["count"] == hj.self_join_count(xs[i], eps[i], form="fp16")
+    used = free0 - low[0]
+    assert used <= budget + (256 << 20), (used >> 20, budget >> 20)

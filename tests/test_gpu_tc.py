@@ -154,3 +154,55 @@ def test_auto_form_picks_by_size_and_stays_exact(hj):
     eps_w = W.calibrate_eps(wide, 3000, 16)
     c, st = hj.self_join_count(wide, eps_w, form="auto", return_stats=True)
     assert st["form_used"] == "tc_fp16" and c == hj.self_join_count(wide, eps_w)
+
+
+def _cancellation_sets(d, n_a, n_b, seed):
+    """Mixed-sign coordinates of equal magnitude c with small noise: every A
+    point has a random sign pattern; half of the B points copy an A point's
+    signs on the first d/2 dims and flip them on the rest, so that their dot
+    product climbs to about +c^2 d/2 and cancels back to about 0 -- the
+    accumulator's running sum peaks far above the result. The other B points
+    are random. Centring (per-dim midpoint) leaves the patterns as they are."""
+    rng = np.random.default_rng(seed)
+    c = 3.0
+    sa = rng.choice([-1.0, 1.0], size=(n_a, d))
+    sb = rng.choice([-1.0, 1.0], size=(n_b, d))
+    pick = rng.integers(0, n_a, size=n_b // 2)
+    sb[: n_b // 2, : d // 2] = sa[pick, : d // 2]
+    sb[: n_b // 2, d // 2:] = -sa[pick, d // 2:]
+    a = c * sa + 0.05 * rng.standard_normal((n_a, d))
+    b = c * sb + 0.05 * rng.standard_normal((n_b, d))
+    return a.astype(np.float32), b.astype(np.float32), pick
+
+
+@pytest.mark.parametrize("form", ["tf32", "bf16x3", "fp16"])
+def test_estimates_within_bound_under_cancellation(hj, form):
+    """K = 256 (d = 256), mixed signs, the running sum of the dot product far
+    above its result: every estimate stays within the derived bound. The largest
+    |error| / bound ratio is printed for the record."""
+    d = 256
+    a, b, _ = _cancellation_sets(d, 500, 600, 7)
+    est = hj.tc_estimates(a, b, form).astype(np.float64)
+    ex = exact_dist2(a, b)
+    both = np.concatenate([a, b]).astype(np.float64)
+    center = 0.5 * both.min(0) + 0.5 * both.max(0)
+    na = ((a.astype(np.float64) - center) ** 2).sum(1)
+    nb = ((b.astype(np.float64) - center) ** 2).sum(1)
+    c_rel = bound_constants(hj, form, a, b)
+    ratio = np.abs(est - ex) / (c_rel * (na[:, None] + nb[None, :]))
+    print(f"cancellation d={d} form={form}: max |err|/bound = {ratio.max():.4f}")
+    assert np.isfinite(est).all()
+    assert ratio.max() < 1.0, (form, float(ratio.max()))
+
+
+@pytest.mark.parametrize("form", ["tf32", "bf16x3", "fp16"])
+def test_count_exact_under_cancellation(hj, form):
+    """eps^2 at the median distance of the cancelling pairs: those pairs sit at
+    the band; the count is the FP64 oracle's."""
+    d = 256
+    a, b, pick = _cancellation_sets(d, 1500, 1600, 8)
+    d2 = ((a[pick[:300]].astype(np.float64) - b[:300].astype(np.float64)) ** 2).sum(1)
+    eps = float(np.sqrt(np.median(d2)))
+    want = oracle.join_count_brute(a.astype(np.float64), b.astype(np.float64), eps)
+    got, st = hj.join_count(a, b, eps, form=form, return_stats=True)
+    assert got == want, (form, got, want, st["band_pairs"], st["fp64_items"])
