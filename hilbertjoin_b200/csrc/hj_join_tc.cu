@@ -771,8 +771,18 @@ __global__ void k_recheck(const TcJob *__restrict__ jobs, const BandEntry *__res
 //   operand rounding (TF32: 2 * 2^-11 relative per product; BF16 split:
 //   a = a_hi + a_lo + r with |r| <= 2^-16 |a|, dropped a_lo b_lo and r terms
 //   <= 3.1 * 2^-16 |a_k b_k|), FP32 rounding of FP64 inputs (2 * 2^-24),
-//   tensor-core FP32 accumulation budgeted at 2^-22 of the running sum per
-//   product term (K terms TF32, 3K BF16), |a.b| <= sum |a_k b_k| <=
+//   tensor-core FP32 accumulation budgeted at 2^-22 of S = sum |a_k b_k| per
+//   product term (K terms TF32, 3K BF16). The budget follows the model that
+//   Fasi, Higham, Mikaitis and Pranesh (Numerical behavior of NVIDIA tensor
+//   cores, PeerJ Computer Science 7:e330, 2021) measured for earlier tensor
+//   cores: each hardware step adds k products (exact) to the accumulator after
+//   aligning all k + 1 terms to the largest exponent and truncating them to
+//   FP32's 24 bits, then truncates the sum to FP32. Each truncation loses less
+//   than 2^-23 of the largest term, which is at most S, so a step loses less
+//   than (k + 2) 2^-23 S and the K / k steps less than K (1 + 2/k) 2^-23 S,
+//   within K 2^-22 S for every k >= 2. tests/test_gpu_tc.py checks the whole
+//   bound on adversarial cancellation at K = 256 (running sums far above the
+//   result) for every form. |a.b| <= sum |a_k b_k| <=
 //   (|a|^2 + |b|^2) / 2 (Cauchy-Schwarz, AM-GM) -- the dot error enters s
 //   twice; FP32 norms (2^-24 each) and the FP32 epilogue (three roundings of
 //   values up to 2 (|a|^2 + |b|^2), 6 * 2^-24, budgeted 10 * 2^-24); the FP64
