@@ -90,3 +90,25 @@ def test_fma_pair_semantics():
     # the pair test is inclusive: a pair at exactly eps counts
     x = np.array([[0.0, 0.0], [0.5, 0.0]])
     assert oracle.self_count_brute(x, 0.5) == 1
+
+
+CONFIGS = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "config_counts.json")))["configs"]
+
+
+@pytest.mark.parametrize("name", sorted(CONFIGS))
+def test_config_fixture_reference_equals_oracle(name):
+    """At the benchmark configurations' stated sizes the reference built from its
+    own sources and the oracle return the same count (tests/golden/
+    make_config_golden.py), and the fixture's eps is the one the workload
+    generator derives now."""
+    from hilbertjoin_b200 import workloads as W
+    c = CONFIGS[name]
+    assert c["ref_count"] == c["oracle_count"], name
+    spec = W.CONFIGS[name]
+    if "eps" in spec:
+        assert c["eps"] == spec["eps"]
+    elif name.startswith("cfg4"):
+        pytest.skip("regenerating the 4M-point set is left to the GPU test")
+    else:
+        _, _, eps = W.config_sets(name)
+        assert c["eps"] == eps
