@@ -76,9 +76,10 @@ HJ_DEVICE_INLINE bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 }
 
 // Waits until the phase with the given parity has completed. Returns false
-// (and raises kErrTimeout in *err) if that takes longer than kWaitLimitNs or if
-// another thread already raised an error.
-HJ_DEVICE_INLINE bool mbar_wait(uint64_t *bar, uint32_t parity, volatile uint32_t *err) {
+// (and raises kErrTimeout in *err, with `site` in bits 8..15 to tell which
+// wait gave up) if that takes longer than kWaitLimitNs or if another thread
+// already raised an error.
+HJ_DEVICE_INLINE bool mbar_wait(uint64_t *bar, uint32_t parity, volatile uint32_t *err, uint32_t site = 0) {
     if (mbar_try_wait(bar, parity)) return true;
     uint64_t t0 = globaltimer_ns();
     for (uint32_t it = 1;; ++it) {
@@ -86,7 +87,7 @@ HJ_DEVICE_INLINE bool mbar_wait(uint64_t *bar, uint32_t parity, volatile uint32_
         if ((it & 255u) == 0) {
             if (*err != 0) return false;
             if (globaltimer_ns() - t0 > kWaitLimitNs) {
-                atomicOr((uint32_t *)err, kErrTimeout);
+                atomicOr((uint32_t *)err, kErrTimeout | ((site & 0xffu) << 8));
                 return false;
             }
         }

@@ -631,7 +631,11 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
     if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("distance kernel");
     if (int rr = check_cuda("distance kernel")) return rr;
     const uint32_t kerr = (uint32_t)c->h_small[3];
-    if (kerr & kErrTimeout) return fail(HJ_ERR_TIMEOUT, "a bounded device-side wait timed out");
+    if (kerr & kErrTimeout) {
+        char msg[96];
+        snprintf(msg, sizeof msg, "a bounded device-side wait timed out (error word 0x%x)", kerr);
+        return fail(HJ_ERR_TIMEOUT, msg);
+    }
     if (kerr) return fail(HJ_ERR_CUDA, "device error word set");
     *count = c->h_small[2] + c->h_small[6];
     if (stats) {

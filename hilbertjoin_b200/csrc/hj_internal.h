@@ -16,7 +16,7 @@ namespace hj {
 
 // Point-tile sizes of the two distance kernels.
 constexpr int kPlainTile = 64;   // plain FP64 kernel: 64 x 64 point tiles
-constexpr int kTcTileA = 256;    // tensor-core kernel: 256 A rows (UMMA M of a CTA pair) ...
+constexpr int kTcTileA = 128;    // tensor-core kernel: 128 A rows (UMMA M) ...
 constexpr int kTcTileB = 256;    // ... against 256 B rows (UMMA N)
 constexpr int kMaxActiveDims = 5;
 constexpr int kMaxCombos = 243;  // 3^kMaxActiveDims

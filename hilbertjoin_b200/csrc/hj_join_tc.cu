@@ -6,21 +6,16 @@
 //     |a - b|^2 = |a|^2 + |b|^2 - 2 a.b      (egojoin.h:182-195, :329-381),
 // and the a.b tile on the 5th-generation tensor cores:
 //
-//   * persistent CTA pairs (clusters of two CTAs on two SMs), one per two
-//     SMs, warp-specialised, each pair on a 256 x 256 block of dot products
-//     per B tile with tcgen05.mma.cta_group::2 (M = 256, N = 256):
-//       warp 0   TMA producer in each CTA: its 128 A rows (once per work
-//                item, two A buffers) and its 128 B rows per B tile, one
-//                128-byte K atom (16 KB) at a time into a ring of stages;
-//       warp 1   leader CTA: MMA issuer (one thread), operands from both
-//                CTAs' shared memory (128-byte swizzled, K-major), two
-//                accumulators in flight (512 TMEM columns in each CTA);
-//                peer CTA: relays the completion of its own copies to the
-//                leader, so that every copy completes on the CTA that issued
-//                it and each CTA can drain its own copies;
-//       warps 2-9 epilogue in each CTA: tcgen05.ld of its 128 accumulator rows
-//                (TMEM lane quadrant = warp % 4, two warps per quadrant on 128
-//                columns each), dist^2 estimate, classification, count;
+//   * one persistent CTA per SM, 6 warps, warp-specialised:
+//       warp 0   TMA producer: the A tile (128 EGO ranks x K) once per work
+//                item into one of two A buffers, then the B tiles (256 ranks)
+//                one 128-byte K atom (32 KB) at a time into a ring of stages;
+//       warp 1   MMA issuer (one thread): tcgen05.mma, M=128, N=256, operands
+//                from shared memory (128-byte swizzled, K-major), accumulator
+//                in tensor memory, two accumulators in flight (512 columns);
+//       warps 2-9 epilogue: tcgen05.ld of the accumulator rows (TMEM lane
+//                quadrant = warp % 4, two warps per quadrant on 128 columns
+//                each), dist^2 estimate, classification, count;
 //   * TF32: operands rounded to TF32 on the device (round to nearest), one
 //     MMA per K step; BF16X3: a = a_hi + a_lo in BF16, a.b =
 //     a_hi.b_hi + a_lo.b_hi + a_hi.b_lo (three MMAs per K step); FP16: the
@@ -40,14 +35,15 @@
 //     branch-free against per-tile bounds, and queue the band pairs.
 //
 // Every mbarrier wait is bounded in time (hj_common.cuh); on a timeout the
-// kernel raises kErrTimeout, drains its outstanding copies and MMAs, frees its
-// tensor memory and returns.
+// kernel raises kErrTimeout (with the number of the wait that gave up in bits
+// 8..15 of the error word), every role stops at its next wait, the copies and
+// MMAs already issued are drained, the tensor memory is freed and the kernel
+// returns. hj_debug_set_wait_gate makes the epilogue's first wait one that
+// nothing ends, so that tests run this path.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
-#include <algorithm>
 #include <cmath>
-#include <map>
 #include <mutex>
 #include <string>
 
@@ -57,34 +53,24 @@
 
 namespace hj {
 
-// The pair tile: a cluster of two CTAs on two SMs computes one 256 x 256 block
-// of dot products with tcgen05.mma.cta_group::2 (M = 256, N = 256). CTA rank r
-// of the pair holds A ranks [256 a + 128 r, +128) and B ranks
-// [256 b + 128 r, +128) in its shared memory, and its tensor memory receives
-// its 128 A rows against all 256 B columns. Against one SM alone (M = 128,
-// N = 256) every SM loads half the B bytes and its tensor core reads half the
-// B operand per instruction, for the same MMA work and the same epilogue.
-constexpr int kHalfRows = 128;  // rows of A and of B per CTA of the pair
-static_assert(kTcTileA == 2 * kHalfRows && kTcTileB == 2 * kHalfRows, "pair tile is 256 x 256");
-
 // Epilogue warps: kEpiWarps / 4 per TMEM lane quadrant, each on kEpiCols of the
-// 256 accumulator columns, in chunks of kChunkCols (one TMEM load each).
+// 256 accumulator columns, in two chunks of kChunkCols (one TMEM load each).
 constexpr int kEpiWarps = 8;
 constexpr int kEpiCols = 4 * kTcTileB / kEpiWarps;
+// 8 warps: two 64-column chunks each; 16 warps: one 64-column chunk each
 constexpr int kChunkCols = 64;
 constexpr int kChunkGroups = kChunkCols / 32;  // 32-column groups per chunk
 constexpr int kEpiChunks = kEpiCols / kChunkCols;
 constexpr int kEpiVec = kEpiCols / 32;  // norms per lane, group minima per warp
 // 16 epilogue warps (4 per quadrant) were measured slower: at 18 warps the
 // register cap is 96 (spills) and the static shared memory no longer fits next
-// to the operand plan.
+// to the 225 KB operand plan.
 static_assert(kEpiWarps == 8, "the shared-memory plan and register budget assume 8 epilogue warps");
 constexpr int kTcThreads = 64 + 32 * kEpiWarps;
-constexpr uint32_t kAtomBytes = 128;                         // bytes of K per row per swizzle atom
-constexpr uint32_t kAStageBytes = kHalfRows * kAtomBytes;    // 16 KB per A atom (this CTA's rows)
-constexpr uint32_t kBStageBytes = kHalfRows * kAtomBytes;    // 16 KB per B atom (this CTA's rows)
+constexpr uint32_t kAtomBytes = 128;                  // bytes of K per row per swizzle atom
+constexpr uint32_t kAStageBytes = kTcTileA * kAtomBytes;  // 16 KB per A atom
+constexpr uint32_t kBStageBytes = kTcTileB * kAtomBytes;  // 32 KB per B atom
 constexpr uint32_t kTmemCols = 512;
-constexpr uint32_t kMaxStages = 16;
 
 struct BandEntry {
     uint32_t ia, jb;  // EGO ranks in A and B
@@ -118,93 +104,19 @@ struct TcArgs {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ uint32_t cluster_rank() {
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-
-// Address of the same shared-memory object in CTA `rank` of the cluster.
-__device__ __forceinline__ uint32_t mapa_shared(uint32_t saddr, uint32_t rank) {
-    uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
-    return r;
-}
-
-// Arrive on an mbarrier anywhere in the cluster (release at cluster scope).
-__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr) {
-    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
-}
-
-// All threads of both CTAs of the pair.
-__device__ __forceinline__ void cluster_sync() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait_acq_cluster(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// mbar_wait for barriers that threads of the peer CTA arrive on: acquire at
-// cluster scope. Bounded like mbar_wait; gives up early once *err is raised.
-__device__ __forceinline__ bool mbar_wait_cluster(uint64_t *bar, uint32_t parity, volatile uint32_t *err) {
-    if (mbar_try_wait_acq_cluster(bar, parity)) return true;
-    const uint64_t t0 = globaltimer_ns();
-    for (uint32_t it = 1;; ++it) {
-        if (mbar_try_wait_acq_cluster(bar, parity)) return true;
-        if ((it & 255u) == 0) {
-            if (*err != 0) return false;
-            if (globaltimer_ns() - t0 > kWaitLimitNs) {
-                atomicOr((uint32_t *)err, kErrTimeout);
-                return false;
-            }
-        }
-    }
-}
-
-// Waits for a phase regardless of the error word, until `deadline`
-// (%globaltimer): the drain of copies and MMAs already issued.
-__device__ __forceinline__ void drain_until(uint64_t *bar, uint32_t parity, uint64_t deadline) {
-    while (!mbar_try_wait(bar, parity)) {
-        if (globaltimer_ns() > deadline) break;
-    }
-}
-
-// Tensor memory of the pair: both CTAs call these from the same warp (warp 0),
-// with the same shared-memory destination.
-__device__ __forceinline__ void tmem_alloc2(uint32_t *dst_smem, uint32_t ncols) {
-    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+__device__ __forceinline__ void tmem_alloc(uint32_t *dst_smem, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
                  "r"(ncols)
                  : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
 }
 
-__device__ __forceinline__ void tmem_dealloc2(uint32_t taddr, uint32_t ncols) {
-    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
 
-// Arrive on the barrier at this offset in both CTAs once the MMAs issued so
-// far by this thread have completed.
-__device__ __forceinline__ void mma_commit_pair(uint64_t *bar) {
-    asm volatile(
-        "{\n\t.reg .b16 m;\n\t"
-        "mov.b16 m, 3;\n\t"
-        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], m;\n\t}" ::"r"(
-            smem_u32(bar))
-        : "memory");
-}
-
-// The same for a barrier of this CTA only.
-__device__ __forceinline__ void mma_commit_local(uint64_t *bar) {
-    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
 }
 
@@ -215,14 +127,14 @@ __device__ __forceinline__ void mma_issue(uint32_t tmem_d, uint64_t adesc, uint6
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "setp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
             "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
             : "memory");
     } else {
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "setp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
             "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
             : "memory");
     }
@@ -266,32 +178,25 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
     return (uint64_t)((saddr & 0x3FFFFu) >> 4) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
 }
 
-// Instruction descriptor: D = F32, A/B K-major, M = 256 (the pair), N = 256.
+// Instruction descriptor: D = F32, A/B K-major, M = 128, N = 256.
 template <int FORM>
 __device__ __forceinline__ constexpr uint32_t instr_desc() {
     constexpr uint32_t ab = FORM == HJ_FORM_TC_TF32 ? 2u : (FORM == HJ_FORM_TC_BF16X3 ? 1u : 0u);  // TF32, BF16, F16
     return (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(kTcTileB >> 3) << 17) | ((uint32_t)(kTcTileA >> 4) << 24);
 }
 
+// Waits for a phase regardless of the error word, until `deadline`
+// (%globaltimer): the drain of copies and MMAs already issued.
+__device__ __forceinline__ void drain_until(uint64_t *bar, uint32_t parity, uint64_t deadline) {
+    while (!mbar_try_wait(bar, parity)) {
+        if (globaltimer_ns() > deadline) break;
+    }
+}
+
 // ---------------------------------------------------------------- the kernel
-//
-// Roles (320 threads per CTA, both CTAs of the pair alike unless stated):
-//   warp 0 lane 0  TMA producer: this CTA's A rows (once per item) and B rows
-//                  (per B tile and K atom) into its own buffers; each copy
-//                  completes on this CTA's own full barrier.
-//   warp 1 lane 0  rank 0: MMA issuer for the pair. It waits on its own full
-//                  barriers and on the peer's relayed arrivals (apeer/bpeer),
-//                  issues tcgen05.mma.cta_group::2 and commits to the empty
-//                  and accumulator barriers of both CTAs (multicast).
-//                  rank 1: relay. It follows the same sequence of copies,
-//                  waits for each of this CTA's copies to land and arrives on
-//                  the leader's apeer/bpeer barrier. Every copy is thus
-//                  observed on the CTA that issued it, so each CTA can drain
-//                  its own copies before it exits, whatever happened.
-//   warps 2-9      epilogue on this CTA's 128 TMEM lanes; each warp releases
-//                  an accumulator by arriving on the leader's accempty.
+
 template <int FORM>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
+__global__ void __launch_bounds__(kTcThreads, 1)
     k_join_tc(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_a2,
               const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ CUtensorMap tm_b2, TcArgs p) {
     // A atoms per buffer: TF32 ka; BF16 2*ka (hi atoms, then lo atoms). B atoms
@@ -302,9 +207,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
     const uint32_t a_buf_bytes = a_atoms * kAStageBytes;
 
     extern __shared__ unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t bar_afull[2], bar_aempty[2], bar_apeer[2];
-    __shared__ __align__(8) uint64_t bar_accfull[2], bar_accempty[2], bar_drain, bar_gate;
-    __shared__ __align__(8) uint64_t bar_bfull[kMaxStages], bar_bempty[kMaxStages], bar_bpeer[kMaxStages];
+    __shared__ __align__(8) uint64_t bar_afull[2], bar_aempty[2], bar_accfull[2], bar_accempty[2], bar_drain, bar_gate;
+    __shared__ __align__(8) uint64_t bar_bfull[8], bar_bempty[8];
     __shared__ uint32_t tmem_base_sh;
     __shared__ __align__(16) float epi_row[kEpiWarps][32];
 
@@ -312,29 +216,25 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
     const uint32_t a_base = smem_base;
     const uint32_t b_base = smem_base + p.a_bufs * a_buf_bytes;
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    const uint32_t rank = cluster_rank();
-    const uint64_t pair = blockIdx.x >> 1, n_pairs = gridDim.x >> 1;
     volatile uint32_t *err = p.err;
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < 2; ++i) {
             mbar_init(&bar_afull[i], 1);
             mbar_init(&bar_aempty[i], 1);
-            mbar_init(&bar_apeer[i], 1);
             mbar_init(&bar_accfull[i], 1);
-            mbar_init(&bar_accempty[i], 2 * kEpiWarps);  // the epilogue warps of both CTAs
+            mbar_init(&bar_accempty[i], kEpiWarps);
         }
         for (uint32_t i = 0; i < p.nst; ++i) {
             mbar_init(&bar_bfull[i], 1);
             mbar_init(&bar_bempty[i], 1);
-            mbar_init(&bar_bpeer[i], 1);
         }
         mbar_init(&bar_drain, 1);
         mbar_init(&bar_gate, 1);
         fence_barrier_init();
     }
     if (warp == 0) {
-        tmem_alloc2(&tmem_base_sh, kTmemCols);
+        tmem_alloc(&tmem_base_sh, kTmemCols);
         if (lane == 0) {
             prefetch_tmap(&tm_a);
             prefetch_tmap(&tm_b);
@@ -344,39 +244,35 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
             }
         }
     }
-    // both CTAs' barriers are initialised and the tensor memory allocated
-    // before any thread of the pair touches the other CTA
     tc_fence_before();
-    cluster_sync();
+    __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_base_sh;
 
     if (warp == 0) {
-        // ------------------------------------------------ TMA producer (both CTAs)
+        // ------------------------------------------------ TMA producer
         if (lane == 0) {
             uint32_t a_cnt = 0, b_cnt = 0;
             bool ok = true;
-            for (uint64_t it = pair; ok && it < p.n_items; it += n_pairs) {
+            for (uint64_t it = blockIdx.x; ok && it < p.n_items; it += gridDim.x) {
                 const WorkItem w = p.items[it];
                 const uint32_t ka = p.jobs[w.pad].ka;  // this job's K atoms (<= p.ka)
                 const uint32_t ja_atoms = kBf ? 2 * ka : ka;
                 const uint32_t abuf = a_cnt % p.a_bufs, au = a_cnt / p.a_bufs;
-                if (au >= 1 && !mbar_wait(&bar_aempty[abuf], (au - 1) & 1u, err)) break;
+                if (au >= 1 && !mbar_wait(&bar_aempty[abuf], (au - 1) & 1u, err, 1)) break;
                 mbar_arrive_expect_tx(&bar_afull[abuf], ja_atoms * kAStageBytes);
                 const uint32_t adst = a_base + abuf * a_buf_bytes;
-                const int32_t arow = (int32_t)(w.a * kTcTileA + rank * kHalfRows);
                 for (uint32_t q = 0; q < ja_atoms; ++q) {
                     const bool lo = kBf && q >= ka;
                     const uint32_t kq = kBf ? (lo ? q - ka : q) : q;
                     tma_load_2d(smem_raw + (adst + q * kAStageBytes - smem_u32(smem_raw)), lo ? &tm_a2 : &tm_a,
-                                (int32_t)(kq * kAtomElems), arow, &bar_afull[abuf]);
+                                (int32_t)(kq * kAtomElems), (int32_t)(w.a * kTcTileA), &bar_afull[abuf]);
                 }
                 ++a_cnt;
                 for (uint32_t bt = w.b0; ok && bt < w.b1; ++bt) {
-                    const int32_t brow = (int32_t)(bt * kTcTileB + rank * kHalfRows);
                     for (uint32_t q = 0; q < ja_atoms; ++q) {
                         const uint32_t s = b_cnt % p.nst, u = b_cnt / p.nst;
-                        if (u >= 1 && !mbar_wait(&bar_bempty[s], (u - 1) & 1u, err)) {
+                        if (u >= 1 && !mbar_wait(&bar_bempty[s], (u - 1) & 1u, err, 2)) {
                             ok = false;
                             break;
                         }
@@ -384,72 +280,43 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
                         const bool lo = kBf && (q & 1u);
                         const uint32_t kq = kBf ? (q >> 1) : q;
                         tma_load_2d(smem_raw + (b_base + s * kBStageBytes - smem_u32(smem_raw)), lo ? &tm_b2 : &tm_b,
-                                    (int32_t)(kq * kAtomElems), brow, &bar_bfull[s]);
+                                    (int32_t)(kq * kAtomElems), (int32_t)(bt * kTcTileB), &bar_bfull[s]);
                         ++b_cnt;
                     }
                 }
             }
-            // Drain: every copy this CTA issued has landed (its own full barrier)
-            // and, on the normal path, has been consumed (the empty barrier the
-            // MMAs' multicast commit arrives on), so no copy and no remote
-            // arrival is still in flight towards this CTA when it exits.
-            const uint64_t deadline = globaltimer_ns() + kWaitLimitNs;
-            for (uint32_t k = 0; k < p.nst && k < b_cnt; ++k) {
-                const uint32_t j = b_cnt - 1 - k;
-                drain_until(&bar_bfull[j % p.nst], (j / p.nst) & 1u, deadline);
-                drain_until(&bar_bempty[j % p.nst], (j / p.nst) & 1u, deadline);
-            }
-            for (uint32_t k = 0; k < p.a_bufs && k < a_cnt; ++k) {
-                const uint32_t j = a_cnt - 1 - k;
-                drain_until(&bar_afull[j % p.a_bufs], (j / p.a_bufs) & 1u, deadline);
-                drain_until(&bar_aempty[j % p.a_bufs], (j / p.a_bufs) & 1u, deadline);
-            }
-        }
-    } else if (warp == 1 && rank == 1) {
-        // ------------------------------------------------ relay (peer CTA)
-        if (lane == 0) {
-            const uint32_t a_peer0 = mapa_shared(smem_u32(&bar_apeer[0]), 0);
-            const uint32_t b_peer0 = mapa_shared(smem_u32(&bar_bpeer[0]), 0);
-            uint32_t a_cnt = 0, b_cnt = 0;
-            bool ok = true;
-            for (uint64_t it = pair; ok && it < p.n_items; it += n_pairs) {
-                const WorkItem w = p.items[it];
-                const uint32_t ka = p.jobs[w.pad].ka;
-                const uint32_t jb_atoms = kBf ? 2 * ka : ka;
-                const uint32_t abuf = a_cnt % p.a_bufs, au = a_cnt / p.a_bufs;
-                if (!mbar_wait(&bar_afull[abuf], au & 1u, err)) break;
-                mbar_arrive_cluster(a_peer0 + abuf * 8u);
-                ++a_cnt;
-                for (uint32_t bt = w.b0; ok && bt < w.b1; ++bt)
-                    for (uint32_t q = 0; q < jb_atoms; ++q) {
-                        const uint32_t s = b_cnt % p.nst;
-                        if (!mbar_wait(&bar_bfull[s], (b_cnt / p.nst) & 1u, err)) {
-                            ok = false;
-                            break;
-                        }
-                        mbar_arrive_cluster(b_peer0 + s * 8u);
-                        ++b_cnt;
-                    }
+            // Drain: on the normal path every copy has been consumed; after an
+            // error (the loops stop at the first failed wait) every copy issued
+            // has landed before the CTA leaves (its full barrier's phase).
+            if (*err) {
+                const uint64_t deadline = globaltimer_ns() + kWaitLimitNs;
+                for (uint32_t k = 0; k < p.nst && k < b_cnt; ++k) {
+                    const uint32_t j = b_cnt - 1 - k;
+                    drain_until(&bar_bfull[j % p.nst], (j / p.nst) & 1u, deadline);
+                }
+                for (uint32_t k = 0; k < p.a_bufs && k < a_cnt; ++k) {
+                    const uint32_t j = a_cnt - 1 - k;
+                    drain_until(&bar_afull[j % p.a_bufs], (j / p.a_bufs) & 1u, deadline);
+                }
             }
         }
     } else if (warp == 1) {
-        // ------------------------------------------------ MMA issuer (leader CTA)
+        // ------------------------------------------------ MMA issuer
         if (lane == 0) {
             constexpr uint32_t idesc = instr_desc<FORM>();
             uint32_t a_cnt = 0, b_cnt = 0, t_cnt = 0;
             bool issued_any = false, ok = true;
-            for (uint64_t it = pair; ok && it < p.n_items; it += n_pairs) {
+            for (uint64_t it = blockIdx.x; ok && it < p.n_items; it += gridDim.x) {
                 const WorkItem w = p.items[it];
                 const uint32_t ka = p.jobs[w.pad].ka;
                 const uint32_t jb_atoms = kBf ? 2 * ka : ka;
                 const uint32_t abuf = a_cnt % p.a_bufs, au = a_cnt / p.a_bufs;
-                if (!mbar_wait(&bar_afull[abuf], au & 1u, err) || !mbar_wait_cluster(&bar_apeer[abuf], au & 1u, err))
-                    break;
+                if (!mbar_wait(&bar_afull[abuf], au & 1u, err, 3)) break;
                 tc_fence_after();
                 const uint32_t abase = a_base + abuf * a_buf_bytes;
                 for (uint32_t bt = w.b0; ok && bt < w.b1; ++bt) {
                     const uint32_t acc = t_cnt & 1u, tu = t_cnt >> 1;
-                    if (tu >= 1 && !mbar_wait_cluster(&bar_accempty[acc], (tu - 1) & 1u, err)) {
+                    if (tu >= 1 && !mbar_wait(&bar_accempty[acc], (tu - 1) & 1u, err, 4)) {
                         ok = false;
                         break;
                     }
@@ -457,8 +324,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
                     const uint32_t dcol = tmem + acc * kTcTileB;
                     uint32_t accumulate = 0;
                     for (uint32_t q = 0; q < jb_atoms; ++q) {
-                        const uint32_t s = b_cnt % p.nst, par = (b_cnt / p.nst) & 1u;
-                        if (!mbar_wait(&bar_bfull[s], par, err) || !mbar_wait_cluster(&bar_bpeer[s], par, err)) {
+                        const uint32_t s = b_cnt % p.nst;
+                        if (!mbar_wait(&bar_bfull[s], (b_cnt / p.nst) & 1u, err, 5)) {
                             ok = false;
                             break;
                         }
@@ -492,29 +359,28 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
                                                     idesc, 1);
                             }
                         }
-                        mma_commit_pair(&bar_bempty[s]);  // stage free in both CTAs once these MMAs have read it
+                        mma_commit(&bar_bempty[s]);  // stage free once these MMAs have read it
                         ++b_cnt;
                         issued_any = true;
                     }
                     if (!ok) break;
-                    mma_commit_pair(&bar_accfull[acc]);
+                    mma_commit(&bar_accfull[acc]);
                     ++t_cnt;
                 }
-                mma_commit_pair(&bar_aempty[abuf]);
+                mma_commit(&bar_aempty[abuf]);
                 ++a_cnt;
             }
             // all MMAs complete before the tensor memory is released
             if (issued_any) {
-                mma_commit_local(&bar_drain);
+                mma_commit(&bar_drain);
                 drain_until(&bar_drain, 0, globaltimer_ns() + kWaitLimitNs);
             }
         }
     } else {
-        // ------------------------------------------------ epilogue (both CTAs)
+        // ------------------------------------------------ epilogue
         const uint32_t quad = warp & 3u;
         const uint32_t half = (warp - 2) >> 2;  // columns [kEpiCols half, kEpiCols (half + 1))
         const uint32_t lane_base = (quad * 32u) << 16;
-        const uint32_t accempty0 = mapa_shared(smem_u32(&bar_accempty[0]), 0);
         float *srow = epi_row[warp - 2];
         unsigned long long cnt = 0;
         uint32_t t_cnt = 0;
@@ -523,7 +389,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
             const uint64_t t0 = globaltimer_ns();
             while (!mbar_try_wait(&bar_gate, 0)) {
                 if (globaltimer_ns() - t0 > p.gate_ns) {
-                    atomicOr((uint32_t *)err, kErrTimeout);
+                    atomicOr((uint32_t *)err, kErrTimeout | (9u << 8));
                     break;
                 }
             }
@@ -539,8 +405,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
         // exact). Per tile only the group minima are needed on the fast path;
         // they are loaded one tile ahead so that their latency overlaps the
         // current tile. B norms and column bounds are read on the slow path.
-        const uint64_t stride = n_pairs;
-        uint64_t it = run ? pair : p.n_items;
+        const uint64_t stride = gridDim.x;
+        uint64_t it = run ? blockIdx.x : p.n_items;
         WorkItem w = it < p.n_items ? p.items[it] : WorkItem{0, 0, 0, 0};
         WorkItem wn = it + stride < p.n_items ? p.items[it + stride] : WorkItem{0, 0, 0, 0};
         uint32_t bt = w.b0;
@@ -573,7 +439,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
             b_end = J.b_end;
             self = J.self != 0;
             s_unscale = J.s_unscale;
-            gi = (uint64_t)ww.a * kTcTileA + rank * kHalfRows + quad * 32 + lane;
+            gi = (uint64_t)ww.a * kTcTileA + quad * 32 + lane;
             row_ok = gi >= J.a_row0 && gi < J.a_end;
             na = row_ok ? __ldg(p.norm_a + gi) : kPadNorm;
             float tmaxb = 0.f;
@@ -612,7 +478,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
             {
                 const uint32_t acc = t_cnt & 1u;
                 const uint64_t gj0 = (uint64_t)cur_bt * kTcTileB + half * kEpiCols;
-                if (!mbar_wait(&bar_accfull[acc], (t_cnt >> 1) & 1u, err)) break;
+                if (!mbar_wait(&bar_accfull[acc], (t_cnt >> 1) & 1u, err, 6)) break;
                 tc_fence_after();
 #pragma unroll
                 for (uint32_t c = 0; c < kEpiChunks; ++c) {
@@ -625,7 +491,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
                         // chunk is classified
                         tc_fence_before();
                         __syncwarp();
-                        if (lane == 0) mbar_arrive_cluster(accempty0 + acc * 8u);
+                        if (lane == 0) mbar_arrive(&bar_accempty[acc]);
                     }
                     // max_j v_j per 32-column group: with the group's minimum norm,
                     // min_j (|b_j|^2 - 2 v_j) >= gmin - 2 max_j v_j
@@ -709,17 +575,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kTcThreads, 1)
         }
         if (job != 0xffffffffu) flush();
     }
-    // Both CTAs are done with each other's barriers and with the tensor
-    // memory (the MMAs have completed, both epilogues have read it) before the
-    // pair frees it; neither CTA exits while the other may still reach it.
     tc_fence_before();
     __syncthreads();
-    cluster_sync();
     tc_fence_after();
-    if (warp == 0) tmem_dealloc2(tmem, kTmemCols);
+    if (warp == 0) tmem_dealloc(tmem, kTmemCols);
+
 }
-
-
 
 // ---------------------------------------------------------------- recheck
 
@@ -869,37 +730,13 @@ static TcLayout tc_layout(int form, uint32_t d) {
     L.a_bufs = 2 * a_bytes + 3 * kBStageBytes <= budget ? 2 : 1;
     size_t left = budget - L.a_bufs * a_bytes;
     L.nst = (uint32_t)(left / kBStageBytes);
-    if (L.nst > kMaxStages) L.nst = kMaxStages;
+    if (L.nst > 8) L.nst = 8;
     L.smem = L.a_bufs * a_bytes + (size_t)L.nst * kBStageBytes + 1024;  // <= 225 KB
     return L;
 }
 
 static float *g_dbg_out = nullptr;  // set by tests through hj_debug_tc_estimates
 static uint64_t g_gate_ns = 0;      // set by tests through hj_debug_set_wait_gate
-
-// CTA pairs that fit on the device at once (one pair per two SMs of a GPC),
-// cached per device and kernel.
-static int max_pairs(const void *kernel, size_t smem, int num_sms) {
-    static std::mutex mu;
-    static std::map<std::pair<const void *, int>, int> cache;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    std::lock_guard<std::mutex> lk(mu);
-    auto key = std::make_pair(kernel, dev);
-    auto f = cache.find(key);
-    if (f != cache.end()) return f->second;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(2 * (unsigned)std::max(1, num_sms / 2), 1, 1);
-    cfg.blockDim = dim3(kTcThreads, 1, 1);
-    cfg.dynamicSmemBytes = smem;
-    int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, kernel, &cfg) != cudaSuccess || n <= 0) {
-        cudaGetLastError();
-        n = std::max(1, num_sms / 2);
-    }
-    cache[key] = n;
-    return n;
-}
 
 void fill_tc_job(TcJob *j, int form, uint32_t d, double T, double op_scale, double maxabs, uint64_t a_row0,
                  uint64_t na_eff, uint64_t b_row0, uint64_t nb_eff, bool self, unsigned long long *count,
@@ -942,21 +779,21 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
     }
     CUtensorMap ma, ma2, mb, mb2;
     if (form == HJ_FORM_TC_TF32) {
-        if (!make_map(&ma, A.tf32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, A.npad_tc, A.kpad_tf32, kHalfRows, err)) return 1;
-        if (!make_map(&mb, B.tf32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, B.npad_tc, B.kpad_tf32, kHalfRows, err)) return 1;
+        if (!make_map(&ma, A.tf32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, A.npad_tc, A.kpad_tf32, kTcTileA, err)) return 1;
+        if (!make_map(&mb, B.tf32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, B.npad_tc, B.kpad_tf32, kTcTileB, err)) return 1;
         ma2 = ma;
         mb2 = mb;
     } else if (form == HJ_FORM_TC_FP16) {
-        if (!make_map(&ma, A.bf_hi, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, A.npad_tc, A.kpad_bf16, kHalfRows, err)) return 1;
-        if (!make_map(&mb, B.bf_hi, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, B.npad_tc, B.kpad_bf16, kHalfRows, err)) return 1;
+        if (!make_map(&ma, A.bf_hi, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, A.npad_tc, A.kpad_bf16, kTcTileA, err)) return 1;
+        if (!make_map(&mb, B.bf_hi, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, B.npad_tc, B.kpad_bf16, kTcTileB, err)) return 1;
         ma2 = ma;
         mb2 = mb;
     } else {
         const CUtensorMapDataType t = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
-        if (!make_map(&ma, A.bf_hi, t, A.npad_tc, A.kpad_bf16, kHalfRows, err)) return 1;
-        if (!make_map(&ma2, A.bf_lo, t, A.npad_tc, A.kpad_bf16, kHalfRows, err)) return 1;
-        if (!make_map(&mb, B.bf_hi, t, B.npad_tc, B.kpad_bf16, kHalfRows, err)) return 1;
-        if (!make_map(&mb2, B.bf_lo, t, B.npad_tc, B.kpad_bf16, kHalfRows, err)) return 1;
+        if (!make_map(&ma, A.bf_hi, t, A.npad_tc, A.kpad_bf16, kTcTileA, err)) return 1;
+        if (!make_map(&ma2, A.bf_lo, t, A.npad_tc, A.kpad_bf16, kTcTileA, err)) return 1;
+        if (!make_map(&mb, B.bf_hi, t, B.npad_tc, B.kpad_bf16, kTcTileB, err)) return 1;
+        if (!make_map(&mb2, B.bf_lo, t, B.npad_tc, B.kpad_bf16, kTcTileB, err)) return 1;
     }
     TcArgs a;
     memset(&a, 0, sizeof(a));
@@ -980,20 +817,18 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
     a.perm_a = A.perm;
     a.perm_b = B.perm;
     a.gate_ns = g_gate_ns;
-    const void *kern = form == HJ_FORM_TC_TF32   ? (const void *)k_join_tc<HJ_FORM_TC_TF32>
-                       : form == HJ_FORM_TC_FP16 ? (const void *)k_join_tc<HJ_FORM_TC_FP16>
-                                                 : (const void *)k_join_tc<HJ_FORM_TC_BF16X3>;
-    ensure_max_dynamic_smem(kern, 225 * 1024);
-    // one persistent CTA pair per two SMs (as many as fit at once), never more than items
-    uint64_t pairs = (uint64_t)max_pairs(kern, L.smem, num_sms);
-    if (pairs > idx.n_items) pairs = idx.n_items;
-    const unsigned grid = (unsigned)(2 * pairs);
-    if (form == HJ_FORM_TC_TF32)
-        k_join_tc<HJ_FORM_TC_TF32><<<grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
-    else if (form == HJ_FORM_TC_FP16)
-        k_join_tc<HJ_FORM_TC_FP16><<<grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
-    else
-        k_join_tc<HJ_FORM_TC_BF16X3><<<grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
+    uint64_t grid = (uint64_t)num_sms;
+    if (grid > idx.n_items) grid = idx.n_items;
+    if (form == HJ_FORM_TC_TF32) {
+        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_TF32>, 225 * 1024);
+        k_join_tc<HJ_FORM_TC_TF32><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
+    } else if (form == HJ_FORM_TC_FP16) {
+        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_FP16>, 225 * 1024);
+        k_join_tc<HJ_FORM_TC_FP16><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
+    } else {
+        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_BF16X3>, 225 * 1024);
+        k_join_tc<HJ_FORM_TC_BF16X3><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         *err = std::string("tensor-core kernel launch: ") + cudaGetErrorString(e);
