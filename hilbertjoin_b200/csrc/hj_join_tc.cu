@@ -498,15 +498,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     float mg[kChunkGroups];
 #pragma unroll
                     for (int g = 0; g < kChunkGroups; ++g) {
-                        float mx[4];
+                        // 16 three-input maxima in a tree of depth 4 (10 + 4 + 1, then one
+                        // two-input max) for the group's 32 values
+                        const float *vg = v + 32 * g;
+                        float t[10];
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) mx[q] = fmaxf(v[32 * g + q], v[32 * g + q + 4]);
-#pragma unroll
-                        for (int j = 8; j < 32; j += 8)
-#pragma unroll
-                            for (int q = 0; q < 4; ++q) mx[q] = fmax3(mx[q], v[32 * g + j + q], v[32 * g + j + q + 4]);
-                        mg[g] = fmaf(-2.0f, fmaxf(fmaxf(mx[0], mx[1]), fmaxf(mx[2], mx[3])),
-                                     gmin[c * kChunkGroups + g]);
+                        for (int i = 0; i < 10; ++i) t[i] = fmax3(vg[3 * i], vg[3 * i + 1], vg[3 * i + 2]);
+                        const float u0 = fmax3(t[0], t[1], t[2]), u1 = fmax3(t[3], t[4], t[5]);
+                        const float u2 = fmax3(t[6], t[7], t[8]), u3 = fmax3(t[9], vg[30], vg[31]);
+                        mg[g] = fmaf(-2.0f, fmaxf(fmax3(u0, u1, u2), u3), gmin[c * kChunkGroups + g]);
                     }
 #pragma unroll
                     for (int h2 = 0; h2 < kChunkGroups; ++h2) {

@@ -67,41 +67,69 @@ __global__ void __launch_bounds__(256) k_dim_stats(const T *__restrict__ x, uint
     __syncthreads();
     const uint64_t threads = (uint64_t)gridDim.x * blockDim.x;
     const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned long long xmin[V], xmax[V];
+    // running minima and maxima in the input type (non-finite values skipped),
+    // turned into the order-preserving encoding once at the end; four loads
+    // in flight per thread (the steps k*V + i*threads*V, i = 0..3, hit the same
+    // dims because threads * V is a multiple of d)
+    T xmin[V], xmax[V];
 #pragma unroll
-    for (int j = 0; j < V; ++j) xmin[j] = ~0ull, xmax[j] = 0ull;
-    double amax = 0.0;
+    for (int j = 0; j < V; ++j) xmin[j] = T(INFINITY), xmax[j] = T(-INFINITY);
+    T amax = T(0);
     uint32_t lbad = 0;
     using Vec = typename std::conditional<V == 4, float4, typename std::conditional<V == 2, double2, T>::type>::type;
-    for (uint64_t e = k * V; e < total; e += threads * V) {
+    auto take = [&](const T (&v)[V]) {
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+            const T w = v[j];
+            if (isfinite(w)) {
+                amax = fmax(amax, fabs(w));
+                xmin[j] = fmin(xmin[j], w);
+                xmax[j] = fmax(xmax[j], w);
+            } else {
+                lbad |= 1u;
+            }
+        }
+    };
+    const uint64_t stride = threads * V;
+    uint64_t e = k * V;
+    for (; e + 3 * stride + V <= total; e += 4 * stride) {
+        Vec q[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) q[i] = __ldg(reinterpret_cast<const Vec *>(x + e + i * stride));
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            T v[V];
+            memcpy(v, &q[i], sizeof(v));
+            take(v);
+        }
+    }
+    for (; e < total; e += stride) {
         T v[V];
         if (e + V <= total) {
             const Vec q = __ldg(reinterpret_cast<const Vec *>(x + e));
             memcpy(v, &q, sizeof(v));
+            take(v);
         } else {
 #pragma unroll
-            for (int j = 0; j < V; ++j) v[j] = e + j < total ? x[e + j] : T(0);
-        }
-#pragma unroll
-        for (int j = 0; j < V; ++j) {
-            if (e + j >= total) continue;
-            const double w = (double)v[j];
-            if (!isfinite(w)) {
-                lbad |= 1u;
-                continue;
+            for (int j = 0; j < V; ++j) {
+                if (e + j >= total) continue;
+                const T w = x[e + j];
+                if (isfinite(w)) {
+                    amax = fmax(amax, fabs(w));
+                    xmin[j] = fmin(xmin[j], w);
+                    xmax[j] = fmax(xmax[j], w);
+                } else {
+                    lbad |= 1u;
+                }
             }
-            amax = fmax(amax, fabs(w));
-            const unsigned long long o = ordered_from_double(w);
-            xmin[j] = min(xmin[j], o);
-            xmax[j] = max(xmax[j], o);
         }
     }
 #pragma unroll
     for (int j = 0; j < V; ++j) {
-        if (xmin[j] == ~0ull) continue;
+        if (!(xmin[j] <= xmax[j])) continue;  // no finite value in these dims
         const uint32_t t = (uint32_t)((k * V + j) % d);
-        atomicMin(&sxmin[t], xmin[j]);
-        atomicMax(&sxmax[t], xmax[j]);
+        atomicMin(&sxmin[t], ordered_from_double((double)xmin[j]));
+        atomicMax(&sxmax[t], ordered_from_double((double)xmax[j]));
     }
     __syncthreads();
     for (uint32_t u = threadIdx.x; u < d; u += blockDim.x) {
@@ -111,7 +139,7 @@ __global__ void __launch_bounds__(256) k_dim_stats(const T *__restrict__ x, uint
         }
     }
     // non-negative doubles order like their bit patterns
-    if (amax > 0.0) atomicMax(maxabs_bits, (unsigned long long)__double_as_longlong(amax));
+    if (amax > T(0)) atomicMax(maxabs_bits, (unsigned long long)__double_as_longlong((double)amax));
     if (lbad) atomicOr(bad, lbad);
 }
 
@@ -179,6 +207,22 @@ void launch_dim_stats(const void *x, int dtype_bytes, uint64_t n, uint32_t d, do
 }
 
 // ------------------------------------------------------------ key packing
+
+// floor(x / eps) with x / eps the IEEE (correctly rounded) FP64 quotient --
+// the cell of the pair test's convention -- without a division in the common
+// case. With inv = fl(1 / eps), q = fl(x * inv) differs from x / eps by at
+// most |x / eps| (2u + u^2) and from fl(x / eps) by at most 3.01 u |q|
+// (u = 2^-53), so every value within 2^-50 |q| of q has the same floor as
+// fl(x / eps) whenever q - 2^-50 |q| and q + 2^-50 |q| do (the margin also
+// covers the rounding of those two bounds). Only near a cell border, where
+// they differ, is the quotient computed by division.
+__device__ __forceinline__ double cell_of(double x, double eps, double inv) {
+    const double q = x * inv;
+    const double m = fabs(q) * 8.881784197001252e-16;  // 2^-50
+    const double lo = floor(q - m);
+    if (lo == floor(q + m)) return lo;
+    return floor(x / eps);
+}
 
 // One thread per point: digit of every dim, OR-ed into the running key word
 // (fields in key order, so words never decrease). Consecutive threads read
@@ -309,7 +353,7 @@ constexpr uint32_t kPkMaxRowBytes = 512;
 
 template <typename T>
 __global__ void __launch_bounds__(kPkRows) k_pack_keys_staged(const T *__restrict__ x, uint64_t n, uint32_t d,
-                                                              double eps, GridDev g, uint32_t W,
+                                                              double eps, double inv_eps, GridDev g, uint32_t W,
                                                               uint32_t *__restrict__ keys_wm,
                                                               const double *__restrict__ center, double nscale,
                                                               uint32_t *__restrict__ norm_key, bool vec) {
@@ -358,7 +402,7 @@ __global__ void __launch_bounds__(kPkRows) k_pack_keys_staged(const T *__restric
             cur_word = w;
             acc = 0;
         }
-        const double c = floor((double)cols[dim * kPkRows + t] / eps);
+        const double c = cell_of((double)cols[dim * kPkRows + t], eps, inv_eps);
         const long long dig = (long long)c - g.off[dim];
         acc |= (uint32_t)dig << g.shift[dim];
     }
@@ -385,11 +429,13 @@ void launch_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t d, do
         const size_t smem = (size_t)kPkRows * d * dtype_bytes;  // <= 64 KB
         if (dtype_bytes == 8) {
             ensure_max_dynamic_smem((const void *)k_pack_keys_staged<double>, 64 * 1024);
-            k_pack_keys_staged<double><<<blocks, kPkRows, smem, st>>>(static_cast<const double *>(x), n, d, eps, g,
+            k_pack_keys_staged<double><<<blocks, kPkRows, smem, st>>>(static_cast<const double *>(x), n, d, eps,
+                                                                      1.0 / eps, g,
                                                                       W, keys_wm, center, norm_scale, norm_key, vec);
         } else {
             ensure_max_dynamic_smem((const void *)k_pack_keys_staged<float>, 64 * 1024);
-            k_pack_keys_staged<float><<<blocks, kPkRows, smem, st>>>(static_cast<const float *>(x), n, d, eps, g, W,
+            k_pack_keys_staged<float><<<blocks, kPkRows, smem, st>>>(static_cast<const float *>(x), n, d, eps,
+                                                                     1.0 / eps, g, W,
                                                                      keys_wm, center, norm_scale, norm_key, vec);
         }
         return;
@@ -428,7 +474,7 @@ __global__ void __launch_bounds__(1024) k_scan_u32(uint32_t *a, uint64_t count, 
 // Every pass moves (key, index) pairs: the index (the permutation) and the
 // current key word in the current order, so that a pass reads both with
 // coalesced 128-bit loads. Per pass:
-//   k_rs_count      per 4096-item tile, the 256 digit counts;
+//   k_rs_count      per 2048-item tile, the 256 digit counts;
 //   k_rs_scan_rows  one block per digit: exclusive scan of that digit's tile
 //                   counts, and the digit's total;
 //   k_rs_scatter    per tile, a stable local sort by digit in shared memory
@@ -440,10 +486,10 @@ __global__ void __launch_bounds__(1024) k_scan_u32(uint32_t *a, uint64_t count, 
 // (4-byte reads from an array that stays in L2 at the engine's sizes).
 
 constexpr int kRsThreads = 256;
-constexpr int kRsIpt = 16;                      // items per thread
-constexpr int kRsTile = kRsThreads * kRsIpt;    // 4096 items per tile
+constexpr int kRsIpt = 8;                       // items per thread
+constexpr int kRsTile = kRsThreads * kRsIpt;    // 2048 items per tile
 constexpr int kRsWarps = kRsThreads / 32;
-constexpr int kRsWarpItems = kRsTile / kRsWarps;  // 512 consecutive items per warp
+constexpr int kRsWarpItems = kRsTile / kRsWarps;  // 256 consecutive items per warp
 
 static uint64_t rs_round4(uint64_t n) { return hj_ceil_div(n, 4) * 4; }
 
@@ -452,7 +498,7 @@ size_t radix_scratch_bytes(uint64_t n) {
     return (3 * rs_round4(n) + 256 * hj_ceil_div(std::max<uint64_t>(n, 1), kRsTile) + 256) * 4;
 }
 
-// Tile items [base, base + 4096) of a u32 array into s[0 .. 4096): 128-bit
+// Tile items [base, base + kRsTile) of a u32 array into s[0 .. kRsTile): 128-bit
 // loads when the array is 16-byte aligned, 32-bit loads otherwise; items past
 // n are not loaded.
 __device__ __forceinline__ void rs_load_tile(const uint32_t *__restrict__ a, uint64_t base, uint64_t n, bool vec,
@@ -572,7 +618,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint32_t *__res
 #pragma unroll
     for (int w = 0; w < kRsWarps; ++w) s_cnt[w][t] = 0;
     __syncthreads();
-    // 1. ranks within each warp's 512 items, in item order (stable): warp-local
+    // 1. ranks within each warp's kRsWarpItems items, in item order (stable): warp-local
     //    rank of item j of this lane, 0xffff for items past the tile's end
     const uint32_t lt = (1u << lane) - 1u;
     uint32_t r_reg[kRsIpt / 2];
@@ -586,7 +632,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint32_t *__res
         __syncwarp();
         if (dg < 256u && (peers & lt) == 0) s_cnt[warp][dg] = before + __popc(peers);
         __syncwarp();
-        const uint32_t r = ok ? before + __popc(peers & lt) : 0xffffu;  // < 512 for real items
+        const uint32_t r = ok ? before + __popc(peers & lt) : 0xffffu;  // < kRsWarpItems for real items
         if (j & 1)
             r_reg[j >> 1] |= r << 16;
         else
