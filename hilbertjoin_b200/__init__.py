@@ -24,6 +24,9 @@ LIB_PATH = os.path.join(HERE, "lib", "libhj.so")
 
 FORMS = {"plain": 0, "fp64": 0, "tf32": 1, "bf16x3": 2, "auto": 3, "fp16": 4}
 FORM_NAMES = {0: "plain_fp64", 1: "tc_tf32", 2: "tc_bf16x3", 3: "auto", 4: "tc_fp16"}
+# operand centring of the FP16 tensor-core form (hj_centring)
+CENTRINGS = {"auto": 0, "global": 1, "block": 2}
+CENTRING_NAMES = {0: "none", 1: "global", 2: "block"}
 
 OK = 0
 STATUS = {0: "ok", 1: "invalid argument", 2: "out of device memory", 3: "CUDA error", 4: "device wait timed out",
@@ -42,7 +45,7 @@ class Opts(ctypes.Structure):
     _fields_ = [("form", ctypes.c_int32), ("active_dims", ctypes.c_int32), ("ref_compat", ctypes.c_int32),
                 ("device", ctypes.c_int32), ("stream", ctypes.c_void_p), ("shard_index", ctypes.c_int32),
                 ("shard_count", ctypes.c_int32), ("reorder_dims", ctypes.c_int32), ("item_chunk", ctypes.c_int32),
-                ("reserved", ctypes.c_uint64 * 2)]
+                ("tc_centring", ctypes.c_int32), ("reserved_i", ctypes.c_int32), ("reserved", ctypes.c_uint64 * 1)]
 
 
 class Stats(ctypes.Structure):
@@ -54,11 +57,12 @@ class Stats(ctypes.Structure):
                 ("band_fraction", ctypes.c_double), ("band_halfwidth_rel", ctypes.c_double),
                 ("max_abs_err_band", ctypes.c_double), ("fp64_items", ctypes.c_uint64),
                 ("form_used", ctypes.c_int32), ("stripes", ctypes.c_int32), ("kernel_launches", ctypes.c_int32),
-                ("reserved_i", ctypes.c_int32), ("reorder_ms", ctypes.c_double), ("reserved", ctypes.c_uint64 * 3)]
+                ("tc_centring", ctypes.c_int32), ("reorder_ms", ctypes.c_double), ("reserved", ctypes.c_uint64 * 3)]
 
     def to_dict(self) -> dict:
         d = {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("reserved")}
         d["form_used"] = FORM_NAMES.get(d["form_used"], d["form_used"])
+        d["tc_centring"] = CENTRING_NAMES.get(d["tc_centring"], d["tc_centring"])
         return d
 
 
@@ -104,6 +108,7 @@ def lib() -> ctypes.CDLL:
         "hj_self_join_count_device": (I, [P, I, U64, U32, D, pO, pU64, pS]),
         "hj_join_count_device": (I, [P, U64, P, U64, I, U32, D, pO, pU64, pS]),
         "hj_debug_tc_estimates": (I, [P, U64, P, U64, U32, I, P]),
+        "hj_debug_tc_estimates_ex": (I, [P, U64, P, U64, U32, I, I, D, P, pS]),
         "hj_ego_sort": (I, [P, U64, U32, D, pO, P, P]),
         "hj_device_sm_count": (I, [I]),
         "hj_test_ego_loop3_macro": (None, [ctypes.c_size_t, ctypes.c_size_t, D, P, ctypes.POINTER(ctypes.c_size_t),
@@ -129,7 +134,8 @@ def _check(status: int) -> None:
         raise HJError(status, lib().hj_last_error().decode())
 
 
-def _opts(form, active_dims, ref_compat, device, stream, shard=None, reorder_dims=False, item_chunk=None) -> Opts:
+def _opts(form, active_dims, ref_compat, device, stream, shard=None, reorder_dims=False, item_chunk=None,
+          centring="auto") -> Opts:
     o = Opts()
     lib().hj_opts_init(ctypes.byref(o))
     o.form = FORMS[form] if isinstance(form, str) else int(form)
@@ -141,6 +147,7 @@ def _opts(form, active_dims, ref_compat, device, stream, shard=None, reorder_dim
         o.shard_index, o.shard_count = int(shard[0]), int(shard[1])
     o.reorder_dims = int(bool(reorder_dims))
     o.item_chunk = int(item_chunk or 0)
+    o.tc_centring = CENTRINGS[centring] if isinstance(centring, str) else int(centring)
     return o
 
 
@@ -166,7 +173,7 @@ def _torch_stream(x, stream):
 
 
 def self_join_count(points, eps: float, form="plain", active_dims=None, ref_compat=False, device=None,
-                    stream=None, return_stats=False, shard=None, reorder_dims=False, item_chunk=None):
+                    stream=None, return_stats=False, shard=None, reorder_dims=False, item_chunk=None, centring="auto"):
     """Number of unordered pairs {a, b}, a != b, of `points` with |a-b| <= eps.
 
     `points`: (n, d) float32/float64 numpy array (copied to the device inside
@@ -178,13 +185,13 @@ def self_join_count(points, eps: float, form="plain", active_dims=None, ref_comp
             raise ValueError("points must be a 2-D float32/float64 tensor")
         x = points.contiguous()
         opts = _opts(form, active_dims, ref_compat, x.device.index if device is None else device,
-                     _torch_stream(x, stream), shard, reorder_dims, item_chunk)
+                     _torch_stream(x, stream), shard, reorder_dims, item_chunk, centring)
         _check(lib().hj_self_join_count_device(ctypes.c_void_p(x.data_ptr()), x.element_size(), x.shape[0],
                                                x.shape[1], float(eps), ctypes.byref(opts), ctypes.byref(c),
                                                ctypes.byref(o)))
     else:
         x = _host_array(points)
-        opts = _opts(form, active_dims, ref_compat, device, stream, shard, reorder_dims, item_chunk)
+        opts = _opts(form, active_dims, ref_compat, device, stream, shard, reorder_dims, item_chunk, centring)
         fn = lib().hj_self_join_count if x.dtype == np.float64 else lib().hj_self_join_count_f32
         _check(fn(x.ctypes.data_as(ctypes.c_void_p), x.shape[0], x.shape[1], float(eps), ctypes.byref(opts),
                   ctypes.byref(c), ctypes.byref(o)))
@@ -192,7 +199,7 @@ def self_join_count(points, eps: float, form="plain", active_dims=None, ref_comp
 
 
 def join_count(a, b, eps: float, form="plain", active_dims=None, ref_compat=False, device=None, stream=None,
-               return_stats=False, shard=None, reorder_dims=False, item_chunk=None):
+               return_stats=False, shard=None, reorder_dims=False, item_chunk=None, centring="auto"):
     """Number of ordered pairs (p in a, q in b) with |p-q| <= eps."""
     o = Stats()
     c = ctypes.c_uint64(0)
@@ -201,7 +208,7 @@ def join_count(a, b, eps: float, form="plain", active_dims=None, ref_compat=Fals
         if xa.dtype != xb.dtype or xa.shape[1] != xb.shape[1]:
             raise ValueError("a and b must have the same dtype and dimension")
         opts = _opts(form, active_dims, ref_compat, xa.device.index if device is None else device,
-                     _torch_stream(xa, stream), shard, reorder_dims, item_chunk)
+                     _torch_stream(xa, stream), shard, reorder_dims, item_chunk, centring)
         _check(lib().hj_join_count_device(ctypes.c_void_p(xa.data_ptr()), xa.shape[0], ctypes.c_void_p(xb.data_ptr()),
                                           xb.shape[0], xa.element_size(), xa.shape[1], float(eps),
                                           ctypes.byref(opts), ctypes.byref(c), ctypes.byref(o)))
@@ -211,7 +218,7 @@ def join_count(a, b, eps: float, form="plain", active_dims=None, ref_compat=Fals
             xb = xb.astype(xa.dtype)
         if xa.shape[1] != xb.shape[1]:
             raise ValueError("a and b must have the same dimension")
-        opts = _opts(form, active_dims, ref_compat, device, stream, shard, reorder_dims, item_chunk)
+        opts = _opts(form, active_dims, ref_compat, device, stream, shard, reorder_dims, item_chunk, centring)
         fn = lib().hj_join_count if xa.dtype == np.float64 else lib().hj_join_count_f32
         _check(fn(xa.ctypes.data_as(ctypes.c_void_p), xa.shape[0], xb.ctypes.data_as(ctypes.c_void_p), xb.shape[0],
                   xa.shape[1], float(eps), ctypes.byref(opts), ctypes.byref(c), ctypes.byref(o)))
@@ -297,15 +304,27 @@ def ego_sort(points, eps: float, device=None):
     return perm, srt
 
 
-def tc_estimates(a, b, form="tf32") -> np.ndarray:
-    """Testing hook: the tensor-core dist^2 estimate of every pair (FP32 inputs)."""
+def tc_estimates(a, b, form="tf32", centring=None, eps=None, return_stats=False):
+    """Testing hook: the tensor-core dist^2 estimate of every pair (FP32 inputs).
+
+    Without `centring` and `eps`: one global centre and an eps that puts every
+    point in one cell (every pair estimated). With them: that operand centring
+    ("global" / "block") and that eps; pairs outside the work list are NaN."""
     xa = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
     xb = np.ascontiguousarray(np.asarray(b, dtype=np.float32))
     out = np.zeros((xa.shape[0], xb.shape[0]), dtype=np.float32)
-    _check(lib().hj_debug_tc_estimates(xa.ctypes.data_as(ctypes.c_void_p), xa.shape[0],
-                                       xb.ctypes.data_as(ctypes.c_void_p), xb.shape[0], xa.shape[1],
-                                       FORMS[form], out.ctypes.data_as(ctypes.c_void_p)))
-    return out
+    if centring is None and eps is None and not return_stats:
+        _check(lib().hj_debug_tc_estimates(xa.ctypes.data_as(ctypes.c_void_p), xa.shape[0],
+                                           xb.ctypes.data_as(ctypes.c_void_p), xb.shape[0], xa.shape[1],
+                                           FORMS[form], out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+    st = Stats()
+    c = CENTRINGS[centring or "global"]
+    _check(lib().hj_debug_tc_estimates_ex(xa.ctypes.data_as(ctypes.c_void_p), xa.shape[0],
+                                          xb.ctypes.data_as(ctypes.c_void_p), xb.shape[0], xa.shape[1],
+                                          FORMS[form], c, float(eps or 0.0), out.ctypes.data_as(ctypes.c_void_p),
+                                          ctypes.byref(st)))
+    return (out, st.to_dict()) if return_stats else out
 
 
 def test_ego_loop3_macro(array, eps: float, stripes: int = 14):

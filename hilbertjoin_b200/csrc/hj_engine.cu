@@ -139,7 +139,8 @@ enum {
     kSlotTf32A, kSlotTf32B, kSlotHiA, kSlotLoA, kSlotHiB, kSlotLoB, kSlotNormA, kSlotNormB,
     kSlotTmaxAA, kSlotTmaxAB, kSlotTmaxBA, kSlotTmaxBB, kSlotBand, kSlotCenter, kSlotGminA, kSlotGminB,
     kSlotItemCnt, kSlotPairKeys, kSlotPairPerm, kSlotPairTmp, kSlotPairHist, kSlotPairOut, kSlotDimCost,
-    kSlotGridOrd,
+    kSlotGridOrd, kSlotBcOpA, kSlotBcOpB, kSlotBcNormA, kSlotBcNormB, kSlotBcXnA, kSlotBcXnB, kSlotBcGminA,
+    kSlotBcGminB, kSlotBcBlkA, kSlotBcBlkB, kSlotBcCentA, kSlotBcCentB,
     kSlotEngineEnd
 };
 static_assert(kSlotEngineEnd <= kSlotIndexFirst, "engine slots overlap the index stage's");
@@ -318,6 +319,30 @@ static int ensure_plain_tiles(Ctx *c, cudaStream_t st, SortedSet *s, bool is_b, 
     return check_cuda("plain layout");
 }
 
+// Per-block-centred FP16 operands of a sorted set (HJ_CENTRING_BLOCK): the A
+// layout for a join's set A, the B layout for its set B, both for a self-join
+// (is_b false, with_b true); p and |h| per rank, group minima of p (B side),
+// block summaries and centres.
+static int prepare_block_centring(Ctx *c, cudaStream_t st, SortedSet *s, bool with_a, bool with_b, bool is_b,
+                                  const double *center, double op_scale, int *launches) {
+    const uint64_t npad = s->npad_tc, nblk = npad / kBcBlock;
+    s->kpad_bc = tc_atoms(HJ_FORM_TC_FP16, 3 * s->d) * 64;
+    s->bc_op_a = with_a ? (uint16_t *)slot_alloc_impl(c, st, kSlotBcOpA, npad * s->kpad_bc * 2) : nullptr;
+    s->bc_op_b = with_b ? (uint16_t *)slot_alloc_impl(c, st, kSlotBcOpB, npad * s->kpad_bc * 2) : nullptr;
+    s->bc_norms = (float *)slot_alloc_impl(c, st, is_b ? kSlotBcNormB : kSlotBcNormA, npad * 4);
+    s->bc_xn = (float *)slot_alloc_impl(c, st, is_b ? kSlotBcXnB : kSlotBcXnA, npad * 4);
+    s->bc_gmin = with_b ? (float *)slot_alloc_impl(c, st, is_b ? kSlotBcGminB : kSlotBcGminA, (npad / 32) * 4)
+                        : nullptr;
+    s->bc_blk = (float4 *)slot_alloc_impl(c, st, is_b ? kSlotBcBlkB : kSlotBcBlkA, nblk * sizeof(float4));
+    s->bc_cent = (float *)slot_alloc_impl(c, st, is_b ? kSlotBcCentB : kSlotBcCentA, nblk * kBcCentStride * 4);
+    if ((with_a && !s->bc_op_a) || (with_b && (!s->bc_op_b || !s->bc_gmin)) || !s->bc_norms || !s->bc_xn ||
+        !s->bc_blk || !s->bc_cent)
+        return fail(HJ_ERR_OOM, "out of device memory (block-centred operands)");
+    launch_bc_prepare(*s, center, op_scale, s->bc_op_a, s->bc_op_b, s->bc_norms, s->bc_xn, s->bc_blk, s->bc_cent,
+                      s->bc_gmin, st, launches);
+    return check_cuda("block-centred operands");
+}
+
 // Key order by ascending dimension cost (ties by dim index) from set A's
 // sample; see hj_dim_order. Synchronises once on `st`.
 static int dim_order_by_cost(Ctx *c, cudaStream_t st, const void *x, int dtype_bytes, uint64_t n, uint32_t d,
@@ -359,6 +384,8 @@ static int prepare_join(Ctx *c, cudaStream_t st, const JoinIn &in, const hj_opts
     int form = form_override >= 0 ? form_override : (opts ? opts->form : HJ_FORM_PLAIN_FP64);
     if (form < HJ_FORM_PLAIN_FP64 || form > HJ_FORM_TC_FP16) return fail(HJ_ERR_INVALID_ARG, "unknown form");
     if (opts && opts->item_chunk > 4096) return fail(HJ_ERR_INVALID_ARG, "item_chunk must be at most 4096");
+    if (opts && (opts->tc_centring < HJ_CENTRING_AUTO || opts->tc_centring > HJ_CENTRING_BLOCK))
+        return fail(HJ_ERR_INVALID_ARG, "unknown tc_centring");
     int active_dims = opts ? opts->active_dims : -1;
     const bool ref_compat = opts && opts->ref_compat;
     if (active_dims < 0) active_dims = in.self ? 3 : 2;
@@ -537,6 +564,8 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
     cudaMemsetAsync(c->d_small + 2, 0, 5 * sizeof(unsigned long long), st);
     uint64_t band_total = 0, fp_items = 0;
     double c_rel = 0, c_abs = 0;
+    bool bc = false;  // per-block-centred operands (tensor-core forms)
+    BcConsts bck{};
     const double T = in.eps * in.eps;
     cudaEventRecord(c->ev[6], st);
     if (!tc) {
@@ -545,23 +574,64 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
         cudaEventRecord(c->ev[4], st);
         cudaEventRecord(c->ev[5], st);
     } else {
+        // Operand centring: one global centre, or a centre per 128-rank block
+        // (FP16 form, d <= 64) when asked for, or when the global centre would
+        // send more than an eighth of the block pairs to the FP64 kernel.
+        const int centring = opts ? opts->tc_centring : HJ_CENTRING_AUTO;
+        const bool bc_ok = form == HJ_FORM_TC_FP16 && d <= kBcMaxDim;
+        auto enable_bc = [&]() -> int {
+            if (int r = prepare_block_centring(c, st, &A, true, in.self, false, A.center, A.op_scale, &launches))
+                return r;
+            if (in.self) {
+                B.bc_op_b = A.bc_op_b, B.bc_norms = A.bc_norms, B.bc_xn = A.bc_xn, B.bc_gmin = A.bc_gmin;
+                B.bc_blk = A.bc_blk, B.bc_cent = A.bc_cent, B.kpad_bc = A.kpad_bc;
+            } else if (int r = prepare_block_centring(c, st, &B, false, true, true, B.center, B.op_scale,
+                                                      &launches)) {
+                return r;
+            }
+            bc = true;
+            bck = bc_constants(d, T, A.op_scale);
+            return HJ_OK;
+        };
+        if (centring == HJ_CENTRING_BLOCK) {
+            if (!bc_ok) return fail(HJ_ERR_UNSUPPORTED, "per-block centring needs the FP16 form and d <= 64");
+            if (int r = enable_bc()) return r;
+        }
         // the FP16 form works in scaled units: norms, eps^2 and the bound times op_scale^2
         // one-entry job table: counted ranks, thresholds and bound in the operand units
         fill_tc_job(c->h_job, form, d, T, A.op_scale, maxabs, 0, na_eff, 0, nb_eff, in.self, d_count, A.rows,
                     B.rows, &c_rel, &c_abs);
+        if (bc) c->h_job->ka = tc_atoms(form, 3 * d);
         cudaMemcpyAsync(c->d_job, c->h_job, sizeof(TcJob), cudaMemcpyHostToDevice, st);
         const double T_tc = T * A.op_scale * A.op_scale;
         // Items whose error band would exceed half of eps^2 (eps^2 tiny against
         // the squared norms: the cancellation limit of the norm expansion) run
         // on the FP64 kernel instead.
         IndexResult idx_tc, idx_fp;
+        // Routing limits: half of eps^2 for one global centre (wider bands hold
+        // billions of pairs there); with block centres the band of a tile is
+        // bounded by its residuals, and tiles up to 4 eps^2 (wide clusters,
+        // blocks that straddle two clusters) cost less as band pairs than on the
+        // FP64 kernel.
+        auto route_limit = [&](int attempt) { return attempt == 0 ? (bc ? 4.0 : 0.5) * T_tc : -1.0; };
         for (int attempt = 0;; ++attempt) {
-            const double limit = attempt == 0 ? 0.5 * T_tc : -1.0;  // -1: everything to FP64
-            int sr = split_items_by_precision(idx, A, B, c_rel, c_abs, limit, slot_alloc_cb, &actx, st, &idx_tc,
-                                              &idx_fp);
+            int sr = split_items_by_precision(idx, A, B, c_rel, c_abs, route_limit(attempt), bc ? &bck : nullptr,
+                                              slot_alloc_cb, &actx, st, &idx_tc, &idx_fp);
             if (sr == 2) return fail(HJ_ERR_OOM, "out of device memory (work list split)");
             if (sr) return check_cuda("work list split");
             launches += 2;
+            if (attempt == 0 && !bc && bc_ok && centring == HJ_CENTRING_AUTO &&
+                idx_fp.tile_pairs * 8 > idx.tile_pairs) {
+                // the split synchronised the stream: the job's first copy is done
+                if (int r = enable_bc()) return r;
+                c->h_job->ka = tc_atoms(form, 3 * d);
+                cudaMemcpyAsync(c->d_job, c->h_job, sizeof(TcJob), cudaMemcpyHostToDevice, st);
+                sr = split_items_by_precision(idx, A, B, c_rel, c_abs, route_limit(attempt), &bck, slot_alloc_cb,
+                                              &actx, st, &idx_tc, &idx_fp);
+                if (sr == 2) return fail(HJ_ERR_OOM, "out of device memory (work list split)");
+                if (sr) return check_cuda("work list split");
+                launches += 2;
+            }
             fp_items = idx_fp.n_items;
             cudaMemsetAsync(c->d_small + 2, 0, 5 * sizeof(unsigned long long), st);
             if (attempt == 0 && idx_tc.n_items == 0 && idx_fp.n_items && !(opts && opts->shard_count > 1)) {
@@ -591,7 +661,9 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
                 break;
             }
             const uint64_t cand_tc = idx_tc.tile_pairs * (uint64_t)kTcTileA * kTcTileB;
-            uint64_t cap = std::max<uint64_t>(1ull << 20, cand_tc / 4096);
+            // first band queue: 1/4096 of the candidates (1/1024 with block
+            // centres, whose wider tiles stay on the tensor cores)
+            uint64_t cap = std::max<uint64_t>(1ull << 20, cand_tc / (bc ? 1024 : 4096));
             const uint64_t cap_limit = std::max<uint64_t>(1ull << 27, cand_tc / 64);
             bool done = false, fallback = false;
             for (int grow = 0; grow < 4; ++grow) {
@@ -602,7 +674,7 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
                 std::string terr;
                 cudaEventRecord(c->ev[6], st);
                 if (launch_join_tc(A, B, form, c->d_job, na_eff, nb_eff, idx_tc, band, cap, d_band, d_err,
-                                   c->num_sms, st, &terr))
+                                   c->num_sms, st, &terr, bc ? &bck : nullptr))
                     return fail(HJ_ERR_CUDA, terr);
                 ++launches;
                 cudaEventRecord(c->ev[4], st);
@@ -665,6 +737,7 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
             stats->max_abs_err_band = tc ? (double)ef : 0.0;
         }
         stats->form_used = form;
+        stats->tc_centring = tc ? (bc ? HJ_CENTRING_BLOCK : HJ_CENTRING_GLOBAL) : 0;
         stats->fp64_items = fp_items;
         stats->reorder_ms = P.reorder_ms;
         int s = active_dims;
@@ -984,6 +1057,10 @@ uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dt
         b += n * (2 * W + 1) * 4 + n * 8;                     // packed keys (both layouts), permutation
         b += npad * d * 8;                                    // plain FP64 tiles (plain form or routed items)
         if (tc) b += npad * (hj_ceil_div(d, 64) * 64) * 4 + npad * 8;  // operands (widest form), norms
+        if (tc && d <= kBcMaxDim) {  // block-centred operands (both layouts), p, |h|, minima, blocks
+            const uint64_t kbc = hj_ceil_div(3 * d, 64) * 64;
+            b += npad * kbc * 4 + npad * 12 + (npad / kBcBlock) * (16 + kBcCentStride * 4);
+        }
         return b;
     };
     uint64_t b = per_set(na) + (self ? 0 : per_set(nb));
@@ -994,7 +1071,7 @@ uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dt
     b += tiles * (uint64_t)kMaxCombos * 8 + tiles * 64 * 16;
     if (tc) {
         const double cand = (double)na * (double)nb;
-        b += (uint64_t)std::max(1048576.0, cand / 4096.0) * kBandEntryBytes;
+        b += (uint64_t)std::max(1048576.0, cand / (d <= kBcMaxDim ? 1024.0 : 4096.0)) * kBandEntryBytes;
     }
     return b + (16ull << 20);
 }
@@ -1025,8 +1102,8 @@ int engine_prepare_job(cudaStream_t st_in, const void *a, const void *b, uint64_
     tc_band_constants(P.form, d, P.maxabs, &J.c_rel, &J.c_abs);
     const double T_tc = eps * eps * J.op_scale * J.op_scale;
     AllocCtx actx{c, st};
-    int sr = split_items_by_precision(P.idx, J.A, J.B, J.c_rel, J.c_abs, 0.5 * T_tc, slot_alloc_cb, &actx, st,
-                                      &J.idx_tc, &J.idx_fp);
+    int sr = split_items_by_precision(P.idx, J.A, J.B, J.c_rel, J.c_abs, 0.5 * T_tc, nullptr, slot_alloc_cb, &actx,
+                                      st, &J.idx_tc, &J.idx_fp);
     if (sr == 2) return fail(HJ_ERR_OOM, "out of device memory (work list split)");
     if (sr) return check_cuda("work list split");
     launches += 2;
@@ -1150,6 +1227,11 @@ int hj_ego_sort(const double *pts, uint64_t n, uint32_t d, double eps, const hj_
 
 int hj_debug_tc_estimates(const float *A, uint64_t nA, const float *B, uint64_t nB, uint32_t d, int form,
                           float *out) {
+    return hj_debug_tc_estimates_ex(A, nA, B, nB, d, form, HJ_CENTRING_GLOBAL, 0.0, out, nullptr);
+}
+
+int hj_debug_tc_estimates_ex(const float *A, uint64_t nA, const float *B, uint64_t nB, uint32_t d, int form,
+                             int centring, double eps, float *out, hj_stats *stats) {
     tl_error.clear();
     if (!A || !B || !out || nA == 0 || nB == 0) return fail(HJ_ERR_INVALID_ARG, "null pointer or empty set");
     if (!form_is_tc(form)) return fail(HJ_ERR_INVALID_ARG, "not a tensor-core form");
@@ -1160,6 +1242,7 @@ int hj_debug_tc_estimates(const float *A, uint64_t nA, const float *B, uint64_t 
         cudaGetLastError();
         return fail(HJ_ERR_OOM, "out of device memory");
     }
+    cudaMemset(dbg, 0xff, nA * nB * sizeof(float));  // NaN: pairs outside the work list
     double mx = 0;
     for (uint64_t i = 0; i < nA * d; ++i) mx = std::fmax(mx, std::fabs((double)A[i]));
     for (uint64_t i = 0; i < nB * d; ++i) mx = std::fmax(mx, std::fabs((double)B[i]));
@@ -1167,9 +1250,11 @@ int hj_debug_tc_estimates(const float *A, uint64_t nA, const float *B, uint64_t 
     hj_opts_init(&o);
     o.form = form;
     o.active_dims = 0;
+    o.tc_centring = centring;
     uint64_t cnt;
     set_tc_debug_output(dbg);
-    int r = hj_join_count_f32(A, nA, B, nB, d, 4.0 * (mx + 1.0) * std::sqrt((double)d), &o, &cnt, nullptr);
+    const double e = eps > 0 ? eps : 4.0 * (mx + 1.0) * std::sqrt((double)d);
+    int r = hj_join_count_f32(A, nA, B, nB, d, e, &o, &cnt, stats);
     set_tc_debug_output(nullptr);
     if (r == HJ_OK && cudaMemcpy(out, dbg, nA * nB * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
         r = check_cuda("debug copy");

@@ -369,6 +369,30 @@ __global__ void k_item_precision_flags(const WorkItem *__restrict__ items, uint6
     if (!tc) atomicAdd(tile_pairs_fp, (unsigned long long)(w.b1 - w.b0));
 }
 
+// Per-block-centred operands: the item's bound from its A block's summary and
+// the largest of its B blocks' (two per 256-rank B tile), at D = 0 (the D term
+// only grows with the block distance, where every pair is far outside).
+__global__ void k_item_precision_flags_bc(const WorkItem *__restrict__ items, uint64_t n,
+                                          const float4 *__restrict__ blk_a, const float4 *__restrict__ blk_b,
+                                          BcConsts k, double limit, uint32_t *flags,
+                                          unsigned long long *tile_pairs_fp) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const WorkItem w = items[i];
+    const float4 a = blk_a[w.a];
+    float xb = 0.f, cb = 0.f, qb = 0.f;
+    for (uint32_t b = 2 * w.b0; b < 2 * w.b1; ++b) {
+        const float4 v = blk_b[b];
+        xb = fmaxf(xb, v.x);
+        cb = fmaxf(cb, v.y);
+        qb = fmaxf(qb, v.z);
+    }
+    const float tau = bc_tau(a.x, a.y, a.z, xb, cb, qb, 0.f, k, nullptr);
+    const bool tc = (double)tau <= limit;
+    flags[i] = tc ? 1u : 0u;
+    if (!tc) atomicAdd(tile_pairs_fp, (unsigned long long)(w.b1 - w.b0));
+}
+
 // flags[] holds the exclusive prefix count of tensor-core items.
 __global__ void k_item_split(const WorkItem *__restrict__ items, uint64_t n, const uint32_t *__restrict__ flags_scan,
                              unsigned long long n_tc, WorkItem *tc_out, WorkItem *fp_out) {
@@ -394,8 +418,9 @@ __global__ void k_item_split(const WorkItem *__restrict__ items, uint64_t n, con
 }
 
 int split_items_by_precision(const IndexResult &in, const SortedSet &A, const SortedSet &B, double c_rel,
-                             double c_abs, double limit, void *(*alloc)(void *ctx, int slot, size_t bytes),
-                             void *actx, cudaStream_t st, IndexResult *tc_out, IndexResult *fp_out) {
+                             double c_abs, double limit, const BcConsts *bc,
+                             void *(*alloc)(void *ctx, int slot, size_t bytes), void *actx, cudaStream_t st,
+                             IndexResult *tc_out, IndexResult *fp_out) {
     *tc_out = in;
     *fp_out = IndexResult();
     if (in.n_items == 0) return 0;
@@ -404,9 +429,13 @@ int split_items_by_precision(const IndexResult &in, const SortedSet &A, const So
     unsigned long long *stats = (unsigned long long *)alloc(actx, kSlotSplitStats, 2 * sizeof(unsigned long long));
     if (!flags || !stats) return 2;
     cudaMemsetAsync(stats, 0, 2 * sizeof(unsigned long long), st);
-    k_item_precision_flags<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(in.items, n, A.tile_maxnorm_a,
-                                                                         B.tile_maxnorm_b, c_rel, c_abs, limit,
-                                                                         flags, stats + 1);
+    if (bc)
+        k_item_precision_flags_bc<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(in.items, n, A.bc_blk, B.bc_blk, *bc,
+                                                                                limit, flags, stats + 1);
+    else
+        k_item_precision_flags<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(in.items, n, A.tile_maxnorm_a,
+                                                                             B.tile_maxnorm_b, c_rel, c_abs, limit,
+                                                                             flags, stats + 1);
     launch_scan_u32(flags, n, stats, st);
     unsigned long long h[2];
     cudaMemcpyAsync(h, stats, sizeof(h), cudaMemcpyDeviceToHost, st);

@@ -105,7 +105,70 @@ struct SortedSet {
     float *group_minnorm = nullptr;   // per 32-row group: min |x - center|^2
     uint64_t npad_tc = 0;
     uint32_t kpad_tf32 = 0, kpad_bf16 = 0;
+    // per-block centring of the FP16 operands (HJ_CENTRING_BLOCK; see BcConsts):
+    // [npad][kpad_bc] rows in the A layout [h | h | c] and the B layout [h | c | h]
+    uint16_t *bc_op_a = nullptr, *bc_op_b = nullptr;
+    float *bc_norms = nullptr;    // p = |h|^2 + 2 h.c per rank (FP32; padding rows kPadNorm)
+    float *bc_xn = nullptr;       // |h| per rank, rounded up
+    float *bc_gmin = nullptr;     // per 32-rank group: min p
+    float4 *bc_blk = nullptr;     // per 128-rank block: {max |h|, |c|, max |p|, 0}, rounded up
+    float *bc_cent = nullptr;     // per block: c in FP32 (FP16 values), kBcCentStride floats, zero padded
+    uint32_t kpad_bc = 0;
 };
+
+// Per-block centring of the FP16 operands. Every 128-rank block of a sorted
+// set (one A tile, half a B tile) gets a centre c whose coordinates are FP16
+// values in the operand units ((x - center) * op_scale), the midpoint of the
+// block's range rounded to FP16; every rank is stored as that centre plus its
+// residual h = fl16(x - c). Operand rows hold 3d columns,
+//     A: [h | h | c]      B: [h | c | h],
+// so that one MMA gives v_ij = h_i.h_j + h_i.c_j + c_i.h_j = x'_i.x'_j - c_i.c_j
+// for the operand points x' = c + h, and
+//     dist2(x'_i, x'_j) = p_i + p_j + |c_i - c_j|^2 - 2 v_ij,  p = |h|^2 + 2 h.c.
+// The only rounding of the points is h's (relative 2^-11 per coordinate): it
+// moves a point by rho <= 2^-11 |h| (plus the subnormal floor), and distances
+// by rho_i + rho_j. The error bound of s = p_i + p_j + D - 2 v (bc_tau) is
+// therefore linear in the residual norms instead of quadratic in the distance
+// from one global centre, which keeps clustered data with eps far below its
+// spread on the tensor cores.
+constexpr uint32_t kBcBlock = 128;      // ranks per centring block (= kTcTileA, = kTcTileB / 2)
+constexpr uint32_t kBcMaxDim = 64;      // 3d <= 192 operand columns
+constexpr uint32_t kBcCentStride = 64;  // floats per block in bc_cent
+struct BcConsts {
+    float kp21;     // 2 kpad_bc 2^-22: the MMA accumulation error of v per unit of S, doubled for s
+    float eps;      // eps in operand units, rounded up
+    float rho_u;    // rounding radius per unit of |h| (2^-11 with margin)
+    float rho_c;    // rounding radius floor (FP16 subnormals, FP64 shift), per point
+    float u_norm;   // FP32 rounding of p (relative, with margin)
+    float u_d;      // FP32 rounding of D = |c_i - c_j|^2 (relative)
+    float theta_t;  // rounding of the FP64 pair test near eps^2, twice, in operand units
+};
+// Half-width of the band of s around eps^2 for a pair of a row (|h| = xa, its
+// block's |c| = ca, |p| = pa) and a B block (max |h| = xb, |c| = cb, max |p| =
+// qb) at block-centre distance^2 D; *S_out = the bound on sum_k |A_ik B_jk|.
+// With E = |s - dist2(x'_i, x'_j)| <= kp21 S + u_norm (pa + qb) + u_d D and
+// rho = rho_i + rho_j: dist2 <= s + E + 2 rho sqrt(s + E) + rho^2, and
+// 2 rho sqrt(E) <= rho^2 + E, so near eps^2 the FP64 test agrees with
+// "s + tau <= eps^2 is inside, s - tau > eps^2 is outside" for
+// tau = 2 E + 2 eps rho + 2 rho^2 + theta_t (times 1.25 for the FP32 of this
+// function).
+__host__ __device__ inline float bc_tau(float xa, float ca, float pa, float xb, float cb, float qb, float D,
+                                        const BcConsts &k, float *S_out) {
+    const float S = fmaf(xa, xb + cb, ca * xb);
+    const float rho = fmaf(k.rho_u, xa + xb, 2.0f * k.rho_c);
+    const float E = fmaf(k.kp21, S, fmaf(k.u_norm, pa + qb, k.u_d * D));
+    if (S_out) *S_out = S;
+    return 1.25f * fmaf(2.0f, E, fmaf(2.0f * k.eps, rho, fmaf(2.0f * rho, rho, k.theta_t)));
+}
+// Fills the constants for dimension d, eps^2 = T (caller units) and the FP16
+// operand scale.
+BcConsts bc_constants(uint32_t d, double T, double op_scale);
+// Block centres, residual operands (A and/or B layout; null skips one), p, |h|
+// and block summaries of a sorted set from its sorted rows; then the group
+// minima of p when gmin is non-null. centre = the global per-dim shift.
+void launch_bc_prepare(const SortedSet &s, const double *center, double op_scale, uint16_t *op_a, uint16_t *op_b,
+                       float *norms, float *xn, float4 *blk, float *cent, float *gmin, cudaStream_t st,
+                       int *launches);
 
 constexpr float kPadNorm = 1.0e30f;
 
@@ -124,9 +187,12 @@ struct WorkItem {
 constexpr int kSlotIndexFirst = 64;
 
 struct IndexResult;
+// With bc non-null the bound is the per-block-centred one (bc_tau with the
+// sets' block summaries, D = 0) and c_rel / c_abs are unused.
 int split_items_by_precision(const IndexResult &tc_in, const SortedSet &A, const SortedSet &B, double c_rel,
-                             double c_abs, double limit, void *(*alloc)(void *ctx, int slot, size_t bytes),
-                             void *actx, cudaStream_t st, IndexResult *tc_out, IndexResult *fp_out);
+                             double c_abs, double limit, const BcConsts *bc,
+                             void *(*alloc)(void *ctx, int slot, size_t bytes), void *actx, cudaStream_t st,
+                             IndexResult *tc_out, IndexResult *fp_out);
 
 // Restricts a work list to shard k of K: the contiguous item range whose
 // cumulative tile-pair load lies in [k L / K, (k+1) L / K) (L = total load).
@@ -243,9 +309,14 @@ void fill_tc_job(TcJob *j, int form, uint32_t d, double T, double op_scale, doub
 // A and B describe the operand matrices (layout pointers, npad_tc rows, kpad,
 // norms and their tile maxima and group minima); their d is the largest of the
 // jobs'. na0 / nb0: job 0's counted ranks (debug output only).
+// With bc non-null (FP16 form, one job): the per-block-centred operands of
+// A (A layout) and B (B layout) and their summaries; the job's ka must be the
+// one of 3d columns (tc_atoms).
 int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob *d_jobs, uint64_t na0, uint64_t nb0,
                    const IndexResult &idx, uint2 *band, uint64_t band_cap, unsigned long long *d_band_total,
-                   uint32_t *d_err, int num_sms, cudaStream_t st, std::string *err);
+                   uint32_t *d_err, int num_sms, cudaStream_t st, std::string *err, const BcConsts *bc = nullptr);
+// K atoms (128-byte operand column groups) of a form's operand rows of kcols columns.
+uint32_t tc_atoms(int form, uint32_t kcols);
 // FP64 recheck of the band pairs, each against its job's rows and eps^2.
 void launch_recheck(const TcJob *d_jobs, int dtype_bytes, const uint2 *band, const unsigned long long *d_band_total,
                     uint64_t band_cap, unsigned int *d_max_err_bits, cudaStream_t st);

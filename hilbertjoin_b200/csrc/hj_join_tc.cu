@@ -62,6 +62,9 @@ constexpr int kChunkCols = 64;
 constexpr int kChunkGroups = kChunkCols / 32;  // 32-column groups per chunk
 constexpr int kEpiChunks = kEpiCols / kChunkCols;
 constexpr int kEpiVec = kEpiCols / 32;  // norms per lane, group minima per warp
+// From this many rows of a 32-column group on, the lanes classify their own
+// rows (32 shuffled column norms) instead of the warp walking row by row.
+constexpr int kDenseRows = 8;
 // 16 epilogue warps (4 per quadrant) were measured slower: at 18 warps the
 // register cap is 96 (spills) and the static shared memory no longer fits next
 // to the 225 KB operand plan.
@@ -97,6 +100,12 @@ struct TcArgs {
     const uint32_t *perm_a, *perm_b;  // EGO rank -> input index (for dbg)
     uint64_t gate_ns;               // test hook: > 0 makes the epilogue wait this long on a barrier
                                     // that nothing arrives on, then raise kErrTimeout
+    // per-block centring (BC kernels): norm_a / norm_b / gmin_b are then p and its
+    // group minima; |h| of the A rows, block summaries and centres of both sets
+    const float *xn_a;
+    const float4 *blk_a, *blk_b;
+    const float *cent_a, *cent_b;
+    BcConsts bc;
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -195,7 +204,7 @@ __device__ __forceinline__ void drain_until(uint64_t *bar, uint32_t parity, uint
 
 // ---------------------------------------------------------------- the kernel
 
-template <int FORM>
+template <int FORM, bool BC>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_join_tc(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_a2,
               const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ CUtensorMap tm_b2, TcArgs p) {
@@ -410,11 +419,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         WorkItem w = it < p.n_items ? p.items[it] : WorkItem{0, 0, 0, 0};
         WorkItem wn = it + stride < p.n_items ? p.items[it + stride] : WorkItem{0, 0, 0, 0};
         uint32_t bt = w.b0;
+        // per-block centring: the row's p, |h| and |p|, its block's |c| and centre
+        // coordinates (lane, lane + 32), the job's eps^2 bounds; per tile the B
+        // block's summary and centre, prefetched one tile ahead with the minima
+        float p_row = 0.f, xa = 0.f, pa = 0.f, cna = 0.f, t_lo = 0.f, t_hi = 0.f;
+        float ca[2] = {0.f, 0.f}, pf_cb[2] = {0.f, 0.f};
+        float4 pf_blk = make_float4(0.f, 0.f, 0.f, 0.f);
         float pf_gmin[kEpiVec];
         auto prefetch = [&](uint32_t b) {
             const uint64_t g = (uint64_t)b * kTcTileB + half * kEpiCols;
             const float4 m = __ldg(reinterpret_cast<const float4 *>(p.gmin_b + g / 32));
             pf_gmin[0] = m.x, pf_gmin[1] = m.y, pf_gmin[2] = m.z, pf_gmin[3] = m.w;
+            if constexpr (BC) {
+                const uint64_t blkb = g / kBcBlock;
+                pf_blk = __ldg(p.blk_b + blkb);
+                pf_cb[0] = __ldg(p.cent_b + blkb * kBcCentStride + lane);
+                pf_cb[1] = __ldg(p.cent_b + blkb * kBcCentStride + 32 + lane);
+            }
         };
 #pragma unroll
         for (int q = 0; q < kEpiVec; ++q) pf_gmin[q] = 0.f;
@@ -441,6 +462,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             s_unscale = J.s_unscale;
             gi = (uint64_t)ww.a * kTcTileA + quad * 32 + lane;
             row_ok = gi >= J.a_row0 && gi < J.a_end;
+            if constexpr (BC) {
+                // thresholds per tile (they depend on the B block): see the tile loop
+                p_row = row_ok ? __ldg(p.norm_a + gi) : 0.f;
+                xa = row_ok ? __ldg(p.xn_a + gi) : 0.f;
+                pa = fabsf(p_row);
+                const uint64_t blka = (uint64_t)ww.a * kTcTileA / kBcBlock;
+                cna = __ldg(&p.blk_a[blka].y);
+                ca[0] = __ldg(p.cent_a + blka * kBcCentStride + lane);
+                ca[1] = __ldg(p.cent_a + blka * kBcCentStride + 32 + lane);
+                t_lo = T_lo;
+                t_hi = T_hi;
+                na = p_row;
+                thr_out = thr_in = -3.0e38f;
+                (void)crel;
+                (void)cabs;
+                return;
+            }
             na = row_ok ? __ldg(p.norm_a + gi) : kPadNorm;
             float tmaxb = 0.f;
             for (uint32_t b = ww.b0 + lane; b < ww.b1; b += 32) tmaxb = fmaxf(tmaxb, __ldg(p.tmax_b + b));
@@ -463,6 +501,25 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             float gmin[kEpiVec];
 #pragma unroll
             for (int q = 0; q < kEpiVec; ++q) gmin[q] = pf_gmin[q];
+            if constexpr (BC) {
+                // this tile's B block: D = |c_A - c_B|^2 (FP32, lanes over the
+                // dims), the band half-width of the lane's row against the block,
+                // and the thresholds on t = p_j - 2 v (s = p_row + D + t)
+                float D = 0.f;
+#pragma unroll
+                for (int m = 0; m < 2; ++m) {
+                    const float df = ca[m] - pf_cb[m];
+                    D = fmaf(df, df, D);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) D += __shfl_xor_sync(0xffffffffu, D, o);
+                float S;
+                const float tau = bc_tau(xa, cna, pa, pf_blk.x, pf_blk.y, pf_blk.z, D, p.bc, &S);
+                const float marg = 8.0f * 5.9604645e-8f * (fabsf(t_hi) + pa + pf_blk.z + D + tau + 2.0f * S);
+                na = p_row + D;
+                thr_out = row_ok ? (t_hi + tau) - p_row - D + marg : -3.0e38f;
+                thr_in = row_ok ? (t_lo - tau) - p_row - D - marg : -3.0e38f;
+            }
             const uint32_t cur_bt = bt;
             // the item's rows stay for its last tile; the next item's are set after it
             const bool last_tile = bt + 1 >= w.b1;
@@ -530,6 +587,52 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                                 jlo = first > 0 ? (first > kEpiCols ? kEpiCols : (int)first) : 0;
                             }
                         }
+                        if (__popc(rows) >= kDenseRows && p.dbg == nullptr) {
+                            // Many rows (tiles where neighbours are common): every lane
+                            // classifies its own row against the group's 32 columns, the
+                            // column norms broadcast by shuffles; then only the rows with
+                            // band pairs are walked, as below, to queue them.
+                            const bool mine = need && row_ok;
+                            const float *vg = v + h2 * 32;
+                            uint32_t bbits = 0, c32 = 0;
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) {
+                                const float t = fmaf(-2.0f, vg[j], __shfl_sync(0xffffffffu, nbl, j));
+                                const bool ok = mine && (unsigned)(cb + j - jlo) < (unsigned)(jhi - jlo);
+                                c32 += (ok && t <= thr_in) ? 1u : 0u;
+                                bbits |= (ok && t > thr_in && t <= thr_out) ? (1u << j) : 0u;
+                            }
+                            cnt += c32;
+                            rows = __ballot_sync(0xffffffffu, bbits != 0);
+                            while (rows) {
+                                const int L = __ffs(rows) - 1;
+                                rows &= rows - 1;
+                                if (lane == (uint32_t)L) {
+#pragma unroll
+                                    for (int q = 0; q < 8; ++q)
+                                        reinterpret_cast<float4 *>(srow)[q] = make_float4(vg[4 * q], vg[4 * q + 1],
+                                                                                          vg[4 * q + 2], vg[4 * q + 3]);
+                                }
+                                __syncwarp();
+                                const uint32_t bm = __shfl_sync(0xffffffffu, bbits, L);
+                                const float naL = __shfl_sync(0xffffffffu, na, L);
+                                const int lead = __ffs(bm) - 1;
+                                unsigned long long base = 0;
+                                if (lane == (uint32_t)lead) base = atomicAdd(p.band_total, (unsigned long long)__popc(bm));
+                                base = __shfl_sync(0xffffffffu, base, lead);
+                                const unsigned long long k = base + __popc(bm & ((1u << lane) - 1u));
+                                if (((bm >> lane) & 1u) && k < p.band_cap) {
+                                    BandEntry e;
+                                    e.ia = (uint32_t)(gi - (uint64_t)lane + (uint64_t)L);
+                                    e.jb = (uint32_t)(gj0 + cb + (int)lane);
+                                    e.s_hat = (naL + fmaf(-2.0f, srow[lane], nbl)) * s_unscale;
+                                    e.pad = job;
+                                    p.band[k] = e;
+                                }
+                                __syncwarp();
+                            }
+                            continue;
+                        }
                         while (rows) {
                             const int L = __ffs(rows) - 1;
                             rows &= rows - 1;
@@ -554,9 +657,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                             cnt += (ok && t <= tinL) ? 1ull : 0ull;
                             if (p.dbg != nullptr && giL < p.na && gj0 + col < p.nb)
                                 p.dbg[(uint64_t)p.perm_a[giL] * p.nb + p.perm_b[gj0 + col]] = (naL + t) * s_unscale;
-                            if (ok && t > tinL && t <= toutL) {  // band pair: very rare
-                                const unsigned long long k = atomicAdd(p.band_total, 1ull);
-                                if (k < p.band_cap) {
+                            // band pairs of the row: one reservation for the warp
+                            const bool isb = ok && t > tinL && t <= toutL;
+                            const uint32_t bm = __ballot_sync(0xffffffffu, isb);
+                            if (bm) {
+                                const int lead = __ffs(bm) - 1;
+                                unsigned long long base = 0;
+                                if (lane == (uint32_t)lead) base = atomicAdd(p.band_total, (unsigned long long)__popc(bm));
+                                base = __shfl_sync(0xffffffffu, base, lead);
+                                const unsigned long long k = base + __popc(bm & ((1u << lane) - 1u));
+                                if (isb && k < p.band_cap) {
                                     BandEntry e;
                                     e.ia = (uint32_t)giL;
                                     e.jb = (uint32_t)(gj0 + col);
@@ -735,6 +845,38 @@ static TcLayout tc_layout(int form, uint32_t d) {
     return L;
 }
 
+uint32_t tc_atoms(int form, uint32_t kcols) { return tc_layout(form, kcols).ka; }
+
+// Per-block centring constants (operand units, FP16 form):
+//   kp21: the accumulation model above, K = kpad_bc product terms of
+//     magnitude sum <= S per dot, the dot entering s twice: 2 kpad 2^-22;
+//   rho_u: |fl16(h) - h| <= 2^-11 |h| per coordinate (normal range), with
+//     |h| <= |fl16(h)| (1 + 2^-10): 1.001 * 2^-11 per unit of the stored |h|;
+//   rho_c: subnormal FP16 (|h| < 2^-14) is off by at most 2^-25 per
+//     coordinate, and the FP64 shift (x - center) * scale by 2^-52 of 2^15:
+//     sqrt(d) (2^-25 + 2^-37), doubled;
+//   u_norm: p rounded once from FP64 to FP32 (2^-24 relative), doubled;
+//   u_d: D in FP32, two FMAs per lane and a five-step sum of the lanes, with
+//     the differences of FP16 values exact or rounded once: 16 * 2^-24;
+//   theta_t: the FP64 pair test sums d squares of exact differences with FMAs,
+//     relative error below (d + 2) 2^-53 of dist2 ~ eps^2: 2 (d + 2) 2^-53 T.
+BcConsts bc_constants(uint32_t d, double T, double op_scale) {
+    const double s2 = op_scale * op_scale, kpad = (double)tc_atoms(HJ_FORM_TC_FP16, 3 * d) * 64.0;
+    auto up = [](double v) {
+        const float f = (float)v;
+        return (double)f >= v ? f : std::nextafter(f, INFINITY);
+    };
+    BcConsts k;
+    k.kp21 = up(2.0 * kpad * std::ldexp(1.0, -22));
+    k.eps = up(std::sqrt(T * s2) * (1.0 + 1e-12));
+    k.rho_u = up(1.001 * std::ldexp(1.0, -11));
+    k.rho_c = up(2.0 * std::sqrt((double)d) * (std::ldexp(1.0, -25) + std::ldexp(1.0, -37)));
+    k.u_norm = up(std::ldexp(1.0, -23));
+    k.u_d = up(16.0 * std::ldexp(1.0, -24));
+    k.theta_t = up(2.0 * (d + 2.0) * std::ldexp(1.0, -53) * T * s2);
+    return k;
+}
+
 static float *g_dbg_out = nullptr;  // set by tests through hj_debug_tc_estimates
 static uint64_t g_gate_ns = 0;      // set by tests through hj_debug_set_wait_gate
 
@@ -770,15 +912,24 @@ void fill_tc_job(TcJob *j, int form, uint32_t d, double T, double op_scale, doub
 
 int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob *d_jobs, uint64_t na0, uint64_t nb0,
                    const IndexResult &idx, uint2 *band, uint64_t band_cap, unsigned long long *d_band_total,
-                   uint32_t *d_err, int num_sms, cudaStream_t st, std::string *err) {
+                   uint32_t *d_err, int num_sms, cudaStream_t st, std::string *err, const BcConsts *bc) {
     if (idx.n_items == 0) return 0;
-    const TcLayout L = tc_layout(form, A.d);
+    if (bc && (form != HJ_FORM_TC_FP16 || A.d > kBcMaxDim || !A.bc_op_a || !B.bc_op_b)) {
+        *err = "per-block centring needs the FP16 form, d <= 64 and the centred layouts";
+        return 1;
+    }
+    const TcLayout L = tc_layout(form, bc ? 3 * A.d : A.d);
     if (L.nst < 2) {
         *err = "dimension too large for the tensor-core kernel";
         return 1;
     }
     CUtensorMap ma, ma2, mb, mb2;
-    if (form == HJ_FORM_TC_TF32) {
+    if (bc) {
+        if (!make_map(&ma, A.bc_op_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, A.npad_tc, A.kpad_bc, kTcTileA, err)) return 1;
+        if (!make_map(&mb, B.bc_op_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, B.npad_tc, B.kpad_bc, kTcTileB, err)) return 1;
+        ma2 = ma;
+        mb2 = mb;
+    } else if (form == HJ_FORM_TC_TF32) {
         if (!make_map(&ma, A.tf32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, A.npad_tc, A.kpad_tf32, kTcTileA, err)) return 1;
         if (!make_map(&mb, B.tf32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, B.npad_tc, B.kpad_tf32, kTcTileB, err)) return 1;
         ma2 = ma;
@@ -817,17 +968,32 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
     a.perm_a = A.perm;
     a.perm_b = B.perm;
     a.gate_ns = g_gate_ns;
+    if (bc) {
+        a.norm_a = A.bc_norms;
+        a.norm_b = B.bc_norms;
+        a.gmin_b = B.bc_gmin;
+        a.tmax_b = nullptr;
+        a.xn_a = A.bc_xn;
+        a.blk_a = A.bc_blk;
+        a.blk_b = B.bc_blk;
+        a.cent_a = A.bc_cent;
+        a.cent_b = B.bc_cent;
+        a.bc = *bc;
+    }
     uint64_t grid = (uint64_t)num_sms;
     if (grid > idx.n_items) grid = idx.n_items;
-    if (form == HJ_FORM_TC_TF32) {
-        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_TF32>, 225 * 1024);
-        k_join_tc<HJ_FORM_TC_TF32><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
+    if (bc) {
+        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_FP16, true>, 225 * 1024);
+        k_join_tc<HJ_FORM_TC_FP16, true><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
+    } else if (form == HJ_FORM_TC_TF32) {
+        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_TF32, false>, 225 * 1024);
+        k_join_tc<HJ_FORM_TC_TF32, false><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
     } else if (form == HJ_FORM_TC_FP16) {
-        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_FP16>, 225 * 1024);
-        k_join_tc<HJ_FORM_TC_FP16><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
+        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_FP16, false>, 225 * 1024);
+        k_join_tc<HJ_FORM_TC_FP16, false><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
     } else {
-        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_BF16X3>, 225 * 1024);
-        k_join_tc<HJ_FORM_TC_BF16X3><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
+        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_BF16X3, false>, 225 * 1024);
+        k_join_tc<HJ_FORM_TC_BF16X3, false><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {

@@ -963,6 +963,144 @@ __global__ void k_group_min(const float *__restrict__ v, uint64_t npad, int grou
     out[t] = m;
 }
 
+// ------------------------------------------------------------ per-block centring
+
+// One CUDA block per 128-rank block of a sorted set (kBcBlock threads). The
+// block's rows are read once (contiguous in the sorted layout), shifted and
+// scaled as the global FP16 operands are ((x - center) * scale in FP64), and
+// kept in shared memory; per dim the midpoint of the block's range, rounded to
+// FP16, is the centre c; every rank's residual h = fl16(x - c) (round to
+// nearest, once), p = |h|^2 + 2 h.c from the FP16 values in FP64, |h|; then the
+// operand rows (A: [h | h | c], B: [h | c | h], zero padded to kpad) are
+// written as 16-byte chunks, consecutive threads on consecutive chunks.
+// Ranks past n (up to npad) are padding: zero operands, p = kPadNorm, |h| = 0.
+// |h_t| <= (max - min) / 2 + 2^-11 |c_t| < 2^15 (1 + 2^-11): no FP16 overflow.
+template <typename T>
+__global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ rows, uint64_t n, uint32_t d,
+                                                         const double *__restrict__ center, double scale,
+                                                         uint32_t kpad, uint16_t *__restrict__ op_a,
+                                                         uint16_t *__restrict__ op_b, float *__restrict__ norms,
+                                                         float *__restrict__ xn, float4 *__restrict__ blk,
+                                                         float *__restrict__ cent) {
+    extern __shared__ double bc_sm[];  // [kBcBlock][d] shifted coordinates, then residuals; [d] centre
+    double *cs = bc_sm + (size_t)kBcBlock * d;
+    __shared__ float red_x[kBcBlock / 32], red_p[kBcBlock / 32];
+    const uint64_t r0 = (uint64_t)blockIdx.x * kBcBlock;
+    const uint32_t nr = r0 >= n ? 0u : (n - r0 < kBcBlock ? (uint32_t)(n - r0) : kBcBlock);
+    const T *src = rows + r0 * d;
+    for (uint32_t e = threadIdx.x; e < nr * d; e += kBcBlock) bc_sm[e] = ((double)src[e] - center[e % d]) * scale;
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < d; t += kBcBlock) {
+        double lo = INFINITY, hi = -INFINITY;
+        for (uint32_t r = 0; r < nr; ++r) {
+            const double v = bc_sm[r * d + t];
+            lo = fmin(lo, v);
+            hi = fmax(hi, v);
+        }
+        cs[t] = nr ? (double)__half2float(__double2half(0.5 * lo + 0.5 * hi)) : 0.0;
+    }
+    __syncthreads();
+    const uint32_t r = threadIdx.x;
+    float my_x = 0.f, my_p = 0.f;
+    if (r < nr) {
+        double hh = 0.0, hc = 0.0;
+        for (uint32_t t = 0; t < d; ++t) {
+            const double h = (double)__half2float(__double2half(bc_sm[r * d + t] - cs[t]));
+            bc_sm[r * d + t] = h;
+            hh = fma(h, h, hh);
+            hc = fma(h, cs[t], hc);
+        }
+        const double p = fma(2.0, hc, hh);
+        norms[r0 + r] = (float)p;
+        my_p = fabsf((float)p) * (1.0f + 2.4e-7f);
+        my_x = (float)sqrt(hh) * (1.0f + 2.4e-7f);
+        if (xn) xn[r0 + r] = my_x;
+    } else {
+        norms[r0 + r] = kPadNorm;
+        if (xn) xn[r0 + r] = 0.f;
+    }
+    __syncthreads();
+    const uint32_t cpr = kpad / 8;  // 16-byte chunks per operand row
+    for (uint32_t e = threadIdx.x; e < kBcBlock * cpr; e += kBcBlock) {
+        const uint32_t rr = e / cpr, q = e % cpr;
+        uint32_t wa[4], wb[4];
+#pragma unroll
+        for (int h2 = 0; h2 < 4; ++h2) {
+            uint32_t ea = 0, eb = 0;
+#pragma unroll
+            for (int z = 0; z < 2; ++z) {
+                const uint32_t k = 8 * q + 2 * h2 + z;
+                double av = 0.0, bv = 0.0;
+                if (rr < nr) {
+                    if (k < d) {
+                        av = bv = bc_sm[rr * d + k];
+                    } else if (k < 2 * d) {
+                        av = bc_sm[rr * d + k - d];
+                        bv = cs[k - d];
+                    } else if (k < 3 * d) {
+                        av = cs[k - 2 * d];
+                        bv = bc_sm[rr * d + k - 2 * d];
+                    }
+                }
+                // FP16 values already: the conversions are exact
+                ea |= (uint32_t)__half_as_ushort(__double2half(av)) << (16 * z);
+                eb |= (uint32_t)__half_as_ushort(__double2half(bv)) << (16 * z);
+            }
+            wa[h2] = ea;
+            wb[h2] = eb;
+        }
+        const uint64_t o = (r0 + rr) * kpad / 8 + q;
+        if (op_a) reinterpret_cast<uint4 *>(op_a)[o] = make_uint4(wa[0], wa[1], wa[2], wa[3]);
+        if (op_b) reinterpret_cast<uint4 *>(op_b)[o] = make_uint4(wb[0], wb[1], wb[2], wb[3]);
+    }
+    // block summaries: max |h|, |c|, max |p| (all rounded up)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        my_x = fmaxf(my_x, __shfl_xor_sync(0xffffffffu, my_x, o));
+        my_p = fmaxf(my_p, __shfl_xor_sync(0xffffffffu, my_p, o));
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        red_x[threadIdx.x >> 5] = my_x;
+        red_p[threadIdx.x >> 5] = my_p;
+    }
+    for (uint32_t t = threadIdx.x; t < kBcCentStride; t += kBcBlock)
+        cent[(uint64_t)blockIdx.x * kBcCentStride + t] = t < d ? (float)cs[t] : 0.f;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float mx = 0.f, mp = 0.f;
+        for (int w = 0; w < (int)(kBcBlock / 32); ++w) {
+            mx = fmaxf(mx, red_x[w]);
+            mp = fmaxf(mp, red_p[w]);
+        }
+        double cc = 0.0;
+        for (uint32_t t = 0; t < d; ++t) cc = fma(cs[t], cs[t], cc);
+        blk[blockIdx.x] = make_float4(mx, (float)sqrt(cc) * (1.0f + 2.4e-7f), mp, 0.f);
+    }
+}
+
+void launch_bc_prepare(const SortedSet &s, const double *center, double op_scale, uint16_t *op_a, uint16_t *op_b,
+                       float *norms, float *xn, float4 *blk, float *cent, float *gmin, cudaStream_t st,
+                       int *launches) {
+    if (s.npad_tc == 0) return;
+    const unsigned blocks = (unsigned)(s.npad_tc / kBcBlock);
+    const size_t smem = ((size_t)kBcBlock * s.d + s.d) * sizeof(double);
+    if (s.dtype_bytes == 8) {
+        ensure_max_dynamic_smem((const void *)k_bc_prepare<double>, (int)((kBcBlock + 1) * kBcMaxDim * 8));
+        k_bc_prepare<double><<<blocks, kBcBlock, smem, st>>>(static_cast<const double *>(s.rows), s.n, s.d, center,
+                                                             op_scale, s.kpad_bc, op_a, op_b, norms, xn, blk, cent);
+    } else {
+        ensure_max_dynamic_smem((const void *)k_bc_prepare<float>, (int)((kBcBlock + 1) * kBcMaxDim * 8));
+        k_bc_prepare<float><<<blocks, kBcBlock, smem, st>>>(static_cast<const float *>(s.rows), s.n, s.d, center,
+                                                            op_scale, s.kpad_bc, op_a, op_b, norms, xn, blk, cent);
+    }
+    int L = 1;
+    if (gmin) {
+        k_group_min<<<(unsigned)hj_ceil_div(s.npad_tc / 32, 256), 256, 0, st>>>(norms, s.npad_tc, 32, gmin);
+        ++L;
+    }
+    if (launches) *launches += L;
+}
+
 void launch_gather(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const uint32_t *perm,
                    const uint32_t *keys_wm, uint32_t W, const SortedSet &o, uint32_t flags, cudaStream_t st,
                    int *launches) {

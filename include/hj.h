@@ -79,6 +79,23 @@ typedef enum {
     HJ_FORM_TC_FP16 = 4
 } hj_form;
 
+/* Operand centring of the FP16 tensor-core form (hj_opts.tc_centring). */
+typedef enum {
+    /* HJ_CENTRING_BLOCK when, with one global centre, more than an eighth of
+     * the block pairs would run on the FP64 kernel (the norm expansion's
+     * cancellation limit: eps small against the spread of the data) and
+     * d <= 64; HJ_CENTRING_GLOBAL otherwise. */
+    HJ_CENTRING_AUTO = 0,
+    /* One centre for the whole join (the per-dim midpoint of the data). */
+    HJ_CENTRING_GLOBAL = 1,
+    /* A centre per 128-point block of the EGO order, exact in FP16, and each
+     * point stored as that centre plus its FP16 residual; the operand rows
+     * carry the residual and centre cross terms as extra K columns (3d of
+     * them), so the error band scales with the residual norms. FP16 form,
+     * d <= 64. */
+    HJ_CENTRING_BLOCK = 2
+} hj_centring;
+
 typedef struct {
     int32_t form;          /* hj_form; default HJ_FORM_PLAIN_FP64 */
     int32_t active_dims;   /* stripes split the first active_dims dims into neighbour cells
@@ -103,7 +120,9 @@ typedef struct {
                               the tensor-core forms, 16 for the plain form). Smaller chunks
                               balance small joins across the SMs, larger ones keep B tiles in
                               L2; hilbertjoin_b200.autotune picks it per dimension. */
-    uint64_t reserved[2];
+    int32_t tc_centring;   /* hj_centring; 0 = HJ_CENTRING_AUTO */
+    int32_t reserved_i;
+    uint64_t reserved[1];
 } hj_opts;
 
 /* Per-call statistics (all optional). Times are device times of each stage
@@ -130,7 +149,7 @@ typedef struct {
     int32_t form_used;      /* hj_form actually run */
     int32_t stripes;        /* stripe count (3^s+1)/2 for self-joins, 3^s for two-set joins */
     int32_t kernel_launches;/* kernels this call launched */
-    int32_t reserved_i;
+    int32_t tc_centring;    /* hj_centring the tensor-core kernel ran with (0: no tensor-core kernel) */
     double reorder_ms;      /* dimension cost sampling and ordering (opts.reorder_dims) */
     uint64_t reserved[3];
 } hj_stats;
@@ -256,6 +275,12 @@ HJ_API void hj_test_ego_loop3_noself(const size_t nA, const size_t nB, const int
  * Not thread-safe; no reference counterpart. */
 HJ_API int hj_debug_tc_estimates(const float *A, uint64_t nA, const float *B, uint64_t nB, uint32_t d, int form,
                                  float *out);
+/* As hj_debug_tc_estimates with the operand centring (hj_centring) and eps
+ * given (eps <= 0: the one that puts all points in one cell); pairs outside
+ * the work list are left NaN. Statistics of the join into *stats if non-null.
+ * Not thread-safe; no reference counterpart. */
+HJ_API int hj_debug_tc_estimates_ex(const float *A, uint64_t nA, const float *B, uint64_t nB, uint32_t d, int form,
+                                    int centring, double eps, float *out, hj_stats *stats);
 
 /* Testing hook: with gate_ns > 0, every following tensor-core kernel launch
  * of this process makes its epilogue wait gate_ns on a device barrier that
