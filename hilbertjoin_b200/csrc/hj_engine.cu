@@ -139,8 +139,8 @@ enum {
     kSlotTf32A, kSlotTf32B, kSlotHiA, kSlotLoA, kSlotHiB, kSlotLoB, kSlotNormA, kSlotNormB,
     kSlotTmaxAA, kSlotTmaxAB, kSlotTmaxBA, kSlotTmaxBB, kSlotBand, kSlotCenter, kSlotGminA, kSlotGminB,
     kSlotItemCnt, kSlotPairKeys, kSlotPairPerm, kSlotPairTmp, kSlotPairHist, kSlotPairOut, kSlotDimCost,
-    kSlotGridOrd, kSlotBcOpA, kSlotBcOpB, kSlotBcNormA, kSlotBcNormB, kSlotBcXnA, kSlotBcXnB, kSlotBcGminA,
-    kSlotBcGminB, kSlotBcBlkA, kSlotBcBlkB, kSlotBcCentA, kSlotBcCentB,
+    kSlotGridOrd, kSlotBcOpA, kSlotBcOpB, kSlotBcNormA, kSlotBcNormB, kSlotBcXnA, kSlotBcXnB, kSlotBcBlkA,
+    kSlotBcBlkB, kSlotBcCentA, kSlotBcCentB,
     kSlotEngineEnd
 };
 static_assert(kSlotEngineEnd <= kSlotIndexFirst, "engine slots overlap the index stage's");
@@ -321,25 +321,23 @@ static int ensure_plain_tiles(Ctx *c, cudaStream_t st, SortedSet *s, bool is_b, 
 
 // Per-block-centred FP16 operands of a sorted set (HJ_CENTRING_BLOCK): the A
 // layout for a join's set A, the B layout for its set B, both for a self-join
-// (is_b false, with_b true); p and |h| per rank, group minima of p (B side),
-// block summaries and centres.
+// (is_b false, with_b true); q and |h| per rank, block summaries and centres.
+// scale = the global form's operand scale times 2^-kBcScaleShift.
 static int prepare_block_centring(Ctx *c, cudaStream_t st, SortedSet *s, bool with_a, bool with_b, bool is_b,
-                                  const double *center, double op_scale, int *launches) {
+                                  const double *center, double scale, int *launches) {
     const uint64_t npad = s->npad_tc, nblk = npad / kBcBlock;
-    s->kpad_bc = tc_atoms(HJ_FORM_TC_FP16, 3 * s->d) * 64;
+    s->kpad_bc = tc_atoms(HJ_FORM_TC_FP16, bc_cols(s->d)) * 64;
     s->bc_op_a = with_a ? (uint16_t *)slot_alloc_impl(c, st, kSlotBcOpA, npad * s->kpad_bc * 2) : nullptr;
     s->bc_op_b = with_b ? (uint16_t *)slot_alloc_impl(c, st, kSlotBcOpB, npad * s->kpad_bc * 2) : nullptr;
     s->bc_norms = (float *)slot_alloc_impl(c, st, is_b ? kSlotBcNormB : kSlotBcNormA, npad * 4);
     s->bc_xn = (float *)slot_alloc_impl(c, st, is_b ? kSlotBcXnB : kSlotBcXnA, npad * 4);
-    s->bc_gmin = with_b ? (float *)slot_alloc_impl(c, st, is_b ? kSlotBcGminB : kSlotBcGminA, (npad / 32) * 4)
-                        : nullptr;
     s->bc_blk = (float4 *)slot_alloc_impl(c, st, is_b ? kSlotBcBlkB : kSlotBcBlkA, nblk * sizeof(float4));
     s->bc_cent = (float *)slot_alloc_impl(c, st, is_b ? kSlotBcCentB : kSlotBcCentA, nblk * kBcCentStride * 4);
-    if ((with_a && !s->bc_op_a) || (with_b && (!s->bc_op_b || !s->bc_gmin)) || !s->bc_norms || !s->bc_xn ||
-        !s->bc_blk || !s->bc_cent)
+    if ((with_a && !s->bc_op_a) || (with_b && !s->bc_op_b) || !s->bc_norms || !s->bc_xn || !s->bc_blk ||
+        !s->bc_cent)
         return fail(HJ_ERR_OOM, "out of device memory (block-centred operands)");
-    launch_bc_prepare(*s, center, op_scale, s->bc_op_a, s->bc_op_b, s->bc_norms, s->bc_xn, s->bc_blk, s->bc_cent,
-                      s->bc_gmin, st, launches);
+    launch_bc_prepare(*s, center, scale, s->bc_op_a, s->bc_op_b, s->bc_norms, s->bc_xn, s->bc_blk, s->bc_cent, st,
+                      launches);
     return check_cuda("block-centred operands");
 }
 
@@ -579,19 +577,28 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
         // send more than an eighth of the block pairs to the FP64 kernel.
         const int centring = opts ? opts->tc_centring : HJ_CENTRING_AUTO;
         const bool bc_ok = form == HJ_FORM_TC_FP16 && d <= kBcMaxDim;
+        const double bc_scale = std::ldexp(A.op_scale, -kBcScaleShift);
         auto enable_bc = [&]() -> int {
-            if (int r = prepare_block_centring(c, st, &A, true, in.self, false, A.center, A.op_scale, &launches))
+            if (int r = prepare_block_centring(c, st, &A, true, in.self, false, A.center, bc_scale, &launches))
                 return r;
             if (in.self) {
-                B.bc_op_b = A.bc_op_b, B.bc_norms = A.bc_norms, B.bc_xn = A.bc_xn, B.bc_gmin = A.bc_gmin;
+                B.bc_op_b = A.bc_op_b, B.bc_norms = A.bc_norms, B.bc_xn = A.bc_xn;
                 B.bc_blk = A.bc_blk, B.bc_cent = A.bc_cent, B.kpad_bc = A.kpad_bc;
-            } else if (int r = prepare_block_centring(c, st, &B, false, true, true, B.center, B.op_scale,
+            } else if (int r = prepare_block_centring(c, st, &B, false, true, true, B.center, bc_scale,
                                                       &launches)) {
                 return r;
             }
             bc = true;
-            bck = bc_constants(d, T, A.op_scale);
+            bck = bc_constants(d, T, bc_scale);
             return HJ_OK;
+        };
+        // the job in the units of the operands in use (block centring: its own
+        // scale and 3d + 3 columns)
+        auto fill_job = [&]() {
+            fill_tc_job(c->h_job, form, d, T, bc ? bc_scale : A.op_scale, maxabs, 0, na_eff, 0, nb_eff, in.self,
+                        d_count, A.rows, B.rows, &c_rel, &c_abs);
+            if (bc) c->h_job->ka = tc_atoms(form, bc_cols(d));
+            cudaMemcpyAsync(c->d_job, c->h_job, sizeof(TcJob), cudaMemcpyHostToDevice, st);
         };
         if (centring == HJ_CENTRING_BLOCK) {
             if (!bc_ok) return fail(HJ_ERR_UNSUPPORTED, "per-block centring needs the FP16 form and d <= 64");
@@ -599,10 +606,7 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
         }
         // the FP16 form works in scaled units: norms, eps^2 and the bound times op_scale^2
         // one-entry job table: counted ranks, thresholds and bound in the operand units
-        fill_tc_job(c->h_job, form, d, T, A.op_scale, maxabs, 0, na_eff, 0, nb_eff, in.self, d_count, A.rows,
-                    B.rows, &c_rel, &c_abs);
-        if (bc) c->h_job->ka = tc_atoms(form, 3 * d);
-        cudaMemcpyAsync(c->d_job, c->h_job, sizeof(TcJob), cudaMemcpyHostToDevice, st);
+        fill_job();
         const double T_tc = T * A.op_scale * A.op_scale;
         // Items whose error band would exceed half of eps^2 (eps^2 tiny against
         // the squared norms: the cancellation limit of the norm expansion) run
@@ -613,7 +617,9 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
         // bounded by its residuals, and tiles up to 4 eps^2 (wide clusters,
         // blocks that straddle two clusters) cost less as band pairs than on the
         // FP64 kernel.
-        auto route_limit = [&](int attempt) { return attempt == 0 ? (bc ? 4.0 : 0.5) * T_tc : -1.0; };
+        auto route_limit = [&](int attempt) {
+            return attempt > 0 ? -1.0 : bc ? 4.0 * T * bc_scale * bc_scale : 0.5 * T_tc;
+        };
         for (int attempt = 0;; ++attempt) {
             int sr = split_items_by_precision(idx, A, B, c_rel, c_abs, route_limit(attempt), bc ? &bck : nullptr,
                                               slot_alloc_cb, &actx, st, &idx_tc, &idx_fp);
@@ -624,8 +630,7 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
                 idx_fp.tile_pairs * 8 > idx.tile_pairs) {
                 // the split synchronised the stream: the job's first copy is done
                 if (int r = enable_bc()) return r;
-                c->h_job->ka = tc_atoms(form, 3 * d);
-                cudaMemcpyAsync(c->d_job, c->h_job, sizeof(TcJob), cudaMemcpyHostToDevice, st);
+                fill_job();
                 sr = split_items_by_precision(idx, A, B, c_rel, c_abs, route_limit(attempt), &bck, slot_alloc_cb,
                                               &actx, st, &idx_tc, &idx_fp);
                 if (sr == 2) return fail(HJ_ERR_OOM, "out of device memory (work list split)");
@@ -1057,9 +1062,9 @@ uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dt
         b += n * (2 * W + 1) * 4 + n * 8;                     // packed keys (both layouts), permutation
         b += npad * d * 8;                                    // plain FP64 tiles (plain form or routed items)
         if (tc) b += npad * (hj_ceil_div(d, 64) * 64) * 4 + npad * 8;  // operands (widest form), norms
-        if (tc && d <= kBcMaxDim) {  // block-centred operands (both layouts), p, |h|, minima, blocks
-            const uint64_t kbc = hj_ceil_div(3 * d, 64) * 64;
-            b += npad * kbc * 4 + npad * 12 + (npad / kBcBlock) * (16 + kBcCentStride * 4);
+        if (tc && d <= kBcMaxDim) {  // block-centred operands (both layouts), q, |h|, blocks
+            const uint64_t kbc = hj_ceil_div(bc_cols(d), 64) * 64;
+            b += npad * kbc * 4 + npad * 8 + (npad / kBcBlock) * (16 + kBcCentStride * 4);
         }
         return b;
     };

@@ -106,46 +106,51 @@ struct SortedSet {
     uint64_t npad_tc = 0;
     uint32_t kpad_tf32 = 0, kpad_bf16 = 0;
     // per-block centring of the FP16 operands (HJ_CENTRING_BLOCK; see BcConsts):
-    // [npad][kpad_bc] rows in the A layout [h | h | c] and the B layout [h | c | h]
+    // [npad][kpad_bc] rows in the A layout [h | h | c | 2^k] and the B layout [h | c | h | q/2]
     uint16_t *bc_op_a = nullptr, *bc_op_b = nullptr;
-    float *bc_norms = nullptr;    // p = |h|^2 + 2 h.c per rank (FP32; padding rows kPadNorm)
+    float *bc_norms = nullptr;    // q = |h|^2 + 2 h.c per rank (FP32; padding rows kPadNorm)
     float *bc_xn = nullptr;       // |h| per rank, rounded up
-    float *bc_gmin = nullptr;     // per 32-rank group: min p
-    float4 *bc_blk = nullptr;     // per 128-rank block: {max |h|, |c|, max |p|, 0}, rounded up
+    float4 *bc_blk = nullptr;     // per 128-rank block: {max |h|, |c|, max |q|, 0}, rounded up
     float *bc_cent = nullptr;     // per block: c in FP32 (FP16 values), kBcCentStride floats, zero padded
     uint32_t kpad_bc = 0;
 };
 
 // Per-block centring of the FP16 operands. Every 128-rank block of a sorted
 // set (one A tile, half a B tile) gets a centre c whose coordinates are FP16
-// values in the operand units ((x - center) * op_scale), the midpoint of the
-// block's range rounded to FP16; every rank is stored as that centre plus its
-// residual h = fl16(x - c). Operand rows hold 3d columns,
-//     A: [h | h | c]      B: [h | c | h],
-// so that one MMA gives v_ij = h_i.h_j + h_i.c_j + c_i.h_j = x'_i.x'_j - c_i.c_j
-// for the operand points x' = c + h, and
-//     dist2(x'_i, x'_j) = p_i + p_j + |c_i - c_j|^2 - 2 v_ij,  p = |h|^2 + 2 h.c.
-// The only rounding of the points is h's (relative 2^-11 per coordinate): it
-// moves a point by rho <= 2^-11 |h| (plus the subnormal floor), and distances
-// by rho_i + rho_j. The error bound of s = p_i + p_j + D - 2 v (bc_tau) is
-// therefore linear in the residual norms instead of quadratic in the distance
-// from one global centre, which keeps clustered data with eps far below its
-// spread on the tensor cores.
+// values in the operand units ((x - center) * scale, the largest coordinate
+// below 2^10), the midpoint of the block's range rounded to FP16; every rank
+// is stored as that centre plus its residual h = fl16(x - c). With
+// q = |h|^2 + 2 h.c per rank, operand rows hold 3d + 3 columns,
+//     A: [h | h | c | -2^15 -2^4 -2^-7]      B: [h | c | h | m1 m2 m3],
+// m1 2^15 + m2 2^4 + m3 2^-7 = q / 2 (three FP16 pieces, to 2^-33 |q|), so
+// that one MMA gives, for the operand points x' = c + h,
+//     w_ij = h_i.h_j + h_i.c_j + c_i.h_j - q_j / 2 = x'_i.x'_j - c_i.c_j - q_j / 2,
+//     dist2(x'_i, x'_j) = q_i + |c_i - c_j|^2 - 2 w_ij.
+// The accumulator alone orders the columns of a row (no per-column norm), so
+// the epilogue's maximum over 32 columns is exact. The only rounding of the
+// points is h's (relative 2^-11 per coordinate): it moves a point by
+// rho <= 2^-11 |h| (plus the subnormal floor), and distances by rho_i + rho_j.
+// The error bound (bc_tau) is therefore linear in the residual norms instead
+// of quadratic in the distance from one global centre, which keeps clustered
+// data with eps far below its spread on the tensor cores.
 constexpr uint32_t kBcBlock = 128;      // ranks per centring block (= kTcTileA, = kTcTileB / 2)
-constexpr uint32_t kBcMaxDim = 64;      // 3d <= 192 operand columns
+constexpr uint32_t kBcMaxDim = 64;      // 3d + 3 <= 195 operand columns
 constexpr uint32_t kBcCentStride = 64;  // floats per block in bc_cent
+constexpr int kBcScaleShift = 5;        // operand scale of the global form times 2^-5
+inline uint32_t bc_cols(uint32_t d) { return 3 * d + 3; }
 struct BcConsts {
-    float kp21;     // 2 kpad_bc 2^-22: the MMA accumulation error of v per unit of S, doubled for s
+    float kp21;     // 2 kpad_bc 2^-22: the MMA accumulation error of w per unit of S, doubled for s
     float eps;      // eps in operand units, rounded up
     float rho_u;    // rounding radius per unit of |h| (2^-11 with margin)
     float rho_c;    // rounding radius floor (FP16 subnormals, FP64 shift), per point
-    float u_norm;   // FP32 rounding of p (relative, with margin)
+    float u_norm;   // FP32 rounding of q, and the FP16 split of q / 2 (relative, with margin)
     float u_d;      // FP32 rounding of D = |c_i - c_j|^2 (relative)
     float theta_t;  // rounding of the FP64 pair test near eps^2, twice, in operand units
 };
 // Half-width of the band of s around eps^2 for a pair of a row (|h| = xa, its
-// block's |c| = ca, |p| = pa) and a B block (max |h| = xb, |c| = cb, max |p| =
-// qb) at block-centre distance^2 D; *S_out = the bound on sum_k |A_ik B_jk|.
+// block's |c| = ca, |q| = pa) and a B block (max |h| = xb, |c| = cb, max |q| =
+// qb) at block-centre distance^2 D; *S_out = the bound on sum_k |A_ik B_jk|
+// (Cauchy-Schwarz per column group, and |q_j| / 2 for the folded pieces).
 // With E = |s - dist2(x'_i, x'_j)| <= kp21 S + u_norm (pa + qb) + u_d D and
 // rho = rho_i + rho_j: dist2 <= s + E + 2 rho sqrt(s + E) + rho^2, and
 // 2 rho sqrt(E) <= rho^2 + E, so near eps^2 the FP64 test agrees with
@@ -154,7 +159,7 @@ struct BcConsts {
 // function).
 __host__ __device__ inline float bc_tau(float xa, float ca, float pa, float xb, float cb, float qb, float D,
                                         const BcConsts &k, float *S_out) {
-    const float S = fmaf(xa, xb + cb, ca * xb);
+    const float S = fmaf(xa, xb + cb, fmaf(ca, xb, 0.5005f * qb));
     const float rho = fmaf(k.rho_u, xa + xb, 2.0f * k.rho_c);
     const float E = fmaf(k.kp21, S, fmaf(k.u_norm, pa + qb, k.u_d * D));
     if (S_out) *S_out = S;
@@ -163,12 +168,11 @@ __host__ __device__ inline float bc_tau(float xa, float ca, float pa, float xb, 
 // Fills the constants for dimension d, eps^2 = T (caller units) and the FP16
 // operand scale.
 BcConsts bc_constants(uint32_t d, double T, double op_scale);
-// Block centres, residual operands (A and/or B layout; null skips one), p, |h|
-// and block summaries of a sorted set from its sorted rows; then the group
-// minima of p when gmin is non-null. centre = the global per-dim shift.
-void launch_bc_prepare(const SortedSet &s, const double *center, double op_scale, uint16_t *op_a, uint16_t *op_b,
-                       float *norms, float *xn, float4 *blk, float *cent, float *gmin, cudaStream_t st,
-                       int *launches);
+// Block centres, residual operands (A and/or B layout; null skips one), q, |h|
+// and block summaries of a sorted set from its sorted rows. center = the
+// global per-dim shift, scale = the block-centred operand scale.
+void launch_bc_prepare(const SortedSet &s, const double *center, double scale, uint16_t *op_a, uint16_t *op_b,
+                       float *norms, float *xn, float4 *blk, float *cent, cudaStream_t st, int *launches);
 
 constexpr float kPadNorm = 1.0e30f;
 

@@ -100,8 +100,9 @@ struct TcArgs {
     const uint32_t *perm_a, *perm_b;  // EGO rank -> input index (for dbg)
     uint64_t gate_ns;               // test hook: > 0 makes the epilogue wait this long on a barrier
                                     // that nothing arrives on, then raise kErrTimeout
-    // per-block centring (BC kernels): norm_a / norm_b / gmin_b are then p and its
-    // group minima; |h| of the A rows, block summaries and centres of both sets
+    // per-block centring (BC kernels): norm_a is then q of the A rows (norm_b and
+    // gmin_b unused: the accumulator holds w = v - q_j / 2); |h| of the A rows,
+    // block summaries and centres of both sets
     const float *xn_a;
     const float4 *blk_a, *blk_b;
     const float *cent_a, *cent_b;
@@ -428,9 +429,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         float pf_gmin[kEpiVec];
         auto prefetch = [&](uint32_t b) {
             const uint64_t g = (uint64_t)b * kTcTileB + half * kEpiCols;
-            const float4 m = __ldg(reinterpret_cast<const float4 *>(p.gmin_b + g / 32));
-            pf_gmin[0] = m.x, pf_gmin[1] = m.y, pf_gmin[2] = m.z, pf_gmin[3] = m.w;
-            if constexpr (BC) {
+            if constexpr (!BC) {
+                const float4 m = __ldg(reinterpret_cast<const float4 *>(p.gmin_b + g / 32));
+                pf_gmin[0] = m.x, pf_gmin[1] = m.y, pf_gmin[2] = m.z, pf_gmin[3] = m.w;
+            } else {
                 const uint64_t blkb = g / kBcBlock;
                 pf_blk = __ldg(p.blk_b + blkb);
                 pf_cb[0] = __ldg(p.cent_b + blkb * kBcCentStride + lane);
@@ -504,7 +506,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if constexpr (BC) {
                 // this tile's B block: D = |c_A - c_B|^2 (FP32, lanes over the
                 // dims), the band half-width of the lane's row against the block,
-                // and the thresholds on t = p_j - 2 v (s = p_row + D + t)
+                // and the thresholds on t = -2 w (s = q_row + D + t; |w| <= S)
                 float D = 0.f;
 #pragma unroll
                 for (int m = 0; m < 2; ++m) {
@@ -576,7 +578,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         uint32_t rows = __ballot_sync(0xffffffffu, need);
                         if (!rows) continue;
                         const int cb = (int)(c * kChunkCols + h2 * 32);
-                        const float nbl = __ldg(p.norm_b + gj0 + cb + lane);
+                        // the column's |b|^2 (block centring: 0, q_j / 2 is in the accumulator)
+                        const float nbl = BC ? 0.f : __ldg(p.norm_b + gj0 + cb + lane);
                         // columns that may be counted at all: gj < nb, and gj > gi for a self-join
                         int jlo = 0, jhi = kEpiCols;
                         {
@@ -597,7 +600,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                             uint32_t bbits = 0, c32 = 0;
 #pragma unroll
                             for (int j = 0; j < 32; ++j) {
-                                const float t = fmaf(-2.0f, vg[j], __shfl_sync(0xffffffffu, nbl, j));
+                                const float t = fmaf(-2.0f, vg[j], BC ? 0.f : __shfl_sync(0xffffffffu, nbl, j));
                                 const bool ok = mine && (unsigned)(cb + j - jlo) < (unsigned)(jhi - jlo);
                                 c32 += (ok && t <= thr_in) ? 1u : 0u;
                                 bbits |= (ok && t > thr_in && t <= thr_out) ? (1u << j) : 0u;
@@ -855,13 +858,14 @@ uint32_t tc_atoms(int form, uint32_t kcols) { return tc_layout(form, kcols).ka; 
 //   rho_c: subnormal FP16 (|h| < 2^-14) is off by at most 2^-25 per
 //     coordinate, and the FP64 shift (x - center) * scale by 2^-52 of 2^15:
 //     sqrt(d) (2^-25 + 2^-37), doubled;
-//   u_norm: p rounded once from FP64 to FP32 (2^-24 relative), doubled;
+//   u_norm: q rounded once from FP64 to FP32 (2^-24 relative), doubled, and
+//     the split of q / 2 into FP16 pieces (2^-34 relative);
 //   u_d: D in FP32, two FMAs per lane and a five-step sum of the lanes, with
 //     the differences of FP16 values exact or rounded once: 16 * 2^-24;
 //   theta_t: the FP64 pair test sums d squares of exact differences with FMAs,
 //     relative error below (d + 2) 2^-53 of dist2 ~ eps^2: 2 (d + 2) 2^-53 T.
 BcConsts bc_constants(uint32_t d, double T, double op_scale) {
-    const double s2 = op_scale * op_scale, kpad = (double)tc_atoms(HJ_FORM_TC_FP16, 3 * d) * 64.0;
+    const double s2 = op_scale * op_scale, kpad = (double)tc_atoms(HJ_FORM_TC_FP16, bc_cols(d)) * 64.0;
     auto up = [](double v) {
         const float f = (float)v;
         return (double)f >= v ? f : std::nextafter(f, INFINITY);
@@ -871,9 +875,10 @@ BcConsts bc_constants(uint32_t d, double T, double op_scale) {
     k.eps = up(std::sqrt(T * s2) * (1.0 + 1e-12));
     k.rho_u = up(1.001 * std::ldexp(1.0, -11));
     k.rho_c = up(2.0 * std::sqrt((double)d) * (std::ldexp(1.0, -25) + std::ldexp(1.0, -37)));
-    k.u_norm = up(std::ldexp(1.0, -23));
+    k.u_norm = up(std::ldexp(1.0, -23) + std::ldexp(1.0, -33));
     k.u_d = up(16.0 * std::ldexp(1.0, -24));
-    k.theta_t = up(2.0 * (d + 2.0) * std::ldexp(1.0, -53) * T * s2);
+    // + the absolute floor of the q / 2 split (2^-32 in w, 2^-31 in s, twice in tau)
+    k.theta_t = up(2.0 * (d + 2.0) * std::ldexp(1.0, -53) * T * s2 + std::ldexp(1.0, -29));
     return k;
 }
 
@@ -918,7 +923,7 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
         *err = "per-block centring needs the FP16 form, d <= 64 and the centred layouts";
         return 1;
     }
-    const TcLayout L = tc_layout(form, bc ? 3 * A.d : A.d);
+    const TcLayout L = tc_layout(form, bc ? bc_cols(A.d) : A.d);
     if (L.nst < 2) {
         *err = "dimension too large for the tensor-core kernel";
         return 1;
@@ -970,8 +975,8 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
     a.gate_ns = g_gate_ns;
     if (bc) {
         a.norm_a = A.bc_norms;
-        a.norm_b = B.bc_norms;
-        a.gmin_b = B.bc_gmin;
+        a.norm_b = nullptr;  // q_j / 2 is folded into the accumulator
+        a.gmin_b = nullptr;
         a.tmax_b = nullptr;
         a.xn_a = A.bc_xn;
         a.blk_a = A.bc_blk;

@@ -967,14 +967,18 @@ __global__ void k_group_min(const float *__restrict__ v, uint64_t npad, int grou
 
 // One CUDA block per 128-rank block of a sorted set (kBcBlock threads). The
 // block's rows are read once (contiguous in the sorted layout), shifted and
-// scaled as the global FP16 operands are ((x - center) * scale in FP64), and
-// kept in shared memory; per dim the midpoint of the block's range, rounded to
-// FP16, is the centre c; every rank's residual h = fl16(x - c) (round to
-// nearest, once), p = |h|^2 + 2 h.c from the FP16 values in FP64, |h|; then the
-// operand rows (A: [h | h | c], B: [h | c | h], zero padded to kpad) are
-// written as 16-byte chunks, consecutive threads on consecutive chunks.
-// Ranks past n (up to npad) are padding: zero operands, p = kPadNorm, |h| = 0.
-// |h_t| <= (max - min) / 2 + 2^-11 |c_t| < 2^15 (1 + 2^-11): no FP16 overflow.
+// scaled ((x - center) * scale in FP64, the largest coordinate below 2^10),
+// and kept in shared memory; per dim the midpoint of the block's range,
+// rounded to FP16, is the centre c; every rank's residual h = fl16(x - c)
+// (round to nearest, once), q = |h|^2 + 2 h.c from the FP16 values in FP64,
+// and |h|; then the operand rows (zero padded to kpad) are written as 16-byte
+// chunks, consecutive threads on consecutive chunks:
+//     A: [h | h | c | -2^15 -2^4 -2^-7]      B: [h | c | h | m1 m2 m3]
+// with q / 2 = 2^15 m1 + 2^4 m2 + 2^-7 m3 + r: m1 = fl16(q / 2^16), m2 and
+// m3 the FP16 of the exact remainders, |r| <= 2^-33 |q| + 2^-32. Bounds: with
+// |x - center| * scale < 2^10 per coordinate, |h_t| < 2^10 (1 + 2^-11) and
+// |q| < 3 2^20 d <= 3 2^26, so every piece is below 2^12 in magnitude.
+// Ranks past n (up to npad) are padding: zero operands, q = kPadNorm, |h| = 0.
 template <typename T>
 __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ rows, uint64_t n, uint32_t d,
                                                          const double *__restrict__ center, double scale,
@@ -982,8 +986,9 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
                                                          uint16_t *__restrict__ op_b, float *__restrict__ norms,
                                                          float *__restrict__ xn, float4 *__restrict__ blk,
                                                          float *__restrict__ cent) {
-    extern __shared__ double bc_sm[];  // [kBcBlock][d] shifted coordinates, then residuals; [d] centre
+    extern __shared__ double bc_sm[];  // [kBcBlock][d] shifted coordinates, then residuals; [d] centre; [kBcBlock][3] q pieces
     double *cs = bc_sm + (size_t)kBcBlock * d;
+    double *qp = cs + d;
     __shared__ float red_x[kBcBlock / 32], red_p[kBcBlock / 32];
     const uint64_t r0 = (uint64_t)blockIdx.x * kBcBlock;
     const uint32_t nr = r0 >= n ? 0u : (n - r0 < kBcBlock ? (uint32_t)(n - r0) : kBcBlock);
@@ -1002,6 +1007,7 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
     __syncthreads();
     const uint32_t r = threadIdx.x;
     float my_x = 0.f, my_p = 0.f;
+    double m1 = 0.0, m2 = 0.0, m3 = 0.0;
     if (r < nr) {
         double hh = 0.0, hc = 0.0;
         for (uint32_t t = 0; t < d; ++t) {
@@ -1010,15 +1016,24 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
             hh = fma(h, h, hh);
             hc = fma(h, cs[t], hc);
         }
-        const double p = fma(2.0, hc, hh);
-        norms[r0 + r] = (float)p;
-        my_p = fabsf((float)p) * (1.0f + 2.4e-7f);
+        const double q = fma(2.0, hc, hh);
+        norms[r0 + r] = (float)q;
+        my_p = fabsf((float)q) * (1.0f + 2.4e-7f);
         my_x = (float)sqrt(hh) * (1.0f + 2.4e-7f);
         if (xn) xn[r0 + r] = my_x;
+        const double v1 = 0.5 * q;
+        m1 = (double)__half2float(__double2half(v1 * 0x1p-15));
+        const double v2 = v1 - m1 * 0x1p15;
+        m2 = (double)__half2float(__double2half(v2 * 0x1p-4));
+        const double v3 = v2 - m2 * 0x1p4;
+        m3 = (double)__half2float(__double2half(v3 * 0x1p7));
     } else {
         norms[r0 + r] = kPadNorm;
         if (xn) xn[r0 + r] = 0.f;
     }
+    qp[3 * r] = m1;
+    qp[3 * r + 1] = m2;
+    qp[3 * r + 2] = m3;
     __syncthreads();
     const uint32_t cpr = kpad / 8;  // 16-byte chunks per operand row
     for (uint32_t e = threadIdx.x; e < kBcBlock * cpr; e += kBcBlock) {
@@ -1040,6 +1055,10 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
                     } else if (k < 3 * d) {
                         av = cs[k - 2 * d];
                         bv = bc_sm[rr * d + k - 2 * d];
+                    } else if (k < 3 * d + 3) {
+                        const uint32_t u = k - 3 * d;
+                        av = u == 0 ? -0x1p15 : (u == 1 ? -0x1p4 : -0x1p-7);
+                        bv = qp[3 * rr + u];
                     }
                 }
                 // FP16 values already: the conversions are exact
@@ -1053,7 +1072,7 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
         if (op_a) reinterpret_cast<uint4 *>(op_a)[o] = make_uint4(wa[0], wa[1], wa[2], wa[3]);
         if (op_b) reinterpret_cast<uint4 *>(op_b)[o] = make_uint4(wb[0], wb[1], wb[2], wb[3]);
     }
-    // block summaries: max |h|, |c|, max |p| (all rounded up)
+    // block summaries: max |h|, |c|, max |q| (all rounded up)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         my_x = fmaxf(my_x, __shfl_xor_sync(0xffffffffu, my_x, o));
@@ -1078,27 +1097,22 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
     }
 }
 
-void launch_bc_prepare(const SortedSet &s, const double *center, double op_scale, uint16_t *op_a, uint16_t *op_b,
-                       float *norms, float *xn, float4 *blk, float *cent, float *gmin, cudaStream_t st,
-                       int *launches) {
+void launch_bc_prepare(const SortedSet &s, const double *center, double scale, uint16_t *op_a, uint16_t *op_b,
+                       float *norms, float *xn, float4 *blk, float *cent, cudaStream_t st, int *launches) {
     if (s.npad_tc == 0) return;
     const unsigned blocks = (unsigned)(s.npad_tc / kBcBlock);
-    const size_t smem = ((size_t)kBcBlock * s.d + s.d) * sizeof(double);
+    const size_t smem = ((size_t)kBcBlock * s.d + s.d + 3 * kBcBlock) * sizeof(double);
+    const int smem_max = (int)(((size_t)kBcBlock * kBcMaxDim + kBcMaxDim + 3 * kBcBlock) * sizeof(double));
     if (s.dtype_bytes == 8) {
-        ensure_max_dynamic_smem((const void *)k_bc_prepare<double>, (int)((kBcBlock + 1) * kBcMaxDim * 8));
+        ensure_max_dynamic_smem((const void *)k_bc_prepare<double>, smem_max);
         k_bc_prepare<double><<<blocks, kBcBlock, smem, st>>>(static_cast<const double *>(s.rows), s.n, s.d, center,
-                                                             op_scale, s.kpad_bc, op_a, op_b, norms, xn, blk, cent);
+                                                             scale, s.kpad_bc, op_a, op_b, norms, xn, blk, cent);
     } else {
-        ensure_max_dynamic_smem((const void *)k_bc_prepare<float>, (int)((kBcBlock + 1) * kBcMaxDim * 8));
+        ensure_max_dynamic_smem((const void *)k_bc_prepare<float>, smem_max);
         k_bc_prepare<float><<<blocks, kBcBlock, smem, st>>>(static_cast<const float *>(s.rows), s.n, s.d, center,
-                                                            op_scale, s.kpad_bc, op_a, op_b, norms, xn, blk, cent);
+                                                            scale, s.kpad_bc, op_a, op_b, norms, xn, blk, cent);
     }
-    int L = 1;
-    if (gmin) {
-        k_group_min<<<(unsigned)hj_ceil_div(s.npad_tc / 32, 256), 256, 0, st>>>(norms, s.npad_tc, 32, gmin);
-        ++L;
-    }
-    if (launches) *launches += L;
+    if (launches) *launches += 1;
 }
 
 void launch_gather(const void *x, int dtype_bytes, uint64_t n, uint32_t d, const uint32_t *perm,

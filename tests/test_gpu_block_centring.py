@@ -1,6 +1,7 @@
 """Per-block centring of the FP16 tensor-core operands (HJ_CENTRING_BLOCK):
 every 128-rank block of the EGO order is stored as an FP16 centre plus FP16
-residuals, with the centre cross terms as extra K columns. The counts must be
+residuals, with the centre cross terms and the column's norm as extra K
+columns. The counts must be
 the FP64 counts on every input, including pairs exactly at eps and the
 clustered data that the global centre sends to the FP64 kernel; the estimates
 must sit inside a bound that scales with the residuals."""
@@ -168,8 +169,8 @@ def test_estimates_all_pairs_loose_bound(hj):
         half = 0.5 * (both.max(0) - both.min(0))
         R = float(np.sqrt((half ** 2).sum()))  # |c| <= R (centres inside the box)
         H = 2.0 * R                             # |h| <= diameter of the box
-        kpad = -(-3 * d // 64) * 64
-        S = H * H + 2 * H * R
+        kpad = -(-(3 * d + 3) // 64) * 64
+        S = 1.5 * (H * H + 2 * H * R)           # cross terms and the folded q / 2
         rho = 2 * 2.0 ** -11 * H
         bound = 2 * kpad * 2.0 ** -22 * S + 2 * rho * np.sqrt(ex) + rho * rho + 1e-5 * (1 + ex)
         assert np.isfinite(est).all()
