@@ -108,12 +108,12 @@ struct hj_batch {
 
 static int batch_enqueue(hj_batch *b, cudaStream_t st) {
     cudaMemsetAsync(b->d_counts, 0, b->n_jobs * sizeof(unsigned long long), st);
-    cudaMemsetAsync(b->d_band_total, 0, sizeof(unsigned long long), st);
+    cudaMemsetAsync(b->d_band_total, 0, 2 * sizeof(unsigned long long), st);  // slots reserved, left unused
     cudaMemsetAsync(b->d_err, 0, sizeof(uint32_t), st);
     cudaMemsetAsync(b->d_maxerr, 0, sizeof(unsigned int), st);
     std::string err;
     if (launch_join_tc(b->ops, b->ops, b->form, b->d_jobs, 0, 0, b->idx, b->band, b->band_cap, b->d_band_total,
-                       b->d_err, b->num_sms, st, &err))
+                       b->d_err, b->num_sms, st, &err, nullptr, b->d_band_total + 1))
         return engine_fail(HJ_ERR_CUDA, err);
     launch_recheck(b->d_jobs, b->dtype, b->band, b->d_band_total, b->band_cap, b->d_maxerr, st);
     for (const FpJob &f : b->fp)
@@ -132,13 +132,13 @@ static int batch_finish(hj_batch *b, uint64_t *band_total) {
         return engine_fail(HJ_ERR_CUDA, std::string("batch run: ") + cudaGetErrorString(e));
     }
     uint32_t err = 0;
-    unsigned long long bt = 0;
+    unsigned long long bt[2] = {0, 0};
     cudaMemcpy(&err, b->d_err, sizeof(err), cudaMemcpyDeviceToHost);
-    cudaMemcpy(&bt, b->d_band_total, sizeof(bt), cudaMemcpyDeviceToHost);
+    cudaMemcpy(bt, b->d_band_total, sizeof(bt), cudaMemcpyDeviceToHost);
     if (err & kErrTimeout) return engine_fail(HJ_ERR_TIMEOUT, "a bounded device-side wait timed out");
     if (err) return engine_fail(HJ_ERR_CUDA, "device error word set");
-    if (band_total) *band_total = bt;
-    if (bt > b->band_cap) return engine_fail(HJ_ERR_BAND_OVERFLOW, "band queue overflow");
+    if (band_total) *band_total = bt[0] - std::min(bt[0], bt[1]);  // band pairs: reserved slots less the unused
+    if (bt[0] > b->band_cap) return engine_fail(HJ_ERR_BAND_OVERFLOW, "band queue overflow");
     return HJ_OK;
 }
 
@@ -222,7 +222,7 @@ static int batch_plan(const hj_batch_job *jobs, uint32_t n_jobs, int dtype_bytes
     char *srows = (char *)b->alloc(row_bytes);
     b->d_jobs = (TcJob *)b->alloc(n_jobs * sizeof(TcJob));
     b->d_counts = (unsigned long long *)b->alloc(n_jobs * 8);
-    b->d_band_total = (unsigned long long *)b->alloc(8);
+    b->d_band_total = (unsigned long long *)b->alloc(16);
     b->d_err = (uint32_t *)b->alloc(4);
     b->d_maxerr = (unsigned int *)b->alloc(4);
     if (!hi || (bf && !lo) || !O.norms || !O.tile_maxnorm_a || !O.tile_maxnorm_b || !O.group_minnorm || !srows ||

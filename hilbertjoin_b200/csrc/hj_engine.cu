@@ -559,8 +559,9 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
     uint32_t *d_err = reinterpret_cast<uint32_t *>(c->d_small + 3);
     unsigned long long *d_band = c->d_small + 4;
     unsigned long long *d_count_fp = c->d_small + 6;
+    unsigned long long *d_band_holes = c->d_small + 7;  // band slots reserved but left unused
     cudaMemsetAsync(c->d_small + 2, 0, 5 * sizeof(unsigned long long), st);
-    uint64_t band_total = 0, fp_items = 0;
+    uint64_t band_total = 0, band_holes = 0, fp_items = 0;
     double c_rel = 0, c_abs = 0;
     bool bc = false;  // per-block-centred operands (tensor-core forms)
     BcConsts bck{};
@@ -676,16 +677,19 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
                 if (!band) return fail(HJ_ERR_OOM, "out of device memory (band queue)");
                 cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), st);
                 cudaMemsetAsync(d_band, 0, 2 * sizeof(unsigned long long), st);
+                cudaMemsetAsync(d_band_holes, 0, sizeof(unsigned long long), st);
                 std::string terr;
                 cudaEventRecord(c->ev[6], st);
                 if (launch_join_tc(A, B, form, c->d_job, na_eff, nb_eff, idx_tc, band, cap, d_band, d_err,
-                                   c->num_sms, st, &terr, bc ? &bck : nullptr))
+                                   c->num_sms, st, &terr, bc ? &bck : nullptr, d_band_holes))
                     return fail(HJ_ERR_CUDA, terr);
                 ++launches;
                 cudaEventRecord(c->ev[4], st);
                 cudaMemcpyAsync(c->h_small + 4, d_band, 8, cudaMemcpyDeviceToHost, st);
+                cudaMemcpyAsync(c->h_small + 7, d_band_holes, 8, cudaMemcpyDeviceToHost, st);
                 if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("tensor-core join");
                 band_total = c->h_small[4];
+                band_holes = c->h_small[7];
                 if (band_total <= cap) {
                     launch_recheck(c->d_job, A.dtype_bytes, band, d_band, cap,
                                    reinterpret_cast<unsigned int *>(c->d_small + 5), st);
@@ -732,8 +736,9 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
         stats->tile_pairs = idx.tile_pairs;
         stats->work_items = idx.n_items;
         stats->loadpercent = all > 0 ? 100.0 * (double)idx.candidate_pairs / all : 0.0;
-        stats->band_pairs = band_total;
-        stats->band_fraction = idx.candidate_pairs ? (double)band_total / (double)idx.candidate_pairs : 0.0;
+        const uint64_t band_pairs = band_total - std::min(band_total, band_holes);
+        stats->band_pairs = band_pairs;
+        stats->band_fraction = idx.candidate_pairs ? (double)band_pairs / (double)idx.candidate_pairs : 0.0;
         stats->band_halfwidth_rel = c_rel;
         {
             uint32_t eb = (uint32_t)c->h_small[5];

@@ -283,8 +283,9 @@ void launch_pairs_fp64(const SortedSet &A, const SortedSet &B, bool self, uint64
                        uint32_t *d_err, int num_sms, cudaStream_t st);
 
 // Tensor-core kernel + FP64 recheck of the band. Adds into each job's count;
-// band pair count into *d_band_total (may exceed `band_cap`: then the caller
-// regrows). Band entries are 16 bytes (kBandEntryBytes).
+// band slots reserved into *d_band_total (may exceed `band_cap`: then the
+// caller regrows), of which *d_band_holes were left unused (the recheck skips
+// them). Band entries are 16 bytes (kBandEntryBytes).
 constexpr size_t kBandEntryBytes = 16;
 // One join of a tensor-core launch. A launch runs the work items of one or
 // more jobs (WorkItem.pad = job index) over operand matrices whose rows hold
@@ -318,7 +319,8 @@ void fill_tc_job(TcJob *j, int form, uint32_t d, double T, double op_scale, doub
 // one of 3d columns (tc_atoms).
 int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob *d_jobs, uint64_t na0, uint64_t nb0,
                    const IndexResult &idx, uint2 *band, uint64_t band_cap, unsigned long long *d_band_total,
-                   uint32_t *d_err, int num_sms, cudaStream_t st, std::string *err, const BcConsts *bc = nullptr);
+                   uint32_t *d_err, int num_sms, cudaStream_t st, std::string *err, const BcConsts *bc = nullptr,
+                   unsigned long long *d_band_holes = nullptr);
 // K atoms (128-byte operand column groups) of a form's operand rows of kcols columns.
 uint32_t tc_atoms(int form, uint32_t kcols);
 // FP64 recheck of the band pairs, each against its job's rows and eps^2.

@@ -65,6 +65,10 @@ constexpr int kEpiVec = kEpiCols / 32;  // norms per lane, group minima per warp
 // From this many rows of a 32-column group on, the lanes classify their own
 // rows (32 shuffled column norms) instead of the warp walking row by row.
 constexpr int kDenseRows = 8;
+// Band slots are reserved by each epilogue warp in chunks (one atomic per
+// chunk); slots a warp leaves unused are marked with ia = kBandHole.
+constexpr uint32_t kBandChunk = 256;
+constexpr uint32_t kBandHole = 0xffffffffu;
 // 16 epilogue warps (4 per quadrant) were measured slower: at 18 warps the
 // register cap is 96 (spills) and the static shared memory no longer fits next
 // to the 225 KB operand plan.
@@ -94,7 +98,8 @@ struct TcArgs {
     uint64_t na, nb;                // job 0's counted ranks (debug output only)
     BandEntry *band;
     uint64_t band_cap;
-    unsigned long long *band_total;
+    unsigned long long *band_total;  // slots reserved (chunks of kBandChunk per warp)
+    unsigned long long *band_holes;  // reserved slots left unused (marked kBandHole); may be null
     uint32_t *err;
     float *dbg;                     // optional: s_hat for every pair, input order [na][nb] (tests)
     const uint32_t *perm_a, *perm_b;  // EGO rank -> input index (for dbg)
@@ -452,6 +457,24 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (lane == 0 && wc) atomicAdd(p.jobs[job].count, wc);
             cnt = 0;
         };
+        // the warp's current chunk of band slots [bslot, bend) (warp-uniform);
+        // slot of the entry of rank `rank` among `c` <= 32 new entries
+        unsigned long long bslot = 0, bend = 0;
+        auto band_slot = [&](uint32_t c, uint32_t rank) -> unsigned long long {
+            const unsigned long long rem = bend - bslot;
+            if (c <= rem) {
+                const unsigned long long k = bslot + rank;
+                bslot += c;
+                return k;
+            }
+            unsigned long long nb = 0;
+            if (lane == 0) nb = atomicAdd(p.band_total, (unsigned long long)kBandChunk);
+            nb = __shfl_sync(0xffffffffu, nb, 0);
+            const unsigned long long k = rank < rem ? bslot + rank : nb + (rank - rem);
+            bslot = nb + (c - rem);
+            bend = nb + kBandChunk;
+            return k;
+        };
         auto item_rows = [&](const WorkItem &ww) {
             if (ww.pad != job) {
                 if (job != 0xffffffffu) flush();
@@ -619,11 +642,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                                 __syncwarp();
                                 const uint32_t bm = __shfl_sync(0xffffffffu, bbits, L);
                                 const float naL = __shfl_sync(0xffffffffu, na, L);
-                                const int lead = __ffs(bm) - 1;
-                                unsigned long long base = 0;
-                                if (lane == (uint32_t)lead) base = atomicAdd(p.band_total, (unsigned long long)__popc(bm));
-                                base = __shfl_sync(0xffffffffu, base, lead);
-                                const unsigned long long k = base + __popc(bm & ((1u << lane) - 1u));
+                                const unsigned long long k = band_slot(__popc(bm), __popc(bm & ((1u << lane) - 1u)));
                                 if (((bm >> lane) & 1u) && k < p.band_cap) {
                                     BandEntry e;
                                     e.ia = (uint32_t)(gi - (uint64_t)lane + (uint64_t)L);
@@ -664,11 +683,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                             const bool isb = ok && t > tinL && t <= toutL;
                             const uint32_t bm = __ballot_sync(0xffffffffu, isb);
                             if (bm) {
-                                const int lead = __ffs(bm) - 1;
-                                unsigned long long base = 0;
-                                if (lane == (uint32_t)lead) base = atomicAdd(p.band_total, (unsigned long long)__popc(bm));
-                                base = __shfl_sync(0xffffffffu, base, lead);
-                                const unsigned long long k = base + __popc(bm & ((1u << lane) - 1u));
+                                const unsigned long long k = band_slot(__popc(bm), __popc(bm & ((1u << lane) - 1u)));
                                 if (isb && k < p.band_cap) {
                                     BandEntry e;
                                     e.ia = (uint32_t)giL;
@@ -687,6 +702,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (last_tile && it < p.n_items) item_rows(w);
         }
         if (job != 0xffffffffu) flush();
+        // the unused rest of the warp's band chunk
+        for (unsigned long long k = bslot + lane; k < bend; k += 32)
+            if (k < p.band_cap) {
+                BandEntry e;
+                e.ia = kBandHole;
+                e.jb = 0;
+                e.s_hat = 0.f;
+                e.pad = 0;
+                p.band[k] = e;
+            }
+        if (lane == 0 && bend > bslot && p.band_holes) atomicAdd(p.band_holes, bend - bslot);
     }
     tc_fence_before();
     __syncthreads();
@@ -710,8 +736,8 @@ __global__ void k_recheck(const TcJob *__restrict__ jobs, const BandEntry *__res
         const uint64_t i = i0 + threadIdx.x;
         unsigned long long c = 0;
         uint32_t job = 0xffffffffu;
-        if (i < n) {
-            const BandEntry e = band[i];
+        const BandEntry e = i < n ? band[i] : BandEntry{kBandHole, 0, 0.f, 0};
+        if (e.ia != kBandHole) {
             job = e.pad;
             const TcJob &J = jobs[job];
             const TIn *a = static_cast<const TIn *>(J.rows_a) + (uint64_t)(e.ia - J.a_row0) * J.d;
@@ -917,7 +943,8 @@ void fill_tc_job(TcJob *j, int form, uint32_t d, double T, double op_scale, doub
 
 int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob *d_jobs, uint64_t na0, uint64_t nb0,
                    const IndexResult &idx, uint2 *band, uint64_t band_cap, unsigned long long *d_band_total,
-                   uint32_t *d_err, int num_sms, cudaStream_t st, std::string *err, const BcConsts *bc) {
+                   uint32_t *d_err, int num_sms, cudaStream_t st, std::string *err, const BcConsts *bc,
+                   unsigned long long *d_band_holes) {
     if (idx.n_items == 0) return 0;
     if (bc && (form != HJ_FORM_TC_FP16 || A.d > kBcMaxDim || !A.bc_op_a || !B.bc_op_b)) {
         *err = "per-block centring needs the FP16 form, d <= 64 and the centred layouts";
@@ -968,6 +995,7 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
     a.band = reinterpret_cast<BandEntry *>(band);
     a.band_cap = band_cap;
     a.band_total = d_band_total;
+    a.band_holes = d_band_holes;
     a.err = d_err;
     a.dbg = g_dbg_out;
     a.perm_a = A.perm;
