@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--workload", default="selfjoin", choices=["selfjoin", "serving", "batch", "config"],
                     help="serving: the join-serving stream; config: one benchmark configuration "
                          "(--config) in every form (not the headline line)")
+    ap.add_argument("--prefix", type=int, default=0,
+                    help="--workload config: use only the first N points of each set (no count check)")
     ap.add_argument("--config", default="cfg4_self_4M_d28_gmm64_nbrs100",
                     help="configuration name for --workload config (hilbertjoin_b200.workloads.CONFIGS)")
     ap.add_argument("--requests", type=int, default=2000)
@@ -366,9 +368,12 @@ def run_config(args):
     import hilbertjoin_b200 as hj
     from hilbertjoin_b200 import workloads as W
     a, b, eps = W.config_sets(args.config)
+    if args.prefix:
+        a = np.ascontiguousarray(a[:args.prefix])
+        b = None if b is None else np.ascontiguousarray(b[:args.prefix])
     p = os.path.join(ROOT, "tests", "golden", "config_counts.json")
     want = None
-    if os.path.exists(p):
+    if os.path.exists(p) and not args.prefix:
         with open(p) as f:
             fx = json.load(f)["configs"].get(args.config)
         want = None if fx is None else int(fx["oracle_count"])
@@ -398,7 +403,8 @@ def run_config(args):
                      **{k: st[k] for k in ("sort_ms", "index_ms", "join_ms", "kernel_ms", "recheck_ms",
                                            "candidate_pairs", "work_items", "fp64_items", "band_pairs",
                                            "form_used", "kernel_launches")}}
-    print(json.dumps({"workload": args.config, "eps": eps, "oracle_count_fixture": want, "forms": out}), flush=True)
+    print(json.dumps({"workload": args.config, "prefix": args.prefix or None, "eps": eps,
+                      "oracle_count_fixture": want, "forms": out}), flush=True)
 
 
 def main():

@@ -667,9 +667,9 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
                 break;
             }
             const uint64_t cand_tc = idx_tc.tile_pairs * (uint64_t)kTcTileA * kTcTileB;
-            // first band queue: 1/4096 of the candidates (1/1024 with block
+            // first band queue: 1/4096 of the candidates (1/512 with block
             // centres, whose wider tiles stay on the tensor cores)
-            uint64_t cap = std::max<uint64_t>(1ull << 20, cand_tc / (bc ? 1024 : 4096));
+            uint64_t cap = std::max<uint64_t>(1ull << 20, cand_tc / (bc ? 512 : 4096));
             const uint64_t cap_limit = std::max<uint64_t>(1ull << 27, cand_tc / 64);
             bool done = false, fallback = false;
             for (int grow = 0; grow < 4; ++grow) {
@@ -1081,7 +1081,7 @@ uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dt
     b += tiles * (uint64_t)kMaxCombos * 8 + tiles * 64 * 16;
     if (tc) {
         const double cand = (double)na * (double)nb;
-        b += (uint64_t)std::max(1048576.0, cand / (d <= kBcMaxDim ? 1024.0 : 4096.0)) * kBandEntryBytes;
+        b += (uint64_t)std::max(1048576.0, cand / (d <= kBcMaxDim ? 512.0 : 4096.0)) * kBandEntryBytes;
     }
     return b + (16ull << 20);
 }

@@ -460,20 +460,41 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // the warp's current chunk of band slots [bslot, bend) (warp-uniform);
         // slot of the entry of rank `rank` among `c` <= 32 new entries
         unsigned long long bslot = 0, bend = 0;
-        auto band_slot = [&](uint32_t c, uint32_t rank) -> unsigned long long {
-            const unsigned long long rem = bend - bslot;
-            if (c <= rem) {
-                const unsigned long long k = bslot + rank;
+        // the unused rest of the warp's chunk: marked for the recheck to skip
+        auto band_holes = [&]() {
+            for (unsigned long long k = bslot + lane; k < bend; k += 32)
+                if (k < p.band_cap) {
+                    BandEntry e;
+                    e.ia = kBandHole;
+                    e.jb = 0;
+                    e.s_hat = 0.f;
+                    e.pad = 0;
+                    p.band[k] = e;
+                }
+            if (lane == 0 && bend > bslot && p.band_holes) atomicAdd(p.band_holes, bend - bslot);
+            bslot = bend;
+        };
+        // c new slots (warp-uniform c): the rest of the warp's chunk first, then a
+        // new chunk of max(kBandChunk, the remainder); the slot of rank r is
+        // r < rem ? k0 + r : nb + (r - rem)
+        struct BandSlots {
+            unsigned long long k0, nb;
+            uint32_t rem;
+            __device__ unsigned long long at(uint32_t r) const { return r < rem ? k0 + r : nb + (r - rem); }
+        };
+        auto band_reserve = [&](uint32_t c) -> BandSlots {
+            BandSlots b{bslot, 0, (uint32_t)(bend - bslot)};
+            if (c <= b.rem) {
                 bslot += c;
-                return k;
+                return b;
             }
+            const uint32_t need = c - b.rem, size = need > kBandChunk ? need : kBandChunk;
             unsigned long long nb = 0;
-            if (lane == 0) nb = atomicAdd(p.band_total, (unsigned long long)kBandChunk);
-            nb = __shfl_sync(0xffffffffu, nb, 0);
-            const unsigned long long k = rank < rem ? bslot + rank : nb + (rank - rem);
-            bslot = nb + (c - rem);
-            bend = nb + kBandChunk;
-            return k;
+            if (lane == 0) nb = atomicAdd(p.band_total, (unsigned long long)size);
+            b.nb = __shfl_sync(0xffffffffu, nb, 0);
+            bslot = b.nb + need;
+            bend = b.nb + size;
+            return b;
         };
         auto item_rows = [&](const WorkItem &ww) {
             if (ww.pad != job) {
@@ -629,6 +650,39 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                                 bbits |= (ok && t > thr_in && t <= thr_out) ? (1u << j) : 0u;
                             }
                             cnt += c32;
+                            if constexpr (BC) {
+                                // band entries straight from the lane's registers: ranks by a
+                                // warp prefix sum, slots from one warp-wide reservation
+                                const uint32_t nbits = __popc(bbits);
+                                uint32_t incl = nbits;
+#pragma unroll
+                                for (int o = 1; o < 32; o <<= 1) {
+                                    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                                    if (lane >= (uint32_t)o) incl += y;
+                                }
+                                const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+                                if (total) {
+                                    // the estimate is not kept here (reading it back by column
+                                    // index would take the values out of registers): NaN, which
+                                    // the recheck's error statistic skips
+                                    const BandSlots sl = band_reserve(total);
+                                    uint32_t rank = incl - nbits;
+                                    while (bbits) {
+                                        const int j = __ffs(bbits) - 1;
+                                        bbits &= bbits - 1;
+                                        const unsigned long long k = sl.at(rank++);
+                                        if (k < p.band_cap) {
+                                            BandEntry e;
+                                            e.ia = (uint32_t)gi;
+                                            e.jb = (uint32_t)(gj0 + cb + j);
+                                            e.s_hat = __int_as_float(0x7fc00000);
+                                            e.pad = job;
+                                            p.band[k] = e;
+                                        }
+                                    }
+                                }
+                                continue;
+                            }
                             rows = __ballot_sync(0xffffffffu, bbits != 0);
                             while (rows) {
                                 const int L = __ffs(rows) - 1;
@@ -642,7 +696,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                                 __syncwarp();
                                 const uint32_t bm = __shfl_sync(0xffffffffu, bbits, L);
                                 const float naL = __shfl_sync(0xffffffffu, na, L);
-                                const unsigned long long k = band_slot(__popc(bm), __popc(bm & ((1u << lane) - 1u)));
+                                const uint32_t rank = __popc(bm & ((1u << lane) - 1u));
+                                const unsigned long long k = band_reserve(__popc(bm)).at(rank);
                                 if (((bm >> lane) & 1u) && k < p.band_cap) {
                                     BandEntry e;
                                     e.ia = (uint32_t)(gi - (uint64_t)lane + (uint64_t)L);
@@ -683,7 +738,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                             const bool isb = ok && t > tinL && t <= toutL;
                             const uint32_t bm = __ballot_sync(0xffffffffu, isb);
                             if (bm) {
-                                const unsigned long long k = band_slot(__popc(bm), __popc(bm & ((1u << lane) - 1u)));
+                                const uint32_t rank = __popc(bm & ((1u << lane) - 1u));
+                                const unsigned long long k = band_reserve(__popc(bm)).at(rank);
                                 if (isb && k < p.band_cap) {
                                     BandEntry e;
                                     e.ia = (uint32_t)giL;
@@ -702,17 +758,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (last_tile && it < p.n_items) item_rows(w);
         }
         if (job != 0xffffffffu) flush();
-        // the unused rest of the warp's band chunk
-        for (unsigned long long k = bslot + lane; k < bend; k += 32)
-            if (k < p.band_cap) {
-                BandEntry e;
-                e.ia = kBandHole;
-                e.jb = 0;
-                e.s_hat = 0.f;
-                e.pad = 0;
-                p.band[k] = e;
-            }
-        if (lane == 0 && bend > bslot && p.band_holes) atomicAdd(p.band_holes, bend - bslot);
+        band_holes();
     }
     tc_fence_before();
     __syncthreads();

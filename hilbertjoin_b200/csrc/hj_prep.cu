@@ -986,7 +986,8 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
                                                          uint16_t *__restrict__ op_b, float *__restrict__ norms,
                                                          float *__restrict__ xn, float4 *__restrict__ blk,
                                                          float *__restrict__ cent) {
-    extern __shared__ double bc_sm[];  // [kBcBlock][d] shifted coordinates, then residuals; [d] centre; [kBcBlock][3] q pieces
+    // [kBcBlock][d] shifted coordinates, then residuals; [d] centre; [kBcBlock][3] pieces of q / 2
+    extern __shared__ double bc_sm[];
     double *cs = bc_sm + (size_t)kBcBlock * d;
     double *qp = cs + d;
     __shared__ float red_x[kBcBlock / 32], red_p[kBcBlock / 32];
