@@ -69,7 +69,7 @@ class Stats(ctypes.Structure):
 class ServerOpts(ctypes.Structure):
     _fields_ = [("memory_budget_bytes", ctypes.c_uint64), ("max_inflight", ctypes.c_int32),
                 ("device", ctypes.c_int32), ("form", ctypes.c_int32), ("batch_max", ctypes.c_int32),
-                ("reserved", ctypes.c_uint64 * 4)]
+                ("block_centring", ctypes.c_int32), ("reserved_i", ctypes.c_int32), ("reserved", ctypes.c_uint64 * 3)]
 
 
 class Result(ctypes.Structure):

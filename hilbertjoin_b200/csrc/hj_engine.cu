@@ -598,7 +598,10 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
         auto fill_job = [&]() {
             fill_tc_job(c->h_job, form, d, T, bc ? bc_scale : A.op_scale, maxabs, 0, na_eff, 0, nb_eff, in.self,
                         d_count, A.rows, B.rows, &c_rel, &c_abs);
-            if (bc) c->h_job->ka = tc_atoms(form, bc_cols(d));
+            if (bc) {
+                c->h_job->ka = tc_atoms(form, bc_cols(d));
+                c->h_job->ksteps = tc_ksteps(form, bc_cols(d));
+            }
             cudaMemcpyAsync(c->d_job, c->h_job, sizeof(TcJob), cudaMemcpyHostToDevice, st);
         };
         if (centring == HJ_CENTRING_BLOCK) {
@@ -1058,16 +1061,18 @@ void engine_ctx_trim(int device, cudaStream_t st) {
 // bounded by 6 bits per dim (cell ranges up to 60 cells per dim; wider key
 // words are rare and are measured after the join) and the band queue at its
 // first size (a larger band regrows it; the server measures that too).
-uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dtype_bytes, int form, bool self) {
+uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dtype_bytes, int form, bool self,
+                                    bool block_centring) {
     const uint64_t W = (6ull * d + 31) / 32 + 1;
     const bool tc = form_is_tc(form) || form == HJ_FORM_AUTO;
+    const bool bc = block_centring && (form == HJ_FORM_TC_FP16 || form == HJ_FORM_AUTO) && d <= kBcMaxDim;
     auto per_set = [&](uint64_t n) -> uint64_t {
         const uint64_t npad = hj_ceil_div(std::max<uint64_t>(n, 1), kTcTileB) * kTcTileB;
         uint64_t b = n * d * (uint64_t)dtype_bytes;          // sorted rows
         b += n * (2 * W + 1) * 4 + n * 8;                     // packed keys (both layouts), permutation
         b += npad * d * 8;                                    // plain FP64 tiles (plain form or routed items)
         if (tc) b += npad * (hj_ceil_div(d, 64) * 64) * 4 + npad * 8;  // operands (widest form), norms
-        if (tc && d <= kBcMaxDim) {  // block-centred operands (both layouts), q, |h|, blocks
+        if (bc) {  // block-centred operands (both layouts), q, |h|, blocks
             const uint64_t kbc = hj_ceil_div(bc_cols(d), 64) * 64;
             b += npad * kbc * 4 + npad * 8 + (npad / kBcBlock) * (16 + kBcCentStride * 4);
         }
@@ -1081,7 +1086,7 @@ uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dt
     b += tiles * (uint64_t)kMaxCombos * 8 + tiles * 64 * 16;
     if (tc) {
         const double cand = (double)na * (double)nb;
-        b += (uint64_t)std::max(1048576.0, cand / (d <= kBcMaxDim ? 512.0 : 4096.0)) * kBandEntryBytes;
+        b += (uint64_t)std::max(1048576.0, cand / (bc ? 512.0 : 4096.0)) * kBandEntryBytes;
     }
     return b + (16ull << 20);
 }

@@ -301,6 +301,8 @@ struct TcJob {
     float s_unscale;              // 1 / op_scale^2 (exact): estimates back to the caller's units
     uint32_t self;                // unordered pairs within one set (A = B)
     uint32_t ka;                  // K atoms of this job's operands
+    uint32_t ksteps;              // MMA K steps of this job (16 columns each; TF32 8): the columns
+                                  // holding data, rounded up; zero columns beyond are not multiplied
     uint32_t d;
 };
 // Fills a job for form `form`, dimension d, eps^2 = T, FP16 operand scale
@@ -323,6 +325,10 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
                    unsigned long long *d_band_holes = nullptr);
 // K atoms (128-byte operand column groups) of a form's operand rows of kcols columns.
 uint32_t tc_atoms(int form, uint32_t kcols);
+// MMA K steps that cover kcols columns (16 per kind::f16 instruction, 8 per kind::tf32),
+// and the product terms K they sum (the accumulation error model's K).
+uint32_t tc_ksteps(int form, uint32_t kcols);
+uint32_t tc_kterms(int form, uint32_t kcols);
 // FP64 recheck of the band pairs, each against its job's rows and eps^2.
 void launch_recheck(const TcJob *d_jobs, int dtype_bytes, const uint2 *band, const unsigned long long *d_band_total,
                     uint64_t band_cap, unsigned int *d_max_err_bits, cudaStream_t st);
@@ -366,8 +372,11 @@ void engine_clear_error();
 // stream have drained.
 uint64_t engine_ctx_bytes(int device);
 void engine_ctx_trim(int device, cudaStream_t st);
-// Upper estimate of the device memory one join takes in a context.
-uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dtype_bytes, int form, bool self);
+// Upper estimate of the device memory one join takes in a context; with
+// block_centring the per-block-centred operands and their first band queue
+// are counted where that centring can be chosen (FP16 or auto form, d <= 64).
+uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dtype_bytes, int form, bool self,
+                                    bool block_centring);
 // Norm summaries over a row-major norm array of npad rows (padding rows hold
 // kPadNorm): per A-tile and per B-tile maxima, per 32-row minima.
 void launch_norm_summaries(const float *norms, uint64_t npad, float *tmax_a, float *tmax_b, float *gmin32,

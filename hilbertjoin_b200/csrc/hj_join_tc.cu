@@ -63,7 +63,8 @@ constexpr int kChunkGroups = kChunkCols / 32;  // 32-column groups per chunk
 constexpr int kEpiChunks = kEpiCols / kChunkCols;
 constexpr int kEpiVec = kEpiCols / 32;  // norms per lane, group minima per warp
 // From this many rows of a 32-column group on, the lanes classify their own
-// rows (32 shuffled column norms) instead of the warp walking row by row.
+// rows (32 shuffled column norms) instead of the warp walking row by row;
+// with block centring (no column norms to shuffle) always.
 constexpr int kDenseRows = 8;
 // Band slots are reserved by each epilogue warp in chunks (one atomic per
 // chunk); slots a warp leaves unused are marked with ia = kBandHole.
@@ -87,6 +88,7 @@ struct BandEntry {
 
 struct TcArgs {
     uint32_t ka;        // K atoms per operand buffer, the largest of the jobs' (TF32: kpad/32; BF16, FP16: kpad16/64)
+                        // (each job multiplies only its own ksteps)
     uint32_t a_bufs;    // 1 or 2 A buffers
     uint32_t nst;       // B ring stages
     const WorkItem *items;
@@ -323,7 +325,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             bool issued_any = false, ok = true;
             for (uint64_t it = blockIdx.x; ok && it < p.n_items; it += gridDim.x) {
                 const WorkItem w = p.items[it];
-                const uint32_t ka = p.jobs[w.pad].ka;
+                const uint32_t ka = p.jobs[w.pad].ka, ksteps = p.jobs[w.pad].ksteps;
                 const uint32_t jb_atoms = kBf ? 2 * ka : ka;
                 const uint32_t abuf = a_cnt % p.a_bufs, au = a_cnt / p.a_bufs;
                 if (!mbar_wait(&bar_afull[abuf], au & 1u, err, 3)) break;
@@ -348,19 +350,20 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         const uint32_t bsm = b_base + s * kBStageBytes;
                         if constexpr (!kBf) {
                             const uint32_t asm_ = abase + q * kAStageBytes;
-#pragma unroll
-                            for (uint32_t kk = 0; kk < 4; ++kk) {
+                            // 4 K steps per atom, fewer in the last (zero columns not multiplied)
+                            const uint32_t kk_end = ksteps - 4 * q < 4 ? ksteps - 4 * q : 4;
+                            for (uint32_t kk = 0; kk < kk_end; ++kk) {
                                 mma_issue<FORM>(dcol, sw128_desc(asm_ + kk * 32), sw128_desc(bsm + kk * 32), idesc,
                                                 accumulate);
                                 accumulate = 1;
                             }
                         } else {
                             const uint32_t kq = q >> 1;
+                            const uint32_t kk_end = ksteps - 4 * kq < 4 ? ksteps - 4 * kq : 4;
                             const uint32_t a_hi = abase + kq * kAStageBytes;
                             const uint32_t a_lo = abase + (ka + kq) * kAStageBytes;
                             if ((q & 1u) == 0) {  // B_hi atom: A_hi.B_hi + A_lo.B_hi
-#pragma unroll
-                                for (uint32_t kk = 0; kk < 4; ++kk) {
+                                for (uint32_t kk = 0; kk < kk_end; ++kk) {
                                     mma_issue<FORM>(dcol, sw128_desc(a_hi + kk * 32), sw128_desc(bsm + kk * 32),
                                                     idesc, accumulate);
                                     accumulate = 1;
@@ -368,8 +371,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                                                     idesc, 1);
                                 }
                             } else {  // B_lo atom: A_hi.B_lo
-#pragma unroll
-                                for (uint32_t kk = 0; kk < 4; ++kk)
+                                for (uint32_t kk = 0; kk < kk_end; ++kk)
                                     mma_issue<FORM>(dcol, sw128_desc(a_hi + kk * 32), sw128_desc(bsm + kk * 32),
                                                     idesc, 1);
                             }
@@ -634,7 +636,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                                 jlo = first > 0 ? (first > kEpiCols ? kEpiCols : (int)first) : 0;
                             }
                         }
-                        if (__popc(rows) >= kDenseRows && p.dbg == nullptr) {
+                        if ((BC || __popc(rows) >= kDenseRows) && p.dbg == nullptr) {
                             // Many rows (tiles where neighbours are common): every lane
                             // classifies its own row against the group's 32 columns, the
                             // column norms broadcast by shuffles; then only the rows with
@@ -845,7 +847,7 @@ __global__ void k_recheck(const TcJob *__restrict__ jobs, const BandEntry *__res
 // in s: c_abs = 1.25 * d * 2^-8.
 void tc_band_constants(int form, uint32_t d, double maxabs, double *c_rel, double *c_abs) {
     const double u24 = std::ldexp(1.0, -24), acc = std::ldexp(1.0, -22);
-    const double kpad = form == HJ_FORM_TC_TF32 ? (double)((d + 31) / 32 * 32) : (double)((d + 63) / 64 * 64);
+    const double kpad = (double)tc_kterms(form, d);  // product terms summed (zero columns are not multiplied)
     double dot;
     if (form == HJ_FORM_TC_TF32 || form == HJ_FORM_TC_FP16) {
         const double u = std::ldexp(1.0, -11);
@@ -921,10 +923,16 @@ static TcLayout tc_layout(int form, uint32_t d) {
 }
 
 uint32_t tc_atoms(int form, uint32_t kcols) { return tc_layout(form, kcols).ka; }
+uint32_t tc_ksteps(int form, uint32_t kcols) {
+    const uint32_t k = form == HJ_FORM_TC_TF32 ? 8u : 16u;
+    return (kcols + k - 1) / k;
+}
+uint32_t tc_kterms(int form, uint32_t kcols) { return tc_ksteps(form, kcols) * (form == HJ_FORM_TC_TF32 ? 8u : 16u); }
 
 // Per-block centring constants (operand units, FP16 form):
-//   kp21: the accumulation model above, K = kpad_bc product terms of
-//     magnitude sum <= S per dot, the dot entering s twice: 2 kpad 2^-22;
+//   kp21: the accumulation model above, K = 3d + 3 rounded up to the MMA's 16
+//     (the product terms summed) of magnitude sum <= S per dot, the dot
+//     entering s twice: 2 K 2^-22;
 //   rho_u: |fl16(h) - h| <= 2^-11 |h| per coordinate (normal range), with
 //     |h| <= |fl16(h)| (1 + 2^-10): 1.001 * 2^-11 per unit of the stored |h|;
 //   rho_c: subnormal FP16 (|h| < 2^-14) is off by at most 2^-25 per
@@ -937,7 +945,7 @@ uint32_t tc_atoms(int form, uint32_t kcols) { return tc_layout(form, kcols).ka; 
 //   theta_t: the FP64 pair test sums d squares of exact differences with FMAs,
 //     relative error below (d + 2) 2^-53 of dist2 ~ eps^2: 2 (d + 2) 2^-53 T.
 BcConsts bc_constants(uint32_t d, double T, double op_scale) {
-    const double s2 = op_scale * op_scale, kpad = (double)tc_atoms(HJ_FORM_TC_FP16, bc_cols(d)) * 64.0;
+    const double s2 = op_scale * op_scale, kpad = (double)tc_kterms(HJ_FORM_TC_FP16, bc_cols(d));
     auto up = [](double v) {
         const float f = (float)v;
         return (double)f >= v ? f : std::nextafter(f, INFINITY);
@@ -982,6 +990,7 @@ void fill_tc_job(TcJob *j, int form, uint32_t d, double T, double op_scale, doub
     j->s_unscale = (float)(1.0 / s2);  // a power of two: exact
     j->self = self ? 1u : 0u;
     j->ka = tc_layout(form, d).ka;
+    j->ksteps = tc_ksteps(form, d);
     j->d = d;
     if (c_rel_out) *c_rel_out = c_rel;
     if (c_abs_out) *c_abs_out = c_abs;

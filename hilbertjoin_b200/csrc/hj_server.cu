@@ -73,6 +73,7 @@ struct Request {
 struct hj_server {
     hj_server_opts opts{};
     int device = 0;
+    int centring = HJ_CENTRING_GLOBAL;  // of the requests' FP16 joins (hj_server_opts.block_centring)
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<uint64_t> queue;
@@ -88,7 +89,8 @@ struct hj_server {
 constexpr double kHeadWaitMs = 1000.0;
 
 static uint64_t request_bytes(const hj_server *s, const DevSet &a, const DevSet &b, bool self) {
-    return hj::engine_join_bytes_estimate(a.n, self ? a.n : b.n, a.d, a.dtype_bytes, s->opts.form, self);
+    return hj::engine_join_bytes_estimate(a.n, self ? a.n : b.n, a.d, a.dtype_bytes, s->opts.form, self,
+                                          s->centring != HJ_CENTRING_GLOBAL);
 }
 
 static uint64_t charged_by_others(const hj_server *s, int w) {
@@ -204,6 +206,7 @@ static void worker_main(hj_server *s, int w) {
         hj_opts o;
         hj_opts_init(&o);
         o.form = s->opts.form;
+        o.tc_centring = s->centring;
         o.device = s->device;
         o.stream = stream;
         const size_t k = ids.size();
@@ -298,6 +301,7 @@ int hj_server_create(const hj_server_opts *opts, hj_server **out) {
     hj_server *s = new hj_server();
     s->opts = o;
     s->device = dev;
+    s->centring = o.block_centring ? HJ_CENTRING_AUTO : HJ_CENTRING_GLOBAL;
     s->held.assign(o.max_inflight, 0);
     s->charged.assign(o.max_inflight, 0);
     for (int i = 0; i < o.max_inflight; ++i) s->workers.emplace_back(worker_main, s, i);

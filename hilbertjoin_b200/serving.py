@@ -55,15 +55,18 @@ def _result_dict(r: Result) -> dict:
 
 class Server:
     def __init__(self, form="auto", memory_budget_bytes: int = 40 << 30, max_inflight: int = 8, device=None,
-                 batch_max: int = 1):
+                 batch_max: int = 1, block_centring: bool = False):
         """batch_max > 1 (tensor-core forms): a free worker runs up to batch_max
-        queued requests as one batch (one persistent launch)."""
+        queued requests as one batch (one persistent launch). block_centring:
+        the requests' FP16 joins may switch to per-block centring (admission
+        then counts its buffers); otherwise they use one global centre."""
         L = _bind()
         o = ServerOpts()
         L.hj_server_opts_init(ctypes.byref(o))
         o.memory_budget_bytes = int(memory_budget_bytes)
         o.max_inflight = int(max_inflight)
         o.batch_max = int(batch_max)
+        o.block_centring = int(bool(block_centring))
         o.device = -1 if device is None else int(device)
         o.form = FORMS[form] if isinstance(form, str) else int(form)
         h = ctypes.c_void_p()

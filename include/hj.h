@@ -341,7 +341,12 @@ typedef struct {
                                      requests (same dtype, within the budget) and runs them as one
                                      batch (hj_batch_*: one persistent launch); 0 or 1 = one
                                      request per worker */
-    uint64_t reserved[4];
+    int32_t block_centring;       /* 0: the requests' FP16 joins use one global centre
+                                     (HJ_CENTRING_GLOBAL); nonzero: HJ_CENTRING_AUTO, and admission
+                                     counts the block-centred operands and band queue of every
+                                     request that could use them (d <= 64) */
+    int32_t reserved_i;
+    uint64_t reserved[3];
 } hj_server_opts;
 
 typedef struct {
