@@ -352,10 +352,22 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                             const uint32_t asm_ = abase + q * kAStageBytes;
                             // 4 K steps per atom, fewer in the last (zero columns not multiplied)
                             const uint32_t kk_end = ksteps - 4 * q < 4 ? ksteps - 4 * q : 4;
-                            for (uint32_t kk = 0; kk < kk_end; ++kk) {
-                                mma_issue<FORM>(dcol, sw128_desc(asm_ + kk * 32), sw128_desc(bsm + kk * 32), idesc,
-                                                accumulate);
-                                accumulate = 1;
+                            if (kk_end == 4) {
+#pragma unroll
+                                for (uint32_t kk = 0; kk < 4; ++kk) {
+                                    mma_issue<FORM>(dcol, sw128_desc(asm_ + kk * 32), sw128_desc(bsm + kk * 32), idesc,
+                                                    accumulate);
+                                    accumulate = 1;
+                                }
+                            } else {
+#pragma unroll
+                                for (uint32_t kk = 0; kk < 3; ++kk) {
+                                    if (kk < kk_end) {
+                                        mma_issue<FORM>(dcol, sw128_desc(asm_ + kk * 32), sw128_desc(bsm + kk * 32),
+                                                        idesc, accumulate);
+                                        accumulate = 1;
+                                    }
+                                }
                             }
                         } else {
                             const uint32_t kq = q >> 1;
@@ -363,7 +375,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                             const uint32_t a_hi = abase + kq * kAStageBytes;
                             const uint32_t a_lo = abase + (ka + kq) * kAStageBytes;
                             if ((q & 1u) == 0) {  // B_hi atom: A_hi.B_hi + A_lo.B_hi
-                                for (uint32_t kk = 0; kk < kk_end; ++kk) {
+#pragma unroll
+                                for (uint32_t kk = 0; kk < 4; ++kk) {
+                                    if (kk >= kk_end) break;
                                     mma_issue<FORM>(dcol, sw128_desc(a_hi + kk * 32), sw128_desc(bsm + kk * 32),
                                                     idesc, accumulate);
                                     accumulate = 1;
@@ -371,9 +385,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                                                     idesc, 1);
                                 }
                             } else {  // B_lo atom: A_hi.B_lo
-                                for (uint32_t kk = 0; kk < kk_end; ++kk)
-                                    mma_issue<FORM>(dcol, sw128_desc(a_hi + kk * 32), sw128_desc(bsm + kk * 32),
-                                                    idesc, 1);
+#pragma unroll
+                                for (uint32_t kk = 0; kk < 4; ++kk)
+                                    if (kk < kk_end)
+                                        mma_issue<FORM>(dcol, sw128_desc(a_hi + kk * 32), sw128_desc(bsm + kk * 32),
+                                                        idesc, 1);
                             }
                         }
                         mma_commit(&bar_bempty[s]);  // stage free once these MMAs have read it
