@@ -319,25 +319,22 @@ static int ensure_plain_tiles(Ctx *c, cudaStream_t st, SortedSet *s, bool is_b, 
     return check_cuda("plain layout");
 }
 
-// Per-block-centred FP16 operands of a sorted set (HJ_CENTRING_BLOCK): the A
-// layout for a join's set A, the B layout for its set B, both for a self-join
-// (is_b false, with_b true); q and |h| per rank, block summaries and centres.
-// scale = the global form's operand scale times 2^-kBcScaleShift.
-static int prepare_block_centring(Ctx *c, cudaStream_t st, SortedSet *s, bool with_a, bool with_b, bool is_b,
-                                  const double *center, double scale, int *launches) {
+// Per-block-centred FP16 operands of a sorted set (HJ_CENTRING_BLOCK): the
+// operand rows whose windows serve as A and as B, q and |h| per rank, block
+// summaries and centres. scale = the global form's operand scale times
+// 2^-kBcScaleShift.
+static int prepare_block_centring(Ctx *c, cudaStream_t st, SortedSet *s, bool is_b, const double *center,
+                                  double scale, int *launches) {
     const uint64_t npad = s->npad_tc, nblk = npad / kBcBlock;
-    s->kpad_bc = tc_atoms(HJ_FORM_TC_FP16, bc_cols(s->d)) * 64;
-    s->bc_op_a = with_a ? (uint16_t *)slot_alloc_impl(c, st, kSlotBcOpA, npad * s->kpad_bc * 2) : nullptr;
-    s->bc_op_b = with_b ? (uint16_t *)slot_alloc_impl(c, st, kSlotBcOpB, npad * s->kpad_bc * 2) : nullptr;
+    s->bc_dp = bc_dp(s->d);
+    s->bc_op = (uint16_t *)slot_alloc_impl(c, st, is_b ? kSlotBcOpB : kSlotBcOpA, npad * 4 * s->bc_dp * 2);
     s->bc_norms = (float *)slot_alloc_impl(c, st, is_b ? kSlotBcNormB : kSlotBcNormA, npad * 4);
     s->bc_xn = (float *)slot_alloc_impl(c, st, is_b ? kSlotBcXnB : kSlotBcXnA, npad * 4);
     s->bc_blk = (float4 *)slot_alloc_impl(c, st, is_b ? kSlotBcBlkB : kSlotBcBlkA, nblk * sizeof(float4));
     s->bc_cent = (float *)slot_alloc_impl(c, st, is_b ? kSlotBcCentB : kSlotBcCentA, nblk * kBcCentStride * 4);
-    if ((with_a && !s->bc_op_a) || (with_b && !s->bc_op_b) || !s->bc_norms || !s->bc_xn || !s->bc_blk ||
-        !s->bc_cent)
+    if (!s->bc_op || !s->bc_norms || !s->bc_xn || !s->bc_blk || !s->bc_cent)
         return fail(HJ_ERR_OOM, "out of device memory (block-centred operands)");
-    launch_bc_prepare(*s, center, scale, s->bc_op_a, s->bc_op_b, s->bc_norms, s->bc_xn, s->bc_blk, s->bc_cent, st,
-                      launches);
+    launch_bc_prepare(*s, center, scale, s->bc_op, s->bc_norms, s->bc_xn, s->bc_blk, s->bc_cent, st, launches);
     return check_cuda("block-centred operands");
 }
 
@@ -580,13 +577,11 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
         const bool bc_ok = form == HJ_FORM_TC_FP16 && d <= kBcMaxDim;
         const double bc_scale = std::ldexp(A.op_scale, -kBcScaleShift);
         auto enable_bc = [&]() -> int {
-            if (int r = prepare_block_centring(c, st, &A, true, in.self, false, A.center, bc_scale, &launches))
-                return r;
+            if (int r = prepare_block_centring(c, st, &A, false, A.center, bc_scale, &launches)) return r;
             if (in.self) {
-                B.bc_op_b = A.bc_op_b, B.bc_norms = A.bc_norms, B.bc_xn = A.bc_xn;
-                B.bc_blk = A.bc_blk, B.bc_cent = A.bc_cent, B.kpad_bc = A.kpad_bc;
-            } else if (int r = prepare_block_centring(c, st, &B, false, true, true, B.center, bc_scale,
-                                                      &launches)) {
+                B.bc_op = A.bc_op, B.bc_dp = A.bc_dp, B.bc_norms = A.bc_norms, B.bc_xn = A.bc_xn;
+                B.bc_blk = A.bc_blk, B.bc_cent = A.bc_cent;
+            } else if (int r = prepare_block_centring(c, st, &B, true, B.center, bc_scale, &launches)) {
                 return r;
             }
             bc = true;
@@ -1072,10 +1067,8 @@ uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dt
         b += n * (2 * W + 1) * 4 + n * 8;                     // packed keys (both layouts), permutation
         b += npad * d * 8;                                    // plain FP64 tiles (plain form or routed items)
         if (tc) b += npad * (hj_ceil_div(d, 64) * 64) * 4 + npad * 8;  // operands (widest form), norms
-        if (bc) {  // block-centred operands (both layouts), q, |h|, blocks
-            const uint64_t kbc = hj_ceil_div(bc_cols(d), 64) * 64;
-            b += npad * kbc * 4 + npad * 8 + (npad / kBcBlock) * (16 + kBcCentStride * 4);
-        }
+        if (bc)  // block-centred operand rows, q, |h|, blocks
+            b += npad * 4 * bc_dp(d) * 2 + npad * 8 + (npad / kBcBlock) * (16 + kBcCentStride * 4);
         return b;
     };
     uint64_t b = per_set(na) + (self ? 0 : per_set(nb));

@@ -106,13 +106,14 @@ struct SortedSet {
     uint64_t npad_tc = 0;
     uint32_t kpad_tf32 = 0, kpad_bf16 = 0;
     // per-block centring of the FP16 operands (HJ_CENTRING_BLOCK; see BcConsts):
-    // [npad][kpad_bc] rows in the A layout [h | h | c | 2^k] and the B layout [h | c | h | q/2]
-    uint16_t *bc_op_a = nullptr, *bc_op_b = nullptr;
+    // [npad][4 bc_dp] rows; the B operand is the window at column 0, the A operand
+    // the window at column bc_dp, both 3 bc_dp wide
+    uint16_t *bc_op = nullptr;
+    uint32_t bc_dp = 0;
     float *bc_norms = nullptr;    // q = |h|^2 + 2 h.c per rank (FP32; padding rows kPadNorm)
     float *bc_xn = nullptr;       // |h| per rank, rounded up
     float4 *bc_blk = nullptr;     // per 128-rank block: {max |h|, |c|, max |q|, 0}, rounded up
     float *bc_cent = nullptr;     // per block: c in FP32 (FP16 values), kBcCentStride floats, zero padded
-    uint32_t kpad_bc = 0;
 };
 
 // Per-block centring of the FP16 operands. Every 128-rank block of a sorted
@@ -120,12 +121,17 @@ struct SortedSet {
 // values in the operand units ((x - center) * scale, the largest coordinate
 // below 2^10), the midpoint of the block's range rounded to FP16; every rank
 // is stored as that centre plus its residual h = fl16(x - c). With
-// q = |h|^2 + 2 h.c per rank, operand rows hold 3d + 3 columns,
-//     A: [h | h | c | -2^15 -2^4 -2^-7]      B: [h | c | h | m1 m2 m3],
-// m1 2^15 + m2 2^4 + m3 2^-7 = q / 2 (three FP16 pieces, to 2^-33 |q|), so
-// that one MMA gives, for the operand points x' = c + h,
-//     w_ij = h_i.h_j + h_i.c_j + c_i.h_j - q_j / 2 = x'_i.x'_j - c_i.c_j - q_j / 2,
+// q = |h|^2 + 2 h.c per rank and m1 2^15 + m2 2^4 + m3 2^-7 = q / 2 (three
+// FP16 pieces, to 2^-33 |q|), a row holds four blocks of dp = roundup(d + 3, 8)
+// columns (zero padded),
+//     [h | h | c m1 m2 m3 | h a1 a2 a3],   (a1, a2, a3) = (-2^15, -2^4, -2^-7),
+// and the operands are two windows of 3 dp columns of the same rows:
+//     B = columns [0, 3dp) = [h | h | c m],   A = columns [dp, 4dp) = [h | c m | h a].
+// Column by column the products are h_i.h_j, c_i.h_j (m_i meets B's zero pad),
+// h_i.c_j and a.m_j, so one MMA gives, for the operand points x' = c + h,
+//     w_ij = h_i.h_j + c_i.h_j + h_i.c_j - q_j / 2 = x'_i.x'_j - c_i.c_j - q_j / 2,
 //     dist2(x'_i, x'_j) = q_i + |c_i - c_j|^2 - 2 w_ij.
+// (The A window's last atom reaches past the row end: the TMA fills zeros.)
 // The accumulator alone orders the columns of a row (no per-column norm), so
 // the epilogue's maximum over 32 columns is exact. The only rounding of the
 // points is h's (relative 2^-11 per coordinate): it moves a point by
@@ -134,10 +140,11 @@ struct SortedSet {
 // of quadratic in the distance from one global centre, which keeps clustered
 // data with eps far below its spread on the tensor cores.
 constexpr uint32_t kBcBlock = 128;      // ranks per centring block (= kTcTileA, = kTcTileB / 2)
-constexpr uint32_t kBcMaxDim = 64;      // 3d + 3 <= 195 operand columns
+constexpr uint32_t kBcMaxDim = 64;      // dp <= 72: windows of <= 216 columns
 constexpr uint32_t kBcCentStride = 64;  // floats per block in bc_cent
 constexpr int kBcScaleShift = 5;        // operand scale of the global form times 2^-5
-inline uint32_t bc_cols(uint32_t d) { return 3 * d + 3; }
+inline uint32_t bc_dp(uint32_t d) { return (d + 3 + 7) / 8 * 8; }
+inline uint32_t bc_cols(uint32_t d) { return 3 * bc_dp(d); }  // columns of an operand window
 struct BcConsts {
     float kp21;     // 2 kpad_bc 2^-22: the MMA accumulation error of w per unit of S, doubled for s
     float eps;      // eps in operand units, rounded up
@@ -168,11 +175,11 @@ __host__ __device__ inline float bc_tau(float xa, float ca, float pa, float xb, 
 // Fills the constants for dimension d, eps^2 = T (caller units) and the FP16
 // operand scale.
 BcConsts bc_constants(uint32_t d, double T, double op_scale);
-// Block centres, residual operands (A and/or B layout; null skips one), q, |h|
-// and block summaries of a sorted set from its sorted rows. center = the
-// global per-dim shift, scale = the block-centred operand scale.
-void launch_bc_prepare(const SortedSet &s, const double *center, double scale, uint16_t *op_a, uint16_t *op_b,
-                       float *norms, float *xn, float4 *blk, float *cent, cudaStream_t st, int *launches);
+// Block centres, the operand rows ([npad][4 dp]), q, |h| and block summaries
+// of a sorted set from its sorted rows. center = the global per-dim shift,
+// scale = the block-centred operand scale.
+void launch_bc_prepare(const SortedSet &s, const double *center, double scale, uint16_t *op, float *norms,
+                       float *xn, float4 *blk, float *cent, cudaStream_t st, int *launches);
 
 constexpr float kPadNorm = 1.0e30f;
 
@@ -316,9 +323,9 @@ void fill_tc_job(TcJob *j, int form, uint32_t d, double T, double op_scale, doub
 // A and B describe the operand matrices (layout pointers, npad_tc rows, kpad,
 // norms and their tile maxima and group minima); their d is the largest of the
 // jobs'. na0 / nb0: job 0's counted ranks (debug output only).
-// With bc non-null (FP16 form, one job): the per-block-centred operands of
-// A (A layout) and B (B layout) and their summaries; the job's ka must be the
-// one of 3d columns (tc_atoms).
+// With bc non-null (FP16 form, one job): the per-block-centred operands of A
+// and B (their windows) and summaries; the job's ka and ksteps must be the
+// ones of bc_cols(d) columns (tc_atoms, tc_ksteps).
 int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob *d_jobs, uint64_t na0, uint64_t nb0,
                    const IndexResult &idx, uint2 *band, uint64_t band_cap, unsigned long long *d_band_total,
                    uint32_t *d_err, int num_sms, cudaStream_t st, std::string *err, const BcConsts *bc = nullptr,

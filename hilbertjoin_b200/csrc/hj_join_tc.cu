@@ -105,6 +105,7 @@ struct TcArgs {
     uint32_t *err;
     float *dbg;                     // optional: s_hat for every pair, input order [na][nb] (tests)
     const uint32_t *perm_a, *perm_b;  // EGO rank -> input index (for dbg)
+    uint32_t a_xoff;                // first column of the A operand in its rows (block centring: dp)
     uint64_t gate_ns;               // test hook: > 0 makes the epilogue wait this long on a barrier
                                     // that nothing arrives on, then raise kErrTimeout
     // per-block centring (BC kernels): norm_a is then q of the A rows (norm_b and
@@ -283,7 +284,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const bool lo = kBf && q >= ka;
                     const uint32_t kq = kBf ? (lo ? q - ka : q) : q;
                     tma_load_2d(smem_raw + (adst + q * kAStageBytes - smem_u32(smem_raw)), lo ? &tm_a2 : &tm_a,
-                                (int32_t)(kq * kAtomElems), (int32_t)(w.a * kTcTileA), &bar_afull[abuf]);
+                                (int32_t)(kq * kAtomElems + p.a_xoff), (int32_t)(w.a * kTcTileA), &bar_afull[abuf]);
                 }
                 ++a_cnt;
                 for (uint32_t bt = w.b0; ok && bt < w.b1; ++bt) {
@@ -1017,7 +1018,7 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
                    uint32_t *d_err, int num_sms, cudaStream_t st, std::string *err, const BcConsts *bc,
                    unsigned long long *d_band_holes) {
     if (idx.n_items == 0) return 0;
-    if (bc && (form != HJ_FORM_TC_FP16 || A.d > kBcMaxDim || !A.bc_op_a || !B.bc_op_b)) {
+    if (bc && (form != HJ_FORM_TC_FP16 || A.d > kBcMaxDim || !A.bc_op || !B.bc_op || A.bc_dp != B.bc_dp)) {
         *err = "per-block centring needs the FP16 form, d <= 64 and the centred layouts";
         return 1;
     }
@@ -1028,8 +1029,10 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
     }
     CUtensorMap ma, ma2, mb, mb2;
     if (bc) {
-        if (!make_map(&ma, A.bc_op_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, A.npad_tc, A.kpad_bc, kTcTileA, err)) return 1;
-        if (!make_map(&mb, B.bc_op_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, B.npad_tc, B.kpad_bc, kTcTileB, err)) return 1;
+        // rows of 4 dp columns; A reads the window from column dp (the producer's
+        // x offset), B from column 0; past the row end the copy fills zeros
+        if (!make_map(&ma, A.bc_op, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, A.npad_tc, 4 * A.bc_dp, kTcTileA, err)) return 1;
+        if (!make_map(&mb, B.bc_op, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, B.npad_tc, 4 * B.bc_dp, kTcTileB, err)) return 1;
         ma2 = ma;
         mb2 = mb;
     } else if (form == HJ_FORM_TC_TF32) {
@@ -1083,6 +1086,7 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
         a.cent_a = A.bc_cent;
         a.cent_b = B.bc_cent;
         a.bc = *bc;
+        a.a_xoff = A.bc_dp;
     }
     uint64_t grid = (uint64_t)num_sms;
     if (grid > idx.n_items) grid = idx.n_items;

@@ -971,21 +971,20 @@ __global__ void k_group_min(const float *__restrict__ v, uint64_t npad, int grou
 // and kept in shared memory; per dim the midpoint of the block's range,
 // rounded to FP16, is the centre c; every rank's residual h = fl16(x - c)
 // (round to nearest, once), q = |h|^2 + 2 h.c from the FP16 values in FP64,
-// and |h|; then the operand rows (zero padded to kpad) are written as 16-byte
-// chunks, consecutive threads on consecutive chunks:
-//     A: [h | h | c | -2^15 -2^4 -2^-7]      B: [h | c | h | m1 m2 m3]
-// with q / 2 = 2^15 m1 + 2^4 m2 + 2^-7 m3 + r: m1 = fl16(q / 2^16), m2 and
-// m3 the FP16 of the exact remainders, |r| <= 2^-33 |q| + 2^-32. Bounds: with
+// and |h|; then the operand rows (four blocks of dp columns, zero padded)
+//     [h | h | c m1 m2 m3 | h -2^15 -2^4 -2^-7]
+// are written as 16-byte chunks, consecutive threads on consecutive chunks,
+// with q / 2 = 2^15 m1 + 2^4 m2 + 2^-7 m3 + r: m1 = fl16(q / 2^16), m2 and m3
+// the FP16 of the exact remainders, |r| <= 2^-33 |q| + 2^-32. Bounds: with
 // |x - center| * scale < 2^10 per coordinate, |h_t| < 2^10 (1 + 2^-11) and
 // |q| < 3 2^20 d <= 3 2^26, so every piece is below 2^12 in magnitude.
-// Ranks past n (up to npad) are padding: zero operands, q = kPadNorm, |h| = 0.
+// Ranks past n (up to npad) are padding: zero rows, q = kPadNorm, |h| = 0.
 template <typename T>
 __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ rows, uint64_t n, uint32_t d,
                                                          const double *__restrict__ center, double scale,
-                                                         uint32_t kpad, uint16_t *__restrict__ op_a,
-                                                         uint16_t *__restrict__ op_b, float *__restrict__ norms,
-                                                         float *__restrict__ xn, float4 *__restrict__ blk,
-                                                         float *__restrict__ cent) {
+                                                         uint32_t dp, uint16_t *__restrict__ op,
+                                                         float *__restrict__ norms, float *__restrict__ xn,
+                                                         float4 *__restrict__ blk, float *__restrict__ cent) {
     // [kBcBlock][d] shifted coordinates, then residuals; [d] centre; [kBcBlock][3] pieces of q / 2
     extern __shared__ double bc_sm[];
     double *cs = bc_sm + (size_t)kBcBlock * d;
@@ -1036,42 +1035,31 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
     qp[3 * r + 1] = m2;
     qp[3 * r + 2] = m3;
     __syncthreads();
-    const uint32_t cpr = kpad / 8;  // 16-byte chunks per operand row
+    const uint32_t cpr = dp / 2;  // 16-byte chunks per row (4 dp halves)
     for (uint32_t e = threadIdx.x; e < kBcBlock * cpr; e += kBcBlock) {
         const uint32_t rr = e / cpr, q = e % cpr;
-        uint32_t wa[4], wb[4];
+        uint32_t w[4];
 #pragma unroll
         for (int h2 = 0; h2 < 4; ++h2) {
-            uint32_t ea = 0, eb = 0;
+            uint32_t ew = 0;
 #pragma unroll
             for (int z = 0; z < 2; ++z) {
-                const uint32_t k = 8 * q + 2 * h2 + z;
-                double av = 0.0, bv = 0.0;
+                const uint32_t k = 8 * q + 2 * h2 + z, blkc = k / dp, t = k % dp;  // block, column within it
+                double v = 0.0;
                 if (rr < nr) {
-                    if (k < d) {
-                        av = bv = bc_sm[rr * d + k];
-                    } else if (k < 2 * d) {
-                        av = bc_sm[rr * d + k - d];
-                        bv = cs[k - d];
-                    } else if (k < 3 * d) {
-                        av = cs[k - 2 * d];
-                        bv = bc_sm[rr * d + k - 2 * d];
-                    } else if (k < 3 * d + 3) {
-                        const uint32_t u = k - 3 * d;
-                        av = u == 0 ? -0x1p15 : (u == 1 ? -0x1p4 : -0x1p-7);
-                        bv = qp[3 * rr + u];
-                    }
+                    if (t < d)
+                        v = blkc == 2 ? cs[t] : bc_sm[rr * d + t];
+                    else if (t < d + 3 && blkc == 2)
+                        v = qp[3 * rr + (t - d)];
+                    else if (t < d + 3 && blkc == 3)
+                        v = t == d ? -0x1p15 : (t == d + 1 ? -0x1p4 : -0x1p-7);
                 }
-                // FP16 values already: the conversions are exact
-                ea |= (uint32_t)__half_as_ushort(__double2half(av)) << (16 * z);
-                eb |= (uint32_t)__half_as_ushort(__double2half(bv)) << (16 * z);
+                // FP16 values already: the conversion is exact
+                ew |= (uint32_t)__half_as_ushort(__double2half(v)) << (16 * z);
             }
-            wa[h2] = ea;
-            wb[h2] = eb;
+            w[h2] = ew;
         }
-        const uint64_t o = (r0 + rr) * kpad / 8 + q;
-        if (op_a) reinterpret_cast<uint4 *>(op_a)[o] = make_uint4(wa[0], wa[1], wa[2], wa[3]);
-        if (op_b) reinterpret_cast<uint4 *>(op_b)[o] = make_uint4(wb[0], wb[1], wb[2], wb[3]);
+        reinterpret_cast<uint4 *>(op)[(r0 + rr) * cpr + q] = make_uint4(w[0], w[1], w[2], w[3]);
     }
     // block summaries: max |h|, |c|, max |q| (all rounded up)
 #pragma unroll
@@ -1098,8 +1086,8 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
     }
 }
 
-void launch_bc_prepare(const SortedSet &s, const double *center, double scale, uint16_t *op_a, uint16_t *op_b,
-                       float *norms, float *xn, float4 *blk, float *cent, cudaStream_t st, int *launches) {
+void launch_bc_prepare(const SortedSet &s, const double *center, double scale, uint16_t *op, float *norms,
+                       float *xn, float4 *blk, float *cent, cudaStream_t st, int *launches) {
     if (s.npad_tc == 0) return;
     const unsigned blocks = (unsigned)(s.npad_tc / kBcBlock);
     const size_t smem = ((size_t)kBcBlock * s.d + s.d + 3 * kBcBlock) * sizeof(double);
@@ -1107,11 +1095,11 @@ void launch_bc_prepare(const SortedSet &s, const double *center, double scale, u
     if (s.dtype_bytes == 8) {
         ensure_max_dynamic_smem((const void *)k_bc_prepare<double>, smem_max);
         k_bc_prepare<double><<<blocks, kBcBlock, smem, st>>>(static_cast<const double *>(s.rows), s.n, s.d, center,
-                                                             scale, s.kpad_bc, op_a, op_b, norms, xn, blk, cent);
+                                                             scale, s.bc_dp, op, norms, xn, blk, cent);
     } else {
         ensure_max_dynamic_smem((const void *)k_bc_prepare<float>, smem_max);
         k_bc_prepare<float><<<blocks, kBcBlock, smem, st>>>(static_cast<const float *>(s.rows), s.n, s.d, center,
-                                                            scale, s.kpad_bc, op_a, op_b, norms, xn, blk, cent);
+                                                            scale, s.bc_dp, op, norms, xn, blk, cent);
     }
     if (launches) *launches += 1;
 }

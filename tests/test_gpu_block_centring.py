@@ -169,7 +169,8 @@ def test_estimates_all_pairs_loose_bound(hj):
         half = 0.5 * (both.max(0) - both.min(0))
         R = float(np.sqrt((half ** 2).sum()))  # |c| <= R (centres inside the box)
         H = 2.0 * R                             # |h| <= diameter of the box
-        kpad = -(-(3 * d + 3) // 16) * 16       # product terms the MMAs sum
+        dp = -(-(d + 3) // 8) * 8                 # block width of the operand rows
+        kpad = -(-(3 * dp) // 16) * 16            # product terms the MMAs sum
         S = 1.5 * (H * H + 2 * H * R)           # cross terms and the folded q / 2
         rho = 2 * 2.0 ** -11 * H
         bound = 2 * kpad * 2.0 ** -22 * S + 2 * rho * np.sqrt(ex) + rho * rho + 1e-5 * (1 + ex)
