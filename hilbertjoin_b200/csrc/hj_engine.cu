@@ -689,8 +689,11 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
                 band_total = c->h_small[4];
                 band_holes = c->h_small[7];
                 if (band_total <= cap) {
+                    // sorted rows: slot buffers (256-byte aligned) of n rows of d coordinates
+                    const bool vec_rows = ((uint64_t)d * A.dtype_bytes) % 16 == 0 &&
+                                          ((uintptr_t)A.rows & 15u) == 0 && ((uintptr_t)B.rows & 15u) == 0;
                     launch_recheck(c->d_job, A.dtype_bytes, band, d_band, cap,
-                                   reinterpret_cast<unsigned int *>(c->d_small + 5), st);
+                                   reinterpret_cast<unsigned int *>(c->d_small + 5), st, vec_rows);
                     ++launches;
                     cudaEventRecord(c->ev[5], st);
                     done = true;

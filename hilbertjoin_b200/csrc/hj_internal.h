@@ -337,8 +337,10 @@ uint32_t tc_atoms(int form, uint32_t kcols);
 uint32_t tc_ksteps(int form, uint32_t kcols);
 uint32_t tc_kterms(int form, uint32_t kcols);
 // FP64 recheck of the band pairs, each against its job's rows and eps^2.
+// vec_rows: every job's rows are 16-byte aligned with d * dtype_bytes a
+// multiple of 16 (then the rows are read with 16-byte loads).
 void launch_recheck(const TcJob *d_jobs, int dtype_bytes, const uint2 *band, const unsigned long long *d_band_total,
-                    uint64_t band_cap, unsigned int *d_max_err_bits, cudaStream_t st);
+                    uint64_t band_cap, unsigned int *d_max_err_bits, cudaStream_t st, bool vec_rows = false);
 // Test hook: when non-null, the tensor-core kernel writes its dist^2 estimate
 // of every pair to dbg[ia * nb + jb] (EGO ranks). Not thread-safe.
 void set_tc_debug_output(float *dbg);

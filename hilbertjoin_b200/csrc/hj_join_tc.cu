@@ -46,6 +46,7 @@
 #include <cmath>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 #include "../../include/hj.h"
 #include "hj_common.cuh"
@@ -791,9 +792,38 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // FP64 pair test (the oracle's) on every band pair, against the pair's job
 // (BandEntry.pad); also the largest |s_hat - dist2| seen, as FP32 bits in
 // max_err_bits.
+// 16-byte loads of both rows where the rows allow it (every job's d * sizeof(TIn)
+// a multiple of 16: `vec`); the FP64 sum runs over the dims in order either way.
+template <typename TIn>
+__device__ __forceinline__ double pair_dist2(const TIn *a, const TIn *b, uint32_t d, bool vec) {
+    double acc = 0.0;
+    if (vec) {
+        constexpr uint32_t V = 16 / sizeof(TIn);
+        using Vec = typename std::conditional<sizeof(TIn) == 4, float4, double2>::type;
+        const Vec *av = reinterpret_cast<const Vec *>(a), *bv = reinterpret_cast<const Vec *>(b);
+        for (uint32_t k = 0; k < d / V; ++k) {
+            const Vec x = __ldg(av + k), y = __ldg(bv + k);
+            TIn xs[V], ys[V];
+            memcpy(xs, &x, 16);
+            memcpy(ys, &y, 16);
+#pragma unroll
+            for (uint32_t j = 0; j < V; ++j) {
+                const double df = __dsub_rn((double)xs[j], (double)ys[j]);
+                acc = __fma_rn(df, df, acc);
+            }
+        }
+        return acc;
+    }
+    for (uint32_t k = 0; k < d; ++k) {
+        const double df = __dsub_rn((double)a[k], (double)b[k]);
+        acc = __fma_rn(df, df, acc);
+    }
+    return acc;
+}
+
 template <typename TIn>
 __global__ void k_recheck(const TcJob *__restrict__ jobs, const BandEntry *__restrict__ band,
-                          const unsigned long long *band_total, uint64_t cap, unsigned int *max_err_bits) {
+                          const unsigned long long *band_total, uint64_t cap, unsigned int *max_err_bits, bool vec) {
     const uint64_t n = min((unsigned long long)cap, *band_total);
     const uint32_t lane = threadIdx.x & 31u;
     float emax = 0.f;
@@ -807,11 +837,7 @@ __global__ void k_recheck(const TcJob *__restrict__ jobs, const BandEntry *__res
             const TcJob &J = jobs[job];
             const TIn *a = static_cast<const TIn *>(J.rows_a) + (uint64_t)(e.ia - J.a_row0) * J.d;
             const TIn *b = static_cast<const TIn *>(J.rows_b) + (uint64_t)(e.jb - J.b_row0) * J.d;
-            double acc = 0.0;
-            for (uint32_t k = 0; k < J.d; ++k) {
-                const double df = __dsub_rn((double)a[k], (double)b[k]);
-                acc = __fma_rn(df, df, acc);
-            }
+            const double acc = pair_dist2(a, b, J.d, vec);
             c = acc <= J.T ? 1ull : 0ull;
             emax = fmaxf(emax, (float)fabs((double)e.s_hat - acc));
         }
@@ -1112,12 +1138,12 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
 }
 
 void launch_recheck(const TcJob *d_jobs, int dtype_bytes, const uint2 *band, const unsigned long long *d_band_total,
-                    uint64_t band_cap, unsigned int *d_max_err_bits, cudaStream_t st) {
+                    uint64_t band_cap, unsigned int *d_max_err_bits, cudaStream_t st, bool vec_rows) {
     const BandEntry *b = reinterpret_cast<const BandEntry *>(band);
     if (dtype_bytes == 8)
-        k_recheck<double><<<1184, 256, 0, st>>>(d_jobs, b, d_band_total, band_cap, d_max_err_bits);
+        k_recheck<double><<<1184, 256, 0, st>>>(d_jobs, b, d_band_total, band_cap, d_max_err_bits, vec_rows);
     else
-        k_recheck<float><<<1184, 256, 0, st>>>(d_jobs, b, d_band_total, band_cap, d_max_err_bits);
+        k_recheck<float><<<1184, 256, 0, st>>>(d_jobs, b, d_band_total, band_cap, d_max_err_bits, vec_rows);
 }
 
 void set_tc_debug_output(float *dbg) { g_dbg_out = dbg; }

@@ -55,15 +55,32 @@ __global__ void k_dim_stats_init(DimStats *s, uint32_t d, unsigned long long *ma
 // is monotone in x (IEEE division by a positive eps rounds monotonically), so
 // a dim's smallest and largest cells are those of its smallest and largest
 // coordinate; k_dim_stats_cells computes them once per dim.
+// Per-dim minima and maxima of the block's threads are combined in three
+// steps without contention: lanes of a warp whose elements fall in the same
+// dims (lanes P apart, P = d / gcd(d, V)) by shuffles; the warps' results in
+// per-warp shared arrays (warps = 1 when they would not fit: one array); the
+// arrays per dim, then one global atomic per dim and block. The largest |x|
+// and the non-finite flag are reduced over the block before their single
+// global atomic.
+constexpr uint32_t kStatsWarpArraysMaxDim = 384;  // 8 warps x 2 x d x 8 bytes <= 48 KB
+__host__ __device__ inline uint32_t gcd_u32(uint32_t a, uint32_t b) {
+    while (b) {
+        const uint32_t t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
 template <typename T, int V>
 __global__ void __launch_bounds__(256) k_dim_stats(const T *__restrict__ x, uint64_t total, uint32_t d,
                                                    DimStats *s, unsigned long long *maxabs_bits, uint32_t *bad) {
-    extern __shared__ unsigned long long shx[];  // [2][d]
-    unsigned long long *sxmin = shx, *sxmax = shx + d;
-    for (uint32_t t = threadIdx.x; t < d; t += blockDim.x) {
-        sxmin[t] = ~0ull;
-        sxmax[t] = 0ull;
-    }
+    extern __shared__ unsigned long long shx[];  // [arrays][2][d]
+    __shared__ T red_amax[8];
+    __shared__ uint32_t red_bad[8];
+    const uint32_t arrays = d <= kStatsWarpArraysMaxDim ? (blockDim.x >> 5) : 1u;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    unsigned long long *sxmin = shx + (size_t)(arrays > 1 ? warp : 0) * 2 * d, *sxmax = sxmin + d;
+    for (uint32_t t = threadIdx.x; t < arrays * 2 * d; t += blockDim.x) shx[t] = (t / d) % 2 == 0 ? ~0ull : 0ull;
     __syncthreads();
     const uint64_t threads = (uint64_t)gridDim.x * blockDim.x;
     const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -124,23 +141,57 @@ __global__ void __launch_bounds__(256) k_dim_stats(const T *__restrict__ x, uint
             }
         }
     }
+    // lanes P apart hold the same dims (k * V + j mod d depends on k mod P);
+    // min / max are idempotent, so overlapping shuffle windows are harmless
+    const uint32_t P = d / gcd_u32(d, (uint32_t)V);
+    for (uint32_t off = P; off < 32; off <<= 1) {
 #pragma unroll
-    for (int j = 0; j < V; ++j) {
-        if (!(xmin[j] <= xmax[j])) continue;  // no finite value in these dims
-        const uint32_t t = (uint32_t)((k * V + j) % d);
-        atomicMin(&sxmin[t], ordered_from_double((double)xmin[j]));
-        atomicMax(&sxmax[t], ordered_from_double((double)xmax[j]));
+        for (int j = 0; j < V; ++j) {
+            xmin[j] = fmin(xmin[j], __shfl_down_sync(0xffffffffu, xmin[j], off));
+            xmax[j] = fmax(xmax[j], __shfl_down_sync(0xffffffffu, xmax[j], off));
+        }
+    }
+    if (lane < P) {
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+            if (!(xmin[j] <= xmax[j])) continue;  // no finite value in these dims
+            const uint32_t t = (uint32_t)((k * V + j) % d);
+            atomicMin(&sxmin[t], ordered_from_double((double)xmin[j]));
+            atomicMax(&sxmax[t], ordered_from_double((double)xmax[j]));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+        lbad |= __shfl_xor_sync(0xffffffffu, lbad, o);
+    }
+    if (lane == 0) {
+        red_amax[warp] = amax;
+        red_bad[warp] = lbad;
     }
     __syncthreads();
     for (uint32_t u = threadIdx.x; u < d; u += blockDim.x) {
-        if (sxmin[u] != ~0ull) {
-            atomicMin(&s[u].xmin, sxmin[u]);
-            atomicMax(&s[u].xmax, sxmax[u]);
+        unsigned long long mn = ~0ull, mx = 0ull;
+        for (uint32_t w = 0; w < arrays; ++w) {
+            mn = min(mn, shx[(size_t)w * 2 * d + u]);
+            mx = max(mx, shx[(size_t)w * 2 * d + d + u]);
+        }
+        if (mn != ~0ull) {
+            atomicMin(&s[u].xmin, mn);
+            atomicMax(&s[u].xmax, mx);
         }
     }
-    // non-negative doubles order like their bit patterns
-    if (amax > T(0)) atomicMax(maxabs_bits, (unsigned long long)__double_as_longlong((double)amax));
-    if (lbad) atomicOr(bad, lbad);
+    if (threadIdx.x == 0) {
+        T am = T(0);
+        uint32_t b = 0;
+        for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) {
+            am = fmax(am, red_amax[w]);
+            b |= red_bad[w];
+        }
+        // non-negative doubles order like their bit patterns
+        if (am > T(0)) atomicMax(maxabs_bits, (unsigned long long)__double_as_longlong((double)am));
+        if (b) atomicOr(bad, b);
+    }
 }
 
 // Cells beyond +-2^62 cannot be represented; such inputs are rejected.
@@ -180,11 +231,12 @@ static void dim_stats_launch(const T *x, uint64_t n, uint32_t d, DimStats *dstat
     // threads * V must be a multiple of d: blocks a multiple of L
     const uint64_t dv = d / gcd_u64(d, V);
     const uint64_t L = dv / gcd_u64(dv, 256);
-    uint64_t want = std::min<uint64_t>(hj_ceil_div(total, 256 * V * 8), 148 * 8);
+    uint64_t want = std::min<uint64_t>(hj_ceil_div(total, 256 * V * 16), 148 * 4);
     if (want < 1) want = 1;
     const uint64_t blocks = hj_ceil_div(want, L) * L;
-    k_dim_stats<T, V><<<(unsigned)blocks, 256, 2 * d * sizeof(unsigned long long), st>>>(x, total, d, dstats, maxabs,
-                                                                                         bad);
+    const uint32_t arrays = d <= kStatsWarpArraysMaxDim ? 8u : 1u;
+    k_dim_stats<T, V><<<(unsigned)blocks, 256, arrays * 2 * d * sizeof(unsigned long long), st>>>(x, total, d, dstats,
+                                                                                                  maxabs, bad);
 }
 
 void launch_dim_stats(const void *x, int dtype_bytes, uint64_t n, uint32_t d, double eps, DimStats *dstats,
@@ -350,6 +402,13 @@ void launch_dim_cost(const void *x, int dtype_bytes, uint64_t n, uint32_t d, dou
 // d <= 64 FP64) take this path.
 constexpr int kPkRows = 128;
 constexpr uint32_t kPkMaxRowBytes = 512;
+// Per key position: the dim, its word and shift (word << 8 | shift), the cell
+// offset; staged in shared memory once per block so that the packing loop
+// reads one broadcast 16-byte entry per position.
+struct PkPos {
+    long long off;
+    uint32_t dim, word_shift;
+};
 
 template <typename T>
 __global__ void __launch_bounds__(kPkRows) k_pack_keys_staged(const T *__restrict__ x, uint64_t n, uint32_t d,
@@ -359,6 +418,13 @@ __global__ void __launch_bounds__(kPkRows) k_pack_keys_staged(const T *__restric
                                                               uint32_t *__restrict__ norm_key, bool vec) {
     extern __shared__ __align__(16) unsigned char pk_smem[];
     T *cols = reinterpret_cast<T *>(pk_smem);  // [d][kPkRows]
+    PkPos *prm = reinterpret_cast<PkPos *>(pk_smem + (size_t)d * kPkRows * sizeof(T));  // [d] (16-byte aligned)
+    double *cen = reinterpret_cast<double *>(prm + d);                                 // [d]
+    for (uint32_t pos = threadIdx.x; pos < d; pos += kPkRows) {
+        const uint32_t dim = grid_dim_at(g, pos);
+        prm[pos] = PkPos{g.off[dim], dim, (g.word[dim] << 8) | g.shift[dim]};
+        if (norm_key) cen[pos] = center[pos];
+    }
     const uint64_t r0 = (uint64_t)blockIdx.x * kPkRows;
     const uint32_t m = (uint32_t)(n - r0 < (uint64_t)kPkRows ? n - r0 : kPkRows);
     const uint32_t ne = m * d;
@@ -394,24 +460,24 @@ __global__ void __launch_bounds__(kPkRows) k_pack_keys_staged(const T *__restric
     const uint64_t i = r0 + t;
     uint32_t cur_word = 0, acc = 0;
     for (uint32_t pos = 0; pos < d; ++pos) {
-        const uint32_t dim = grid_dim_at(g, pos);
-        const uint32_t w = g.word[dim];
+        const PkPos pp = prm[pos];
+        const uint32_t w = pp.word_shift >> 8;
         if (w != cur_word) {
             keys_wm[(uint64_t)cur_word * n + i] = acc;
             for (uint32_t z = cur_word + 1; z < w; ++z) keys_wm[(uint64_t)z * n + i] = 0u;
             cur_word = w;
             acc = 0;
         }
-        const double c = cell_of((double)cols[dim * kPkRows + t], eps, inv_eps);
-        const long long dig = (long long)c - g.off[dim];
-        acc |= (uint32_t)dig << g.shift[dim];
+        const double c = cell_of((double)cols[pp.dim * kPkRows + t], eps, inv_eps);
+        const long long dig = (long long)c - pp.off;
+        acc |= (uint32_t)dig << (pp.word_shift & 255u);
     }
     keys_wm[(uint64_t)cur_word * n + i] = acc;
     for (uint32_t z = cur_word + 1; z < W; ++z) keys_wm[(uint64_t)z * n + i] = 0u;
     if (norm_key) {
         double sum = 0.0;
         for (uint32_t k = 0; k < d; ++k) {
-            const double v = (double)cols[k * kPkRows + t] - center[k];
+            const double v = (double)cols[k * kPkRows + t] - cen[k];
             sum = fma(v, v, sum);
         }
         const double q = floor(sum * nscale);
@@ -426,14 +492,16 @@ void launch_pack_keys(const void *x, int dtype_bytes, uint64_t n, uint32_t d, do
     const bool vec = ((uintptr_t)x & 15u) == 0;
     if ((uint64_t)d * dtype_bytes <= kPkMaxRowBytes) {
         const unsigned blocks = (unsigned)hj_ceil_div(n, kPkRows);
-        const size_t smem = (size_t)kPkRows * d * dtype_bytes;  // <= 64 KB
+        // rows (<= 64 KB; a multiple of 16 bytes), then the positions and the centre
+        const size_t smem = (size_t)kPkRows * d * dtype_bytes + (size_t)d * (sizeof(PkPos) + 8);
+        const int smem_max = (int)(64 * 1024 + (kPkMaxRowBytes / 4) * (sizeof(PkPos) + 8));
         if (dtype_bytes == 8) {
-            ensure_max_dynamic_smem((const void *)k_pack_keys_staged<double>, 64 * 1024);
+            ensure_max_dynamic_smem((const void *)k_pack_keys_staged<double>, smem_max);
             k_pack_keys_staged<double><<<blocks, kPkRows, smem, st>>>(static_cast<const double *>(x), n, d, eps,
                                                                       1.0 / eps, g,
                                                                       W, keys_wm, center, norm_scale, norm_key, vec);
         } else {
-            ensure_max_dynamic_smem((const void *)k_pack_keys_staged<float>, 64 * 1024);
+            ensure_max_dynamic_smem((const void *)k_pack_keys_staged<float>, smem_max);
             k_pack_keys_staged<float><<<blocks, kPkRows, smem, st>>>(static_cast<const float *>(x), n, d, eps,
                                                                      1.0 / eps, g, W,
                                                                      keys_wm, center, norm_scale, norm_key, vec);
@@ -979,40 +1047,113 @@ __global__ void k_group_min(const float *__restrict__ v, uint64_t npad, int grou
 // |x - center| * scale < 2^10 per coordinate, |h_t| < 2^10 (1 + 2^-11) and
 // |q| < 3 2^20 d <= 3 2^26, so every piece is below 2^12 in magnitude.
 // Ranks past n (up to npad) are padding: zero rows, q = kPadNorm, |h| = 0.
+// Shared memory of k_bc_prepare for dimension d: the rows in FP64 with an odd
+// row stride (fewer bank conflicts when a thread walks its own row), the
+// centre, per-part minima and maxima, and the FP16 bits of the residuals, the
+// centre and the pieces of q / 2.
+struct BcSmem {
+    uint32_t xstride, hstride, parts;
+    size_t o_x, o_c, o_min, o_max, o_h, o_ch, o_m, bytes;
+};
+__host__ __device__ inline BcSmem bc_smem_plan(uint32_t d) {
+    BcSmem p;
+    p.xstride = d | 1u;
+    p.hstride = d;
+    p.parts = kBcBlock / d < 8 ? kBcBlock / d : 8;
+    if (p.parts < 1) p.parts = 1;
+    p.o_x = 0;
+    p.o_c = p.o_x + (size_t)kBcBlock * p.xstride * 8;
+    p.o_min = p.o_c + (size_t)d * 8;
+    p.o_max = p.o_min + (size_t)p.parts * d * 8;
+    p.o_h = p.o_max + (size_t)p.parts * d * 8;
+    p.o_ch = p.o_h + ((size_t)kBcBlock * p.hstride * 2 + 7) / 8 * 8;
+    p.o_m = p.o_ch + ((size_t)d * 2 + 7) / 8 * 8;
+    p.bytes = p.o_m + (size_t)kBcBlock * 4 * 2;
+    return p;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ rows, uint64_t n, uint32_t d,
                                                          const double *__restrict__ center, double scale,
-                                                         uint32_t dp, uint16_t *__restrict__ op,
+                                                         uint32_t dp, bool vec, uint16_t *__restrict__ op,
                                                          float *__restrict__ norms, float *__restrict__ xn,
                                                          float4 *__restrict__ blk, float *__restrict__ cent) {
-    // [kBcBlock][d] shifted coordinates, then residuals; [d] centre; [kBcBlock][3] pieces of q / 2
-    extern __shared__ double bc_sm[];
-    double *cs = bc_sm + (size_t)kBcBlock * d;
-    double *qp = cs + d;
+    extern __shared__ __align__(16) unsigned char bc_raw[];
+    const BcSmem P = bc_smem_plan(d);
+    double *xs = reinterpret_cast<double *>(bc_raw + P.o_x);    // [kBcBlock][xstride]
+    double *cs = reinterpret_cast<double *>(bc_raw + P.o_c);    // [d]
+    double *pmin = reinterpret_cast<double *>(bc_raw + P.o_min);  // [parts][d]
+    double *pmax = reinterpret_cast<double *>(bc_raw + P.o_max);
+    uint16_t *hs = reinterpret_cast<uint16_t *>(bc_raw + P.o_h);  // [kBcBlock][d] FP16 bits of h
+    uint16_t *chs = reinterpret_cast<uint16_t *>(bc_raw + P.o_ch);  // [d] FP16 bits of c
+    uint16_t *ms = reinterpret_cast<uint16_t *>(bc_raw + P.o_m);    // [kBcBlock][4] FP16 bits of m1 m2 m3
     __shared__ float red_x[kBcBlock / 32], red_p[kBcBlock / 32];
     const uint64_t r0 = (uint64_t)blockIdx.x * kBcBlock;
     const uint32_t nr = r0 >= n ? 0u : (n - r0 < kBcBlock ? (uint32_t)(n - r0) : kBcBlock);
     const T *src = rows + r0 * d;
-    for (uint32_t e = threadIdx.x; e < nr * d; e += kBcBlock) bc_sm[e] = ((double)src[e] - center[e % d]) * scale;
+    const uint32_t ne = nr * d;
+    // 1. the block's rows (one contiguous range), shifted and scaled in FP64;
+    // element e -> (e / d, e % d) by an FP32 quotient (e < 2^14: off by at most
+    // one, corrected)
+    const float inv_d = 1.0f / (float)d;
+    auto put = [&](uint32_t e, T v) {
+        uint32_t r = (uint32_t)((float)e * inv_d);
+        int t = (int)e - (int)(r * d);
+        if (t < 0) t += (int)d, --r;
+        if (t >= (int)d) t -= (int)d, ++r;
+        xs[r * P.xstride + (uint32_t)t] = ((double)v - center[t]) * scale;
+    };
+    constexpr uint32_t V = 16 / sizeof(T);
+    using Vec = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+    uint32_t e0 = 0;
+    if (vec) {
+        const uint32_t nv = ne / V;
+        const Vec *s4 = reinterpret_cast<const Vec *>(src);
+        for (uint32_t u = threadIdx.x; u < nv; u += kBcBlock) {
+            const Vec q = __ldg(s4 + u);
+            T v[V];
+            memcpy(v, &q, 16);
+#pragma unroll
+            for (uint32_t j = 0; j < V; ++j) put(u * V + j, v[j]);
+        }
+        e0 = nv * V;
+    }
+    for (uint32_t e = e0 + threadIdx.x; e < ne; e += kBcBlock) put(e, __ldg(src + e));
     __syncthreads();
-    for (uint32_t t = threadIdx.x; t < d; t += kBcBlock) {
+    // 2. per dim the range of the block, `parts` threads per dim
+    if (threadIdx.x < P.parts * d) {
+        const uint32_t t = threadIdx.x % d, part = threadIdx.x / d;
         double lo = INFINITY, hi = -INFINITY;
-        for (uint32_t r = 0; r < nr; ++r) {
-            const double v = bc_sm[r * d + t];
+        for (uint32_t r = part; r < nr; r += P.parts) {
+            const double v = xs[r * P.xstride + t];
             lo = fmin(lo, v);
             hi = fmax(hi, v);
         }
-        cs[t] = nr ? (double)__half2float(__double2half(0.5 * lo + 0.5 * hi)) : 0.0;
+        pmin[part * d + t] = lo;
+        pmax[part * d + t] = hi;
     }
     __syncthreads();
+    for (uint32_t t = threadIdx.x; t < d; t += kBcBlock) {
+        double lo = INFINITY, hi = -INFINITY;
+        for (uint32_t part = 0; part < P.parts; ++part) {
+            lo = fmin(lo, pmin[part * d + t]);
+            hi = fmax(hi, pmax[part * d + t]);
+        }
+        const __half ch = __double2half(nr ? 0.5 * lo + 0.5 * hi : 0.0);
+        cs[t] = (double)__half2float(ch);
+        chs[t] = __half_as_ushort(ch);
+    }
+    __syncthreads();
+    // 3. per rank: residual (rounded once), q = |h|^2 + 2 h.c, |h|, pieces of q / 2
     const uint32_t r = threadIdx.x;
     float my_x = 0.f, my_p = 0.f;
-    double m1 = 0.0, m2 = 0.0, m3 = 0.0;
+    uint16_t m16[3] = {0, 0, 0};
     if (r < nr) {
         double hh = 0.0, hc = 0.0;
         for (uint32_t t = 0; t < d; ++t) {
-            const double h = (double)__half2float(__double2half(bc_sm[r * d + t] - cs[t]));
-            bc_sm[r * d + t] = h;
+            const __half hv = __double2half(xs[r * P.xstride + t] - cs[t]);
+            const double h = (double)__half2float(hv);
+            hs[r * P.hstride + t] = __half_as_ushort(hv);
             hh = fma(h, h, hh);
             hc = fma(h, cs[t], hc);
         }
@@ -1022,44 +1163,50 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
         my_x = (float)sqrt(hh) * (1.0f + 2.4e-7f);
         if (xn) xn[r0 + r] = my_x;
         const double v1 = 0.5 * q;
-        m1 = (double)__half2float(__double2half(v1 * 0x1p-15));
-        const double v2 = v1 - m1 * 0x1p15;
-        m2 = (double)__half2float(__double2half(v2 * 0x1p-4));
-        const double v3 = v2 - m2 * 0x1p4;
-        m3 = (double)__half2float(__double2half(v3 * 0x1p7));
+        const __half h1 = __double2half(v1 * 0x1p-15);
+        const double v2 = v1 - (double)__half2float(h1) * 0x1p15;
+        const __half h2 = __double2half(v2 * 0x1p-4);
+        const double v3 = v2 - (double)__half2float(h2) * 0x1p4;
+        const __half h3 = __double2half(v3 * 0x1p7);
+        m16[0] = __half_as_ushort(h1);
+        m16[1] = __half_as_ushort(h2);
+        m16[2] = __half_as_ushort(h3);
     } else {
         norms[r0 + r] = kPadNorm;
         if (xn) xn[r0 + r] = 0.f;
     }
-    qp[3 * r] = m1;
-    qp[3 * r + 1] = m2;
-    qp[3 * r + 2] = m3;
+    ms[4 * r] = m16[0];
+    ms[4 * r + 1] = m16[1];
+    ms[4 * r + 2] = m16[2];
     __syncthreads();
-    const uint32_t cpr = dp / 2;  // 16-byte chunks per row (4 dp halves)
+    // 4. the rows [h | h | c m | h a] as 16-byte chunks, consecutive threads on
+    // consecutive chunks (FP16 bits copied, no conversion)
+    const uint16_t a16[3] = {__half_as_ushort(__double2half(-0x1p15)), __half_as_ushort(__double2half(-0x1p4)),
+                             __half_as_ushort(__double2half(-0x1p-7))};
+    // chunk e = (row rr, chunk q of the row), q = (block b, chunk within it);
+    // the indices advance by kBcBlock chunks per step without divisions
+    const uint32_t cpb = dp / 8, cpr = 4 * cpb;  // 16-byte chunks per block, per row (4 dp halves)
+    const uint32_t step_r = kBcBlock / cpr, step_q = kBcBlock - step_r * cpr;
+    uint32_t rr = threadIdx.x / cpr, q = threadIdx.x - rr * cpr;
     for (uint32_t e = threadIdx.x; e < kBcBlock * cpr; e += kBcBlock) {
-        const uint32_t rr = e / cpr, q = e % cpr;
-        uint32_t w[4];
+        const uint32_t b = (q >= cpb) + (q >= 2 * cpb) + (q >= 3 * cpb), t0 = 8 * (q - b * cpb);
+        uint32_t w[4] = {0u, 0u, 0u, 0u};
+        if (rr < nr) {
 #pragma unroll
-        for (int h2 = 0; h2 < 4; ++h2) {
-            uint32_t ew = 0;
-#pragma unroll
-            for (int z = 0; z < 2; ++z) {
-                const uint32_t k = 8 * q + 2 * h2 + z, blkc = k / dp, t = k % dp;  // block, column within it
-                double v = 0.0;
-                if (rr < nr) {
-                    if (t < d)
-                        v = blkc == 2 ? cs[t] : bc_sm[rr * d + t];
-                    else if (t < d + 3 && blkc == 2)
-                        v = qp[3 * rr + (t - d)];
-                    else if (t < d + 3 && blkc == 3)
-                        v = t == d ? -0x1p15 : (t == d + 1 ? -0x1p4 : -0x1p-7);
-                }
-                // FP16 values already: the conversion is exact
-                ew |= (uint32_t)__half_as_ushort(__double2half(v)) << (16 * z);
+            for (int z = 0; z < 8; ++z) {
+                const uint32_t t = t0 + z;
+                uint32_t bits = 0;
+                if (t < d)
+                    bits = b == 2 ? chs[t] : hs[rr * P.hstride + t];
+                else if (t < d + 3)
+                    bits = b == 2 ? ms[4 * rr + (t - d)] : (b == 3 ? a16[t - d] : 0u);
+                w[z >> 1] |= bits << (16 * (z & 1));
             }
-            w[h2] = ew;
         }
         reinterpret_cast<uint4 *>(op)[(r0 + rr) * cpr + q] = make_uint4(w[0], w[1], w[2], w[3]);
+        rr += step_r;
+        q += step_q;
+        if (q >= cpr) q -= cpr, ++rr;
     }
     // block summaries: max |h|, |c|, max |q| (all rounded up)
 #pragma unroll
@@ -1090,16 +1237,18 @@ void launch_bc_prepare(const SortedSet &s, const double *center, double scale, u
                        float *xn, float4 *blk, float *cent, cudaStream_t st, int *launches) {
     if (s.npad_tc == 0) return;
     const unsigned blocks = (unsigned)(s.npad_tc / kBcBlock);
-    const size_t smem = ((size_t)kBcBlock * s.d + s.d + 3 * kBcBlock) * sizeof(double);
-    const int smem_max = (int)(((size_t)kBcBlock * kBcMaxDim + kBcMaxDim + 3 * kBcBlock) * sizeof(double));
+    const size_t smem = bc_smem_plan(s.d).bytes;
+    // the block's rows start at r0 d coordinates: 16-byte loads when that and the base allow
+    const bool vec = ((uintptr_t)s.rows & 15u) == 0 && ((uint64_t)kBcBlock * s.d * s.dtype_bytes) % 16 == 0;
+    const int smem_max = (int)bc_smem_plan(kBcMaxDim).bytes;
     if (s.dtype_bytes == 8) {
         ensure_max_dynamic_smem((const void *)k_bc_prepare<double>, smem_max);
         k_bc_prepare<double><<<blocks, kBcBlock, smem, st>>>(static_cast<const double *>(s.rows), s.n, s.d, center,
-                                                             scale, s.bc_dp, op, norms, xn, blk, cent);
+                                                             scale, s.bc_dp, vec, op, norms, xn, blk, cent);
     } else {
         ensure_max_dynamic_smem((const void *)k_bc_prepare<float>, smem_max);
         k_bc_prepare<float><<<blocks, kBcBlock, smem, st>>>(static_cast<const float *>(s.rows), s.n, s.d, center,
-                                                            scale, s.bc_dp, op, norms, xn, blk, cent);
+                                                            scale, s.bc_dp, vec, op, norms, xn, blk, cent);
     }
     if (launches) *launches += 1;
 }
