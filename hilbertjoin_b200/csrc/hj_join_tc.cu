@@ -63,12 +63,13 @@ constexpr int kChunkCols = 64;
 constexpr int kChunkGroups = kChunkCols / 32;  // 32-column groups per chunk
 constexpr int kEpiChunks = kEpiCols / kChunkCols;
 constexpr int kEpiVec = kEpiCols / 32;  // norms per lane, group minima per warp
-// From this many rows of a 32-column group on, the lanes classify their own
-// rows (32 shuffled column norms) instead of the warp walking row by row;
-// with block centring (no column norms to shuffle) always.
-constexpr int kDenseRows = 8;
-// Band slots are reserved by each epilogue warp in chunks (one atomic per
-// chunk); slots a warp leaves unused are marked with ia = kBandHole.
+// Block centring, where tiles in which near pairs are common make up much of
+// the work: the lanes classify their own rows against a 32-column group (the
+// dense path) instead of the warp walking row by row, and band slots are
+// reserved by each epilogue warp in chunks (one atomic per chunk); slots a
+// warp leaves unused are marked with ia = kBandHole. With one global centre
+// (near pairs rare) both measured slower, the row walk with one atomic per
+// band pair stays.
 constexpr uint32_t kBandChunk = 256;
 constexpr uint32_t kBandHole = 0xffffffffu;
 // 16 epilogue warps (4 per quadrant) were measured slower: at 18 warps the
@@ -654,25 +655,23 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                                 jlo = first > 0 ? (first > kEpiCols ? kEpiCols : (int)first) : 0;
                             }
                         }
-                        if ((BC || __popc(rows) >= kDenseRows) && p.dbg == nullptr) {
-                            // Many rows (tiles where neighbours are common): every lane
-                            // classifies its own row against the group's 32 columns, the
-                            // column norms broadcast by shuffles; then only the rows with
-                            // band pairs are walked, as below, to queue them.
-                            const bool mine = need && row_ok;
-                            const float *vg = v + h2 * 32;
-                            uint32_t bbits = 0, c32 = 0;
-#pragma unroll
-                            for (int j = 0; j < 32; ++j) {
-                                const float t = fmaf(-2.0f, vg[j], BC ? 0.f : __shfl_sync(0xffffffffu, nbl, j));
-                                const bool ok = mine && (unsigned)(cb + j - jlo) < (unsigned)(jhi - jlo);
-                                c32 += (ok && t <= thr_in) ? 1u : 0u;
-                                bbits |= (ok && t > thr_in && t <= thr_out) ? (1u << j) : 0u;
-                            }
-                            cnt += c32;
-                            if constexpr (BC) {
+                        if constexpr (BC) {
+                            if (p.dbg == nullptr) {
+                                // Dense path: every lane classifies its own row against the
+                                // group's 32 columns (the column norm is in the accumulator);
                                 // band entries straight from the lane's registers: ranks by a
                                 // warp prefix sum, slots from one warp-wide reservation
+                                const bool mine = need && row_ok;
+                                const float *vg = v + h2 * 32;
+                                uint32_t bbits = 0, c32 = 0;
+#pragma unroll
+                                for (int j = 0; j < 32; ++j) {
+                                    const float t = -2.0f * vg[j];
+                                    const bool ok = mine && (unsigned)(cb + j - jlo) < (unsigned)(jhi - jlo);
+                                    c32 += (ok && t <= thr_in) ? 1u : 0u;
+                                    bbits |= (ok && t > thr_in && t <= thr_out) ? (1u << j) : 0u;
+                                }
+                                cnt += c32;
                                 const uint32_t nbits = __popc(bbits);
                                 uint32_t incl = nbits;
 #pragma unroll
@@ -703,32 +702,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                                 }
                                 continue;
                             }
-                            rows = __ballot_sync(0xffffffffu, bbits != 0);
-                            while (rows) {
-                                const int L = __ffs(rows) - 1;
-                                rows &= rows - 1;
-                                if (lane == (uint32_t)L) {
-#pragma unroll
-                                    for (int q = 0; q < 8; ++q)
-                                        reinterpret_cast<float4 *>(srow)[q] = make_float4(vg[4 * q], vg[4 * q + 1],
-                                                                                          vg[4 * q + 2], vg[4 * q + 3]);
-                                }
-                                __syncwarp();
-                                const uint32_t bm = __shfl_sync(0xffffffffu, bbits, L);
-                                const float naL = __shfl_sync(0xffffffffu, na, L);
-                                const uint32_t rank = __popc(bm & ((1u << lane) - 1u));
-                                const unsigned long long k = band_reserve(__popc(bm)).at(rank);
-                                if (((bm >> lane) & 1u) && k < p.band_cap) {
-                                    BandEntry e;
-                                    e.ia = (uint32_t)(gi - (uint64_t)lane + (uint64_t)L);
-                                    e.jb = (uint32_t)(gj0 + cb + (int)lane);
-                                    e.s_hat = (naL + fmaf(-2.0f, srow[lane], nbl)) * s_unscale;
-                                    e.pad = job;
-                                    p.band[k] = e;
-                                }
-                                __syncwarp();
-                            }
-                            continue;
                         }
                         while (rows) {
                             const int L = __ffs(rows) - 1;
@@ -756,18 +729,20 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                                 p.dbg[(uint64_t)p.perm_a[giL] * p.nb + p.perm_b[gj0 + col]] = (naL + t) * s_unscale;
                             // band pairs of the row: one reservation for the warp
                             const bool isb = ok && t > tinL && t <= toutL;
-                            const uint32_t bm = __ballot_sync(0xffffffffu, isb);
-                            if (bm) {
-                                const uint32_t rank = __popc(bm & ((1u << lane) - 1u));
-                                const unsigned long long k = band_reserve(__popc(bm)).at(rank);
-                                if (isb && k < p.band_cap) {
-                                    BandEntry e;
-                                    e.ia = (uint32_t)giL;
-                                    e.jb = (uint32_t)(gj0 + col);
-                                    e.s_hat = (naL + t) * s_unscale;
-                                    e.pad = job;
-                                    p.band[k] = e;
-                                }
+                            unsigned long long k = 0;
+                            if constexpr (BC) {
+                                const uint32_t bm = __ballot_sync(0xffffffffu, isb);
+                                if (bm) k = band_reserve(__popc(bm)).at(__popc(bm & ((1u << lane) - 1u)));
+                            } else if (isb) {  // band pair: rare with one centre
+                                k = atomicAdd(p.band_total, 1ull);
+                            }
+                            if (isb && k < p.band_cap) {
+                                BandEntry e;
+                                e.ia = (uint32_t)giL;
+                                e.jb = (uint32_t)(gj0 + col);
+                                e.s_hat = (naL + t) * s_unscale;
+                                e.pad = job;
+                                p.band[k] = e;
                             }
                             __syncwarp();
                         }
@@ -778,7 +753,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             if (last_tile && it < p.n_items) item_rows(w);
         }
         if (job != 0xffffffffu) flush();
-        band_holes();
+        if constexpr (BC) band_holes();
     }
     tc_fence_before();
     __syncthreads();
