@@ -661,17 +661,24 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                                 // group's 32 columns (the column norm is in the accumulator);
                                 // band entries straight from the lane's registers: ranks by a
                                 // warp prefix sum, slots from one warp-wide reservation
-                                const bool mine = need && row_ok;
+                                // t = -2 w, so t <= thr  <=>  w >= -thr / 2 (exact scaling);
+                                // the columns the row may count form one mask per group
                                 const float *vg = v + h2 * 32;
-                                uint32_t bbits = 0, c32 = 0;
+                                const float w_in = -0.5f * thr_in, w_out = -0.5f * thr_out;
+                                const int lo = jlo - cb > 0 ? jlo - cb : 0, hi = jhi - cb < 32 ? jhi - cb : 32;
+                                const uint32_t colmask =
+                                    (need && row_ok && lo < hi)
+                                        ? ((hi >= 32 ? 0xffffffffu : (1u << hi) - 1u) & ~((1u << lo) - 1u))
+                                        : 0u;
+                                uint32_t g_in = 0, g_out = 0;
 #pragma unroll
                                 for (int j = 0; j < 32; ++j) {
-                                    const float t = -2.0f * vg[j];
-                                    const bool ok = mine && (unsigned)(cb + j - jlo) < (unsigned)(jhi - jlo);
-                                    c32 += (ok && t <= thr_in) ? 1u : 0u;
-                                    bbits |= (ok && t > thr_in && t <= thr_out) ? (1u << j) : 0u;
+                                    g_in |= vg[j] >= w_in ? (1u << j) : 0u;
+                                    g_out |= vg[j] >= w_out ? (1u << j) : 0u;
                                 }
-                                cnt += c32;
+                                g_in &= colmask;
+                                uint32_t bbits = g_out & colmask & ~g_in;
+                                cnt += __popc(g_in);
                                 const uint32_t nbits = __popc(bbits);
                                 uint32_t incl = nbits;
 #pragma unroll
