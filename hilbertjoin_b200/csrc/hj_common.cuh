@@ -125,6 +125,22 @@ HJ_DEVICE_INLINE unsigned long long warp_sum_u64(unsigned long long v) {
     return v;
 }
 
+// floor(x / eps) with x / eps the IEEE (correctly rounded) FP64 quotient --
+// the cell of the pair test's convention -- without a division in the common
+// case. With inv = fl(1 / eps), q = fl(x * inv) differs from x / eps by at
+// most |x / eps| (2u + u^2) and from fl(x / eps) by at most 3.01 u |q|
+// (u = 2^-53), so every value within 2^-50 |q| of q has the same floor as
+// fl(x / eps) whenever q - 2^-50 |q| and q + 2^-50 |q| do (the margin also
+// covers the rounding of those two bounds). Only near a cell border, where
+// they differ, is the quotient computed by division.
+__device__ __forceinline__ double cell_of(double x, double eps, double inv) {
+    const double q = x * inv;
+    const double m = fabs(q) * 8.881784197001252e-16;  // 2^-50
+    const double lo = floor(q - m);
+    if (lo == floor(q + m)) return lo;
+    return floor(x / eps);
+}
+
 }  // namespace hj
 
 // Host-side helpers ---------------------------------------------------------

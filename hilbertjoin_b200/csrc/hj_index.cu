@@ -36,7 +36,7 @@ struct BoundsArgs {
     int dtype_bytes;
     uint64_t na;       // A rows considered
     uint32_t d;
-    double eps, epsw;
+    double eps, epsw, inv;  // inv = fl(1 / eps) (cell_of)
     GridDev g;
     uint32_t W;
     int k;             // active dims requested
@@ -61,8 +61,10 @@ __device__ __forceinline__ uint32_t digit_of(const BoundsArgs &a, double cell, u
     return (uint32_t)v;
 }
 
-__device__ __forceinline__ double cell_lo(const BoundsArgs &a, double x) { return floor((x - a.epsw) / a.eps); }
-__device__ __forceinline__ double cell_hi(const BoundsArgs &a, double x) { return floor((x + a.epsw) / a.eps); }
+// floor((x -+ epsw) / eps) with the quotient rounded as FP64 division does
+// (cell_of: a multiply, and the division only next to a cell border)
+__device__ __forceinline__ double cell_lo(const BoundsArgs &a, double x) { return cell_of(x - a.epsw, a.eps, a.inv); }
+__device__ __forceinline__ double cell_hi(const BoundsArgs &a, double x) { return cell_of(x + a.epsw, a.eps, a.inv); }
 
 // -1, 0, 1: lexicographic comparison (in key order) of the lo-vectors of rows p and q.
 __device__ int cmp_lo(const BoundsArgs &a, uint64_t p, uint64_t q) {
@@ -481,6 +483,7 @@ int build_index(const SortedSet &A, const SortedSet &B, const Grid &grid, const 
     ba.d = grid.d;
     ba.eps = grid.eps;
     ba.epsw = grid.eps_wide;
+    ba.inv = 1.0 / grid.eps;
     ba.g = gdev;
     ba.W = grid.W;
     ba.k = k;

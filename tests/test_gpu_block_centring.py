@@ -205,3 +205,18 @@ def test_estimates_tighter_than_global_on_clusters(hj):
     # straddle two clusters have large residuals); typical pairs far below
     assert err_b.max() < eps * eps, (err_b.max(), eps)
     assert np.quantile(err_b, 0.99) < 0.02 * eps * eps, (np.quantile(err_b, 0.99), eps)
+
+
+def test_server_block_centring_switch(hj):
+    """The server runs its FP16 joins with one global centre unless asked for
+    block centring; with it, clustered requests at a small eps switch to block
+    centres. Counts equal the oracle's either way."""
+    from hilbertjoin_b200 import serving
+    x = tight_clusters(30000, 28, 61)
+    eps = eps_for(x, 40)
+    want = oracle.self_count_brute(x.astype(np.float64), eps)
+    for block in (False, True):
+        with serving.Server(form="fp16", max_inflight=2, block_centring=block) as srv:
+            sid = srv.upload(x)
+            res = [srv.wait(srv.submit(sid, None, eps)) for _ in range(2)]
+        assert all(r["status"] == 0 and r["count"] == want for r in res), (block, res)
