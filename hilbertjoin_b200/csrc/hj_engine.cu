@@ -1077,9 +1077,10 @@ uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dt
     uint64_t b = per_set(na) + (self ? 0 : per_set(nb));
     const uint64_t nmax = std::max(na, nb);
     b += radix_scratch_bytes(nmax) + 2 * radix_scratch_bytes(1);
-    // work list: per A tile up to kMaxCombos runs, items of a few B tiles
+    // work list: per A tile up to kMaxCombos runs, items of a few B tiles; the
+    // A rows' packed bound keys (two of W words)
     const uint64_t tiles = hj_ceil_div(std::max<uint64_t>(na, 1), kPlainTile);
-    b += tiles * (uint64_t)kMaxCombos * 8 + tiles * 64 * 16;
+    b += tiles * (uint64_t)kMaxCombos * 8 + tiles * 64 * 16 + na * W * 8;
     if (tc) {
         const double cand = (double)na * (double)nb;
         b += (uint64_t)std::max(1048576.0, cand / (bc ? 512.0 : 4096.0)) * kBandEntryBytes;

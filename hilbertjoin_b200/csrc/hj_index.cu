@@ -47,6 +47,7 @@ struct BoundsArgs {
     uint2 *runs;       // [n_tiles][kMaxCombos]
     uint32_t *nruns;   // [n_tiles]
     unsigned long long *cand;  // candidate pairs (tile granularity)
+    uint32_t *lokeys, *hikeys;  // per A row [na][W]: packed digits of cell_lo / cell_hi (k_bound_keys)
 };
 
 __device__ __forceinline__ double crd(const BoundsArgs &a, uint64_t r, uint32_t t) {
@@ -66,23 +67,53 @@ __device__ __forceinline__ uint32_t digit_of(const BoundsArgs &a, double cell, u
 __device__ __forceinline__ double cell_lo(const BoundsArgs &a, double x) { return cell_of(x - a.epsw, a.eps, a.inv); }
 __device__ __forceinline__ double cell_hi(const BoundsArgs &a, double x) { return cell_of(x + a.epsw, a.eps, a.inv); }
 
-// -1, 0, 1: lexicographic comparison (in key order) of the lo-vectors of rows p and q.
-__device__ int cmp_lo(const BoundsArgs &a, uint64_t p, uint64_t q) {
+// Per A row, the clamped digits of its cell_lo and cell_hi vectors packed like
+// the sort keys (fields in key order from the most significant bit of word 0):
+// unsigned word-by-word order of these keys is the lexicographic order of the
+// digit vectors. One thread per row, written row-major [na][W].
+__global__ void k_bound_keys(BoundsArgs a) {
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.na) return;
+    uint32_t *lo = a.lokeys + r * a.W, *hi = a.hikeys + r * a.W;
+    uint32_t cur = 0, al = 0, ah = 0;
     for (uint32_t pos = 0; pos < a.d; ++pos) {
-        const uint32_t t = grid_dim_at(a.g, pos);
-        double cp = cell_lo(a, crd(a, p, t)), cq = cell_lo(a, crd(a, q, t));
-        if (cp != cq) return cp < cq ? -1 : 1;
+        const uint32_t t = grid_dim_at(a.g, pos), w = a.g.word[t];
+        if (w != cur) {
+            lo[cur] = al;
+            hi[cur] = ah;
+            for (uint32_t z = cur + 1; z < w; ++z) lo[z] = hi[z] = 0u;
+            cur = w;
+            al = ah = 0;
+        }
+        const double x = crd(a, r, t);
+        al |= digit_of(a, cell_lo(a, x), t) << a.g.shift[t];
+        ah |= digit_of(a, cell_hi(a, x), t) << a.g.shift[t];
+    }
+    lo[cur] = al;
+    hi[cur] = ah;
+    for (uint32_t z = cur + 1; z < a.W; ++z) lo[z] = hi[z] = 0u;
+}
+
+// Word w of row p's upper key: lo digits at key positions < kt, hi digits from
+// kt on; `mw` / `mbits` describe the boundary (positions < kt fill the words
+// before mw and the bits of word mw above mbits).
+__device__ __forceinline__ uint32_t up_word(const BoundsArgs &a, uint64_t p, uint32_t w, uint32_t mw, uint32_t mbits) {
+    const uint32_t m = w < mw ? 0xffffffffu : (w > mw || mbits >= 32 ? 0u : ~((1u << mbits) - 1u));
+    return (__ldg(a.lokeys + p * a.W + w) & m) | (__ldg(a.hikeys + p * a.W + w) & ~m);
+}
+// -1, 0, 1: lexicographic comparison of the lo digit vectors of rows p and q.
+__device__ int cmp_lo(const BoundsArgs &a, uint64_t p, uint64_t q) {
+    for (uint32_t w = 0; w < a.W; ++w) {
+        const uint32_t kp = __ldg(a.lokeys + p * a.W + w), kq = __ldg(a.lokeys + q * a.W + w);
+        if (kp != kq) return kp < kq ? -1 : 1;
     }
     return 0;
 }
-// Same for the upper vectors (lo cells at key positions < k, hi cells from k on).
-__device__ int cmp_up(const BoundsArgs &a, uint64_t p, uint64_t q, int k) {
-    for (uint32_t pos = 0; pos < a.d; ++pos) {
-        const uint32_t t = grid_dim_at(a.g, pos);
-        double xp = crd(a, p, t), xq = crd(a, q, t);
-        double cp = (int)pos < k ? cell_lo(a, xp) : cell_hi(a, xp);
-        double cq = (int)pos < k ? cell_lo(a, xq) : cell_hi(a, xq);
-        if (cp != cq) return cp < cq ? -1 : 1;
+// Same for the upper vectors (lo digits at key positions < kt, hi digits from kt on).
+__device__ int cmp_up(const BoundsArgs &a, uint64_t p, uint64_t q, uint32_t mw, uint32_t mbits) {
+    for (uint32_t w = 0; w < a.W; ++w) {
+        const uint32_t kp = up_word(a, p, w, mw, mbits), kq = up_word(a, q, w, mw, mbits);
+        if (kp != kq) return kp < kq ? -1 : 1;
     }
     return 0;
 }
@@ -143,11 +174,18 @@ __global__ void __launch_bounds__(kBoundsWarps * 32) k_tile_bounds(BoundsArgs a,
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) kt = min(kt, __shfl_xor_sync(0xffffffffu, kt, o));
-    // 2. lexicographic min of lo vectors, max of upper vectors
+    // the upper key's boundary: the field of key position kt (hi from there on)
+    uint32_t mw = 0xffffffffu, mbits = 0;  // kt >= d: every position takes its lo digit
+    if ((uint32_t)kt < a.d) {
+        const uint32_t t = grid_dim_at(a.g, (uint32_t)kt);
+        mw = a.g.word[t];
+        mbits = a.g.shift[t] + a.g.bits[t];
+    }
+    // 2. lexicographic min of lo vectors, max of upper vectors (packed keys)
     uint64_t pmin = p0 + hj_umin(lane, p1 - p0 - 1), pmax = pmin;
     for (uint64_t p = p0 + lane + 32; p < p1; p += 32) {
         if (cmp_lo(a, p, pmin) < 0) pmin = p;
-        if (cmp_up(a, p, pmax, kt) > 0) pmax = p;
+        if (cmp_up(a, p, pmax, mw, mbits) > 0) pmax = p;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -155,22 +193,13 @@ __global__ void __launch_bounds__(kBoundsWarps * 32) k_tile_bounds(BoundsArgs a,
         uint64_t qmax = __shfl_xor_sync(0xffffffffu, pmax, o);
         int c1 = cmp_lo(a, qmin, pmin);
         if (c1 < 0 || (c1 == 0 && qmin < pmin)) pmin = qmin;
-        int c2 = cmp_up(a, qmax, pmax, kt);
+        int c2 = cmp_up(a, qmax, pmax, mw, mbits);
         if (c2 > 0 || (c2 == 0 && qmax < pmax)) pmax = qmax;
     }
-    // 3. packed base queries
+    // 3. packed base queries: the lo key of pmin and the upper key of pmax
     for (uint32_t w = lane; w < a.W; w += 32) {
-        qlo[w] = 0;
-        qhi[w] = 0;
-    }
-    __syncwarp();
-    for (uint32_t pos = lane; pos < a.d; pos += 32) {
-        const uint32_t t = grid_dim_at(a.g, pos);
-        double xl = crd(a, pmin, t), xu = crd(a, pmax, t);
-        uint32_t dl = digit_of(a, cell_lo(a, xl), t);
-        uint32_t du = digit_of(a, (int)pos < kt ? cell_lo(a, xu) : cell_hi(a, xu), t);
-        atomicOr(&qlo[a.g.word[t]], dl << a.g.shift[t]);
-        atomicOr(&qhi[a.g.word[t]], du << a.g.shift[t]);
+        qlo[w] = __ldg(a.lokeys + pmin * a.W + w);
+        qhi[w] = up_word(a, pmax, w, mw, mbits);
     }
     __syncwarp();
     // 4. one pair of searches per combination of the first kt dims
@@ -310,7 +339,7 @@ __global__ void k_permute_items(const WorkItem *__restrict__ in, const uint32_t 
 // Scratch slots requested through the caller's allocator.
 enum { kSlotRuns = kSlotIndexFirst, kSlotNruns, kSlotCounts, kSlotItemsTmp, kSlotItems, kSlotItemKeys, kSlotItemPerm,
        kSlotItemPermTmp, kSlotItemHist, kSlotIdxStats, kSlotSplitFlags, kSlotSplitTc, kSlotSplitFp, kSlotSplitStats,
-       kSlotShardLoad, kSlotShardCut, kSlotIndexEnd };
+       kSlotShardLoad, kSlotShardCut, kSlotBoundKeysLo, kSlotBoundKeysHi, kSlotIndexEnd };
 static_assert(kSlotIndexEnd <= kSlotIndexFirst + 32, "index-stage slots");
 
 __global__ void k_item_loads(const WorkItem *__restrict__ items, uint64_t n, uint32_t *load) {
@@ -471,7 +500,9 @@ int build_index(const SortedSet &A, const SortedSet &B, const Grid &grid, const 
     uint32_t *nruns = (uint32_t *)alloc(actx, kSlotNruns, n_tiles * sizeof(uint32_t));
     uint32_t *counts = (uint32_t *)alloc(actx, kSlotCounts, (n_tiles + 1) * sizeof(uint32_t));
     unsigned long long *stats = (unsigned long long *)alloc(actx, kSlotIdxStats, 4 * sizeof(unsigned long long));
-    if (!runs || !nruns || !counts || !stats) {
+    uint32_t *lokeys = (uint32_t *)alloc(actx, kSlotBoundKeysLo, na_eff * grid.W * sizeof(uint32_t));
+    uint32_t *hikeys = (uint32_t *)alloc(actx, kSlotBoundKeysHi, na_eff * grid.W * sizeof(uint32_t));
+    if (!runs || !nruns || !counts || !stats || !lokeys || !hikeys) {
         *err = "out of device memory (index scratch)";
         return 2;
     }
@@ -495,6 +526,9 @@ int build_index(const SortedSet &A, const SortedSet &B, const Grid &grid, const 
     ba.runs = runs;
     ba.nruns = nruns;
     ba.cand = stats;
+    ba.lokeys = lokeys;
+    ba.hikeys = hikeys;
+    k_bound_keys<<<(unsigned)hj_ceil_div(na_eff, 256), 256, 0, st>>>(ba);
     size_t smem = (size_t)kBoundsWarps * (2 * grid.W + 2 * kMaxCombos) * sizeof(uint32_t);
     if (smem > 48 * 1024) ensure_max_dynamic_smem((const void *)k_tile_bounds, (int)smem);
     k_tile_bounds<<<(unsigned)hj_ceil_div(n_tiles, kBoundsWarps), kBoundsWarps * 32, smem, st>>>(ba, n_tiles);
@@ -503,7 +537,7 @@ int build_index(const SortedSet &A, const SortedSet &B, const Grid &grid, const 
     launch_scan_u32(counts, n_tiles, stats + 2, st);
     unsigned long long hstats[4];
     cudaMemcpyAsync(hstats, stats, sizeof(hstats), cudaMemcpyDeviceToHost, st);
-    if (launches) *launches += 3;
+    if (launches) *launches += 4;
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         *err = std::string("index stage: ") + cudaGetErrorString(e);
