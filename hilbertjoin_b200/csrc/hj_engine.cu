@@ -140,7 +140,7 @@ enum {
     kSlotTmaxAA, kSlotTmaxAB, kSlotTmaxBA, kSlotTmaxBB, kSlotBand, kSlotCenter, kSlotGminA, kSlotGminB,
     kSlotItemCnt, kSlotPairKeys, kSlotPairPerm, kSlotPairTmp, kSlotPairHist, kSlotPairOut, kSlotDimCost,
     kSlotGridOrd, kSlotBcOpA, kSlotBcOpB, kSlotBcNormA, kSlotBcNormB, kSlotBcXnA, kSlotBcXnB, kSlotBcBlkA,
-    kSlotBcBlkB, kSlotBcCentA, kSlotBcCentB,
+    kSlotBcBlkB, kSlotBcCentA, kSlotBcCentB, kSlotScanTiles,
     kSlotEngineEnd
 };
 static_assert(kSlotEngineEnd <= kSlotIndexFirst, "engine slots overlap the index stage's");
@@ -795,7 +795,8 @@ static int run_pairs(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *pa
     cudaMemsetAsync(item_cnt, 0, (n_items + 1) * 4, st);
     cudaEventRecord(c->ev[6], st);
     launch_pairs_fp64(A, B, in.self, P.na_eff, P.nb_eff, T, idx, item_cnt, nullptr, nullptr, d_err, c->num_sms, st);
-    launch_scan_u32(item_cnt, n_items, c->d_small + 2, st);
+    launch_scan_u32(item_cnt, n_items, c->d_small + 2, st,
+                    (unsigned long long *)slot_alloc_impl(c, st, kSlotScanTiles, scan_scratch_bytes(n_items)));
     launches += 2;
     cudaMemcpyAsync(c->h_small + 2, c->d_small + 2, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return check_cuda("pair count");

@@ -339,7 +339,7 @@ __global__ void k_permute_items(const WorkItem *__restrict__ in, const uint32_t 
 // Scratch slots requested through the caller's allocator.
 enum { kSlotRuns = kSlotIndexFirst, kSlotNruns, kSlotCounts, kSlotItemsTmp, kSlotItems, kSlotItemKeys, kSlotItemPerm,
        kSlotItemPermTmp, kSlotItemHist, kSlotIdxStats, kSlotSplitFlags, kSlotSplitTc, kSlotSplitFp, kSlotSplitStats,
-       kSlotShardLoad, kSlotShardCut, kSlotBoundKeysLo, kSlotBoundKeysHi, kSlotIndexEnd };
+       kSlotShardLoad, kSlotShardCut, kSlotBoundKeysLo, kSlotBoundKeysHi, kSlotScanTiles, kSlotIndexEnd };
 static_assert(kSlotIndexEnd <= kSlotIndexFirst + 32, "index-stage slots");
 
 __global__ void k_item_loads(const WorkItem *__restrict__ items, uint64_t n, uint32_t *load) {
@@ -370,7 +370,8 @@ int shard_items(const IndexResult &in, int k, int K, void *(*alloc)(void *ctx, i
     unsigned long long *cut = (unsigned long long *)alloc(actx, kSlotShardCut, 4 * sizeof(unsigned long long));
     if (!load || !cut) return 2;
     k_item_loads<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(in.items, n, load);
-    launch_scan_u32(load, n, cut + 2, st);
+    launch_scan_u32(load, n, cut + 2, st,
+                    (unsigned long long *)alloc(actx, kSlotScanTiles, scan_scratch_bytes(n)));
     unsigned long long total = 0;
     cudaMemcpyAsync(&total, cut + 2, 8, cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return 3;
@@ -467,7 +468,8 @@ int split_items_by_precision(const IndexResult &in, const SortedSet &A, const So
         k_item_precision_flags<<<(unsigned)hj_ceil_div(n, 256), 256, 0, st>>>(in.items, n, A.tile_maxnorm_a,
                                                                              B.tile_maxnorm_b, c_rel, c_abs, limit,
                                                                              flags, stats + 1);
-    launch_scan_u32(flags, n, stats, st);
+    launch_scan_u32(flags, n, stats, st,
+                    (unsigned long long *)alloc(actx, kSlotScanTiles, scan_scratch_bytes(n)));
     unsigned long long h[2];
     cudaMemcpyAsync(h, stats, sizeof(h), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return 3;
@@ -534,7 +536,8 @@ int build_index(const SortedSet &A, const SortedSet &B, const Grid &grid, const 
     k_tile_bounds<<<(unsigned)hj_ceil_div(n_tiles, kBoundsWarps), kBoundsWarps * 32, smem, st>>>(ba, n_tiles);
     k_item_counts<<<(unsigned)hj_ceil_div(n_tiles, 256), 256, 0, st>>>(runs, nruns, n_tiles, chunk, counts,
                                                                      stats + 1);
-    launch_scan_u32(counts, n_tiles, stats + 2, st);
+    launch_scan_u32(counts, n_tiles, stats + 2, st,
+                    (unsigned long long *)alloc(actx, kSlotScanTiles, scan_scratch_bytes(n_tiles)));
     unsigned long long hstats[4];
     cudaMemcpyAsync(hstats, stats, sizeof(hstats), cudaMemcpyDeviceToHost, st);
     if (launches) *launches += 4;

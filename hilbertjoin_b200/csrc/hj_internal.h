@@ -256,8 +256,12 @@ void radix_sort_perm(const uint32_t *keys_wm, uint64_t n, const std::pair<uint32
 void radix_sort_perm(const uint32_t *keys_wm, uint64_t n, const std::vector<std::pair<uint32_t, uint32_t>> &passes,
                      uint32_t *perm_out, void *scratch, cudaStream_t st, int *launches);
 void launch_iota(uint32_t *p, uint64_t n, cudaStream_t st);
-// Exclusive scan of u32 entries in place (one block); total into *total if non-null.
-void launch_scan_u32(uint32_t *a, uint64_t count, unsigned long long *total, cudaStream_t st);
+// Exclusive scan of u32 entries in place; total into *total if non-null. With
+// `tile_sums` (scan_scratch_bytes(count) of device scratch) it runs over many
+// blocks, else in one block.
+size_t scan_scratch_bytes(uint64_t count);
+void launch_scan_u32(uint32_t *a, uint64_t count, unsigned long long *total, cudaStream_t st,
+                     unsigned long long *tile_sums = nullptr);
 
 // Gathers the sorted layouts of a set (flags select the layouts to build).
 enum GatherFlags : uint32_t { kGatherRows = 1, kGatherKeys = 2, kGatherPlain = 4, kGatherTf32 = 8, kGatherBf16 = 16,

@@ -812,8 +812,92 @@ void ensure_max_dynamic_smem(const void *func, int bytes) {
     }
 }
 
-void launch_scan_u32(uint32_t *a, uint64_t count, unsigned long long *total, cudaStream_t st) {
-    k_scan_u32<<<1, 1024, 0, st>>>(a, count, total);
+// Multi-block exclusive scan (u32 values, u32 results as the single-block scan's,
+// u64 total): per 2048-entry tile a local scan in shared memory and its sum;
+// the tile sums scanned by one block; the tile offsets added.
+constexpr uint32_t kScanTile = 2048;
+
+__global__ void __launch_bounds__(256) k_scan_tiles(uint32_t *a, uint64_t count, unsigned long long *tile_sums) {
+    __shared__ uint32_t sv[kScanTile];
+    __shared__ unsigned long long wsum[8];
+    const uint64_t base = (uint64_t)blockIdx.x * kScanTile;
+    for (uint32_t j = threadIdx.x; j < kScanTile; j += 256) sv[j] = base + j < count ? a[base + j] : 0u;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t vals[8];
+    unsigned long long run = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        vals[k] = sv[8 * threadIdx.x + k];
+        run += vals[k];
+    }
+    unsigned long long incl = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    unsigned long long woff = 0, tot = 0;
+    for (uint32_t w = 0; w < 8; ++w) {
+        if (w < warp) woff += wsum[w];
+        tot += wsum[w];
+    }
+    unsigned long long e = woff + incl - run;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        sv[8 * threadIdx.x + k] = (uint32_t)e;
+        e += vals[k];
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < kScanTile; j += 256)
+        if (base + j < count) a[base + j] = sv[j];
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+// Exclusive scan of n u64 tile sums in place (one block), total into *total.
+__global__ void __launch_bounds__(1024) k_scan_u64_one(unsigned long long *v, uint64_t n,
+                                                       unsigned long long *total_out) {
+    __shared__ unsigned long long part[1024];
+    const uint64_t per = hj_ceil_div(n, 1024);
+    const uint64_t b = threadIdx.x * per, e = b + per < n ? b + per : n;
+    unsigned long long s = 0;
+    for (uint64_t i = b; i < e; ++i) s += v[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        unsigned long long x = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0ull;
+        __syncthreads();
+        part[threadIdx.x] += x;
+        __syncthreads();
+    }
+    unsigned long long run = threadIdx.x ? part[threadIdx.x - 1] : 0ull;
+    for (uint64_t i = b; i < e; ++i) {
+        const unsigned long long x = v[i];
+        v[i] = run;
+        run += x;
+    }
+    if (total_out && threadIdx.x == 1023) *total_out = part[1023];
+}
+
+__global__ void k_scan_add(uint32_t *a, uint64_t count, const unsigned long long *tile_off) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) a[i] += (uint32_t)tile_off[i / kScanTile];
+}
+
+size_t scan_scratch_bytes(uint64_t count) { return hj_ceil_div(count, kScanTile) * sizeof(unsigned long long); }
+
+void launch_scan_u32(uint32_t *a, uint64_t count, unsigned long long *total, cudaStream_t st,
+                     unsigned long long *sums) {
+    const uint64_t tiles = hj_ceil_div(count, kScanTile);
+    if (tiles <= 1 || !sums) {  // small, or no scratch: the single-block scan
+        k_scan_u32<<<1, 1024, 0, st>>>(a, count, total);
+        return;
+    }
+    k_scan_tiles<<<(unsigned)tiles, 256, 0, st>>>(a, count, sums);
+    k_scan_u64_one<<<1, 1024, 0, st>>>(sums, tiles, total);
+    k_scan_add<<<(unsigned)hj_ceil_div(count, 256), 256, 0, st>>>(a, count, sums);
 }
 
 void launch_iota(uint32_t *p, uint64_t n, cudaStream_t st) {
