@@ -809,28 +809,32 @@ __global__ void k_recheck(const TcJob *__restrict__ jobs, const BandEntry *__res
     const uint64_t n = min((unsigned long long)cap, *band_total);
     const uint32_t lane = threadIdx.x & 31u;
     float emax = 0.f;
-    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < n; i0 += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t i = i0 + threadIdx.x;
-        unsigned long long c = 0;
-        uint32_t job = 0xffffffffu;
-        const BandEntry e = i < n ? band[i] : BandEntry{kBandHole, 0, 0.f, 0};
-        if (e.ia != kBandHole) {
-            job = e.pad;
-            const TcJob &J = jobs[job];
-            const TIn *a = static_cast<const TIn *>(J.rows_a) + (uint64_t)(e.ia - J.a_row0) * J.d;
-            const TIn *b = static_cast<const TIn *>(J.rows_b) + (uint64_t)(e.jb - J.b_row0) * J.d;
-            const double acc = pair_dist2(a, b, J.d, vec);
-            c = acc <= J.T ? 1ull : 0ull;
-            emax = fmaxf(emax, (float)fabs((double)e.s_hat - acc));
+    // counts accumulate per thread while its entries stay in one job (a launch of
+    // one join: always), flushed when the job changes and once at the end
+    unsigned long long c_acc = 0;
+    uint32_t cur = 0xffffffffu;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const BandEntry e = band[i];
+        if (e.ia == kBandHole) continue;  // a slot reserved and left unused
+        const TcJob &J = jobs[e.pad];
+        const TIn *a = static_cast<const TIn *>(J.rows_a) + (uint64_t)(e.ia - J.a_row0) * J.d;
+        const TIn *b = static_cast<const TIn *>(J.rows_b) + (uint64_t)(e.jb - J.b_row0) * J.d;
+        const double acc = pair_dist2(a, b, J.d, vec);
+        if (e.pad != cur) {
+            if (c_acc) atomicAdd(jobs[cur].count, c_acc);
+            cur = e.pad;
+            c_acc = 0;
         }
-        // one atomic per warp when the warp's entries share a job (the usual case)
-        const uint32_t j0 = __shfl_sync(0xffffffffu, job, 0);
-        if (__all_sync(0xffffffffu, job == j0 || job == 0xffffffffu)) {
-            c = warp_sum_u64(c);
-            if (lane == 0 && c) atomicAdd(jobs[j0].count, c);
-        } else if (c) {
-            atomicAdd(jobs[job].count, c);
-        }
+        c_acc += acc <= J.T ? 1ull : 0ull;
+        emax = fmaxf(emax, (float)fabs((double)e.s_hat - acc));  // NaN estimates (not kept) are skipped
+    }
+    // one atomic per warp when the warp's lanes end in the same job (the usual case)
+    const uint32_t j0 = __shfl_sync(0xffffffffu, cur, 0);
+    if (__all_sync(0xffffffffu, cur == j0 || c_acc == 0)) {
+        const unsigned long long c = warp_sum_u64(c_acc);
+        if (lane == 0 && c) atomicAdd(jobs[j0].count, c);
+    } else if (c_acc) {
+        atomicAdd(jobs[cur].count, c_acc);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) emax = fmaxf(emax, __shfl_xor_sync(0xffffffffu, emax, o));
