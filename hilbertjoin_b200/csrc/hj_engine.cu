@@ -319,15 +319,16 @@ static int ensure_plain_tiles(Ctx *c, cudaStream_t st, SortedSet *s, bool is_b, 
     return check_cuda("plain layout");
 }
 
-// Per-block-centred FP16 operands of a sorted set (HJ_CENTRING_BLOCK): the
-// operand rows whose windows serve as A and as B, q and |h| per rank, block
-// summaries and centres. scale = the global form's operand scale times
-// 2^-kBcScaleShift.
+// Per-block-centred FP16 / TF32 operands of a sorted set (HJ_CENTRING_BLOCK):
+// the operand rows whose windows serve as A and as B, q and |h| per rank,
+// block summaries and centres. scale = the FP16 form's operand scale times
+// 2^-kBcScaleShift (the largest coordinate below 2^10, for both forms).
 static int prepare_block_centring(Ctx *c, cudaStream_t st, SortedSet *s, bool is_b, const double *center,
-                                  double scale, int *launches) {
+                                  double scale, int form, int *launches) {
     const uint64_t npad = s->npad_tc, nblk = npad / kBcBlock;
-    s->bc_dp = bc_dp(s->d);
-    s->bc_op = (uint16_t *)slot_alloc_impl(c, st, is_b ? kSlotBcOpB : kSlotBcOpA, npad * 4 * s->bc_dp * 2);
+    s->bc_form = form;
+    s->bc_dp = bc_dp(s->d, form);
+    s->bc_op = slot_alloc_impl(c, st, is_b ? kSlotBcOpB : kSlotBcOpA, npad * 4 * s->bc_dp * bc_elem_bytes(form));
     s->bc_norms = (float *)slot_alloc_impl(c, st, is_b ? kSlotBcNormB : kSlotBcNormA, npad * 4);
     s->bc_xn = (float *)slot_alloc_impl(c, st, is_b ? kSlotBcXnB : kSlotBcXnA, npad * 4);
     s->bc_blk = (float4 *)slot_alloc_impl(c, st, is_b ? kSlotBcBlkB : kSlotBcBlkA, nblk * sizeof(float4));
@@ -574,18 +575,19 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
         // (FP16 form, d <= 64) when asked for, or when the global centre would
         // send more than an eighth of the block pairs to the FP64 kernel.
         const int centring = opts ? opts->tc_centring : HJ_CENTRING_AUTO;
-        const bool bc_ok = form == HJ_FORM_TC_FP16 && d <= kBcMaxDim;
-        const double bc_scale = std::ldexp(A.op_scale, -kBcScaleShift);
+        const bool bc_ok = (form == HJ_FORM_TC_FP16 || form == HJ_FORM_TC_TF32) && d <= kBcMaxDim;
+        // block-centred operands of both forms: the largest coordinate below 2^10
+        const double bc_scale = std::ldexp(P.op_scale, -kBcScaleShift);
         auto enable_bc = [&]() -> int {
-            if (int r = prepare_block_centring(c, st, &A, false, A.center, bc_scale, &launches)) return r;
+            if (int r = prepare_block_centring(c, st, &A, false, A.center, bc_scale, form, &launches)) return r;
             if (in.self) {
-                B.bc_op = A.bc_op, B.bc_dp = A.bc_dp, B.bc_norms = A.bc_norms, B.bc_xn = A.bc_xn;
-                B.bc_blk = A.bc_blk, B.bc_cent = A.bc_cent;
-            } else if (int r = prepare_block_centring(c, st, &B, true, B.center, bc_scale, &launches)) {
+                B.bc_op = A.bc_op, B.bc_dp = A.bc_dp, B.bc_form = A.bc_form, B.bc_norms = A.bc_norms;
+                B.bc_xn = A.bc_xn, B.bc_blk = A.bc_blk, B.bc_cent = A.bc_cent;
+            } else if (int r = prepare_block_centring(c, st, &B, true, B.center, bc_scale, form, &launches)) {
                 return r;
             }
             bc = true;
-            bck = bc_constants(d, T, bc_scale);
+            bck = bc_constants(form, d, T, bc_scale);
             return HJ_OK;
         };
         // the job in the units of the operands in use (block centring: its own
@@ -594,13 +596,13 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
             fill_tc_job(c->h_job, form, d, T, bc ? bc_scale : A.op_scale, maxabs, 0, na_eff, 0, nb_eff, in.self,
                         d_count, A.rows, B.rows, &c_rel, &c_abs);
             if (bc) {
-                c->h_job->ka = tc_atoms(form, bc_cols(d));
-                c->h_job->ksteps = tc_ksteps(form, bc_cols(d));
+                c->h_job->ka = tc_atoms(form, bc_cols(d, form));
+                c->h_job->ksteps = tc_ksteps(form, bc_cols(d, form));
             }
             cudaMemcpyAsync(c->d_job, c->h_job, sizeof(TcJob), cudaMemcpyHostToDevice, st);
         };
         if (centring == HJ_CENTRING_BLOCK) {
-            if (!bc_ok) return fail(HJ_ERR_UNSUPPORTED, "per-block centring needs the FP16 form and d <= 64");
+            if (!bc_ok) return fail(HJ_ERR_UNSUPPORTED, "per-block centring needs the FP16 or TF32 form and d <= 64");
             if (int r = enable_bc()) return r;
         }
         // the FP16 form works in scaled units: norms, eps^2 and the bound times op_scale^2
@@ -1064,7 +1066,7 @@ uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dt
                                     bool block_centring) {
     const uint64_t W = (6ull * d + 31) / 32 + 1;
     const bool tc = form_is_tc(form) || form == HJ_FORM_AUTO;
-    const bool bc = block_centring && (form == HJ_FORM_TC_FP16 || form == HJ_FORM_AUTO) && d <= kBcMaxDim;
+    const bool bc = block_centring && form != HJ_FORM_PLAIN_FP64 && form != HJ_FORM_TC_BF16X3 && d <= kBcMaxDim;
     auto per_set = [&](uint64_t n) -> uint64_t {
         const uint64_t npad = hj_ceil_div(std::max<uint64_t>(n, 1), kTcTileB) * kTcTileB;
         uint64_t b = n * d * (uint64_t)dtype_bytes;          // sorted rows
@@ -1072,7 +1074,7 @@ uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dt
         b += npad * d * 8;                                    // plain FP64 tiles (plain form or routed items)
         if (tc) b += npad * (hj_ceil_div(d, 64) * 64) * 4 + npad * 8;  // operands (widest form), norms
         if (bc)  // block-centred operand rows, q, |h|, blocks
-            b += npad * 4 * bc_dp(d) * 2 + npad * 8 + (npad / kBcBlock) * (16 + kBcCentStride * 4);
+            b += npad * 4 * bc_dp(d, HJ_FORM_TC_TF32) * 4 + npad * 8 + (npad / kBcBlock) * (16 + kBcCentStride * 4);
         return b;
     };
     uint64_t b = per_set(na) + (self ? 0 : per_set(nb));

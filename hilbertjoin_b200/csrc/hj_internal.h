@@ -105,26 +105,29 @@ struct SortedSet {
     float *group_minnorm = nullptr;   // per 32-row group: min |x - center|^2
     uint64_t npad_tc = 0;
     uint32_t kpad_tf32 = 0, kpad_bf16 = 0;
-    // per-block centring of the FP16 operands (HJ_CENTRING_BLOCK; see BcConsts):
-    // [npad][4 bc_dp] rows; the B operand is the window at column 0, the A operand
-    // the window at column bc_dp, both 3 bc_dp wide
-    uint16_t *bc_op = nullptr;
+    // per-block centring of the FP16 / TF32 operands (HJ_CENTRING_BLOCK; see
+    // BcConsts): [npad][4 bc_dp] rows (FP16, or TF32 values in FP32 containers);
+    // the B operand is the window at column 0, the A operand the window at column
+    // bc_dp, both 3 bc_dp wide
+    void *bc_op = nullptr;
     uint32_t bc_dp = 0;
+    int bc_form = 0;
     float *bc_norms = nullptr;    // q = |h|^2 + 2 h.c per rank (FP32; padding rows kPadNorm)
     float *bc_xn = nullptr;       // |h| per rank, rounded up
     float4 *bc_blk = nullptr;     // per 128-rank block: {max |h|, |c|, max |q|, 0}, rounded up
     float *bc_cent = nullptr;     // per block: c in FP32 (FP16 values), kBcCentStride floats, zero padded
 };
 
-// Per-block centring of the FP16 operands. Every 128-rank block of a sorted
-// set (one A tile, half a B tile) gets a centre c whose coordinates are FP16
-// values in the operand units ((x - center) * scale, the largest coordinate
-// below 2^10), the midpoint of the block's range rounded to FP16; every rank
-// is stored as that centre plus its residual h = fl16(x - c). With
-// q = |h|^2 + 2 h.c per rank and m1 2^15 + m2 2^4 + m3 2^-7 = q / 2 (three
-// FP16 pieces, to 2^-33 |q|), a row holds four blocks of dp = roundup(d + 3, 8)
-// columns (zero padded),
-//     [h | h | c m1 m2 m3 | h a1 a2 a3],   (a1, a2, a3) = (-2^15, -2^4, -2^-7),
+// Per-block centring of the FP16 (or TF32) operands. Every 128-rank block of
+// a sorted set (one A tile, half a B tile) gets a centre c whose coordinates
+// are FP16 (or TF32) values in the operand units ((x - center) * scale, the
+// largest coordinate below 2^10), the midpoint of the block's range rounded;
+// every rank is stored as that centre plus its residual h = fl(x - c),
+// rounded to the operand type. With q = |h|^2 + 2 h.c
+// per rank and three pieces of q / 2 (FP16: m1 2^15 + m2 2^4 + m3 2^-7; TF32:
+// m1 + m2 + m3; to 2^-33 |q|), a row holds four blocks of dp = roundup(d + 3,
+// 8) columns (TF32: roundup(d + 3, 4); zero padded),
+//     [h | h | c m1 m2 m3 | h a1 a2 a3],   (a1, a2, a3) = (-2^15, -2^4, -2^-7) (TF32: -1, -1, -1),
 // and the operands are two windows of 3 dp columns of the same rows:
 //     B = columns [0, 3dp) = [h | h | c m],   A = columns [dp, 4dp) = [h | c m | h a].
 // Column by column the products are h_i.h_j, c_i.h_j (m_i meets B's zero pad),
@@ -143,8 +146,13 @@ constexpr uint32_t kBcBlock = 128;      // ranks per centring block (= kTcTileA,
 constexpr uint32_t kBcMaxDim = 64;      // dp <= 72: windows of <= 216 columns
 constexpr uint32_t kBcCentStride = 64;  // floats per block in bc_cent
 constexpr int kBcScaleShift = 5;        // operand scale of the global form times 2^-5
-inline uint32_t bc_dp(uint32_t d) { return (d + 3 + 7) / 8 * 8; }
-inline uint32_t bc_cols(uint32_t d) { return 3 * bc_dp(d); }  // columns of an operand window
+// block width of the rows: 16-byte multiples (TMA column offsets), FP16 8, TF32 4 columns
+inline uint32_t bc_dp(uint32_t d, int form) {
+    const uint32_t g = form == HJ_FORM_TC_TF32 ? 4u : 8u;
+    return (d + 3 + g - 1) / g * g;
+}
+inline uint32_t bc_cols(uint32_t d, int form) { return 3 * bc_dp(d, form); }  // columns of an operand window
+inline uint32_t bc_elem_bytes(int form) { return form == HJ_FORM_TC_TF32 ? 4u : 2u; }
 struct BcConsts {
     float kp21;     // 2 kpad_bc 2^-22: the MMA accumulation error of w per unit of S, doubled for s
     float eps;      // eps in operand units, rounded up
@@ -172,14 +180,14 @@ __host__ __device__ inline float bc_tau(float xa, float ca, float pa, float xb, 
     if (S_out) *S_out = S;
     return 1.25f * fmaf(2.0f, E, fmaf(2.0f * k.eps, rho, fmaf(2.0f * rho, rho, k.theta_t)));
 }
-// Fills the constants for dimension d, eps^2 = T (caller units) and the FP16
-// operand scale.
-BcConsts bc_constants(uint32_t d, double T, double op_scale);
+// Fills the constants for form (FP16 or TF32), dimension d, eps^2 = T (caller
+// units) and the block-centred operand scale.
+BcConsts bc_constants(int form, uint32_t d, double T, double op_scale);
 // Block centres, the operand rows ([npad][4 dp]), q, |h| and block summaries
 // of a sorted set from its sorted rows. center = the global per-dim shift,
 // scale = the block-centred operand scale.
-void launch_bc_prepare(const SortedSet &s, const double *center, double scale, uint16_t *op, float *norms,
-                       float *xn, float4 *blk, float *cent, cudaStream_t st, int *launches);
+void launch_bc_prepare(const SortedSet &s, const double *center, double scale, void *op, float *norms, float *xn,
+                       float4 *blk, float *cent, cudaStream_t st, int *launches);
 
 constexpr float kPadNorm = 1.0e30f;
 
@@ -327,9 +335,9 @@ void fill_tc_job(TcJob *j, int form, uint32_t d, double T, double op_scale, doub
 // A and B describe the operand matrices (layout pointers, npad_tc rows, kpad,
 // norms and their tile maxima and group minima); their d is the largest of the
 // jobs'. na0 / nb0: job 0's counted ranks (debug output only).
-// With bc non-null (FP16 form, one job): the per-block-centred operands of A
-// and B (their windows) and summaries; the job's ka and ksteps must be the
-// ones of bc_cols(d) columns (tc_atoms, tc_ksteps).
+// With bc non-null (FP16 or TF32 form, one job): the per-block-centred
+// operands of A and B (their windows) and summaries; the job's ka and ksteps
+// must be the ones of bc_cols(d, form) columns (tc_atoms, tc_ksteps).
 int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob *d_jobs, uint64_t na0, uint64_t nb0,
                    const IndexResult &idx, uint2 *band, uint64_t band_cap, unsigned long long *d_band_total,
                    uint32_t *d_err, int num_sms, cudaStream_t st, std::string *err, const BcConsts *bc = nullptr,

@@ -973,8 +973,8 @@ uint32_t tc_kterms(int form, uint32_t kcols) { return tc_ksteps(form, kcols) * (
 //     the differences of FP16 values exact or rounded once: 16 * 2^-24;
 //   theta_t: the FP64 pair test sums d squares of exact differences with FMAs,
 //     relative error below (d + 2) 2^-53 of dist2 ~ eps^2: 2 (d + 2) 2^-53 T.
-BcConsts bc_constants(uint32_t d, double T, double op_scale) {
-    const double s2 = op_scale * op_scale, kpad = (double)tc_kterms(HJ_FORM_TC_FP16, bc_cols(d));
+BcConsts bc_constants(int form, uint32_t d, double T, double op_scale) {
+    const double s2 = op_scale * op_scale, kpad = (double)tc_kterms(form, bc_cols(d, form));
     auto up = [](double v) {
         const float f = (float)v;
         return (double)f >= v ? f : std::nextafter(f, INFINITY);
@@ -983,7 +983,12 @@ BcConsts bc_constants(uint32_t d, double T, double op_scale) {
     k.kp21 = up(2.0 * kpad * std::ldexp(1.0, -22));
     k.eps = up(std::sqrt(T * s2) * (1.0 + 1e-12));
     k.rho_u = up(1.001 * std::ldexp(1.0, -11));
-    k.rho_c = up(2.0 * std::sqrt((double)d) * (std::ldexp(1.0, -25) + std::ldexp(1.0, -37)));
+    // the subnormal spacing of the operand type (half of it per rounding: FP16
+    // 2^-25, TF32 2^-150) and the FP64 shift of coordinates below 2^10 (2^-52 of
+    // 2^10, generously 2^-37)
+    const double floor_abs =
+        (form == HJ_FORM_TC_FP16 ? std::ldexp(1.0, -25) : std::ldexp(1.0, -149)) + std::ldexp(1.0, -37);
+    k.rho_c = up(2.0 * std::sqrt((double)d) * floor_abs);
     k.u_norm = up(std::ldexp(1.0, -23) + std::ldexp(1.0, -33));
     k.u_d = up(16.0 * std::ldexp(1.0, -24));
     // + the absolute floor of the q / 2 split (2^-32 in w, 2^-31 in s, twice in tau)
@@ -1030,11 +1035,12 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
                    uint32_t *d_err, int num_sms, cudaStream_t st, std::string *err, const BcConsts *bc,
                    unsigned long long *d_band_holes) {
     if (idx.n_items == 0) return 0;
-    if (bc && (form != HJ_FORM_TC_FP16 || A.d > kBcMaxDim || !A.bc_op || !B.bc_op || A.bc_dp != B.bc_dp)) {
-        *err = "per-block centring needs the FP16 form, d <= 64 and the centred layouts";
+    if (bc && ((form != HJ_FORM_TC_FP16 && form != HJ_FORM_TC_TF32) || A.d > kBcMaxDim || !A.bc_op || !B.bc_op ||
+               A.bc_dp != B.bc_dp || A.bc_form != form || B.bc_form != form)) {
+        *err = "per-block centring needs the FP16 or TF32 form, d <= 64 and the centred layouts";
         return 1;
     }
-    const TcLayout L = tc_layout(form, bc ? bc_cols(A.d) : A.d);
+    const TcLayout L = tc_layout(form, bc ? bc_cols(A.d, form) : A.d);
     if (L.nst < 2) {
         *err = "dimension too large for the tensor-core kernel";
         return 1;
@@ -1043,8 +1049,10 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
     if (bc) {
         // rows of 4 dp columns; A reads the window from column dp (the producer's
         // x offset), B from column 0; past the row end the copy fills zeros
-        if (!make_map(&ma, A.bc_op, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, A.npad_tc, 4 * A.bc_dp, kTcTileA, err)) return 1;
-        if (!make_map(&mb, B.bc_op, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, B.npad_tc, 4 * B.bc_dp, kTcTileB, err)) return 1;
+        const CUtensorMapDataType ty =
+            form == HJ_FORM_TC_TF32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+        if (!make_map(&ma, A.bc_op, ty, A.npad_tc, 4 * A.bc_dp, kTcTileA, err)) return 1;
+        if (!make_map(&mb, B.bc_op, ty, B.npad_tc, 4 * B.bc_dp, kTcTileB, err)) return 1;
         ma2 = ma;
         mb2 = mb;
     } else if (form == HJ_FORM_TC_TF32) {
@@ -1102,7 +1110,10 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
     }
     uint64_t grid = (uint64_t)num_sms;
     if (grid > idx.n_items) grid = idx.n_items;
-    if (bc) {
+    if (bc && form == HJ_FORM_TC_TF32) {
+        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_TF32, true>, 225 * 1024);
+        k_join_tc<HJ_FORM_TC_TF32, true><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
+    } else if (bc) {
         ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_FP16, true>, 225 * 1024);
         k_join_tc<HJ_FORM_TC_FP16, true><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
     } else if (form == HJ_FORM_TC_TF32) {

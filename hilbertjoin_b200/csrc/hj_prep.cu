@@ -952,6 +952,7 @@ __device__ __forceinline__ void store_row_chunk(T *row, uint32_t k0, uint32_t d,
     }
 }
 
+
 __device__ __forceinline__ float to_tf32_rn(float v) {
     uint32_t u;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(v));
@@ -1116,15 +1117,36 @@ __global__ void k_group_min(const float *__restrict__ v, uint64_t npad, int grou
 // |x - center| * scale < 2^10 per coordinate, |h_t| < 2^10 (1 + 2^-11) and
 // |q| < 3 2^20 d <= 3 2^26, so every piece is below 2^12 in magnitude.
 // Ranks past n (up to npad) are padding: zero rows, q = kPadNorm, |h| = 0.
-// Shared memory of k_bc_prepare for dimension d: the rows in FP64 with an odd
-// row stride (fewer bank conflicts when a thread walks its own row), the
-// centre, per-part minima and maxima, and the FP16 bits of the residuals, the
-// centre and the pieces of q / 2.
+// Operand element of the block-centred rows: FP16 bits, or a TF32 value in an
+// FP32 container (rounded to nearest through FP32; the error stays within the
+// 2^-11 relative radius the bound allows, with its 1.001 margin).
+template <int OP> struct BcElem;
+template <> struct BcElem<2> {  // FP16
+    using E = uint16_t;
+    __device__ static E round(double v, double *back) {
+        const __half h = __double2half(v);
+        *back = (double)__half2float(h);
+        return __half_as_ushort(h);
+    }
+};
+template <> struct BcElem<0> {  // TF32
+    using E = uint32_t;
+    __device__ static E round(double v, double *back) {
+        const float f = to_tf32_rn((float)v);
+        *back = (double)f;
+        return __float_as_uint(f);
+    }
+};
+
+// Shared memory of k_bc_prepare for dimension d and element size eb: the rows
+// in FP64 with an odd row stride (fewer bank conflicts when a thread walks its
+// own row), the centre, per-part minima and maxima, and the operand bits of the
+// residuals, the centre and the pieces of q / 2.
 struct BcSmem {
     uint32_t xstride, hstride, parts;
     size_t o_x, o_c, o_min, o_max, o_h, o_ch, o_m, bytes;
 };
-__host__ __device__ inline BcSmem bc_smem_plan(uint32_t d) {
+__host__ __device__ inline BcSmem bc_smem_plan(uint32_t d, uint32_t eb) {
     BcSmem p;
     p.xstride = d | 1u;
     p.hstride = d;
@@ -1135,27 +1157,30 @@ __host__ __device__ inline BcSmem bc_smem_plan(uint32_t d) {
     p.o_min = p.o_c + (size_t)d * 8;
     p.o_max = p.o_min + (size_t)p.parts * d * 8;
     p.o_h = p.o_max + (size_t)p.parts * d * 8;
-    p.o_ch = p.o_h + ((size_t)kBcBlock * p.hstride * 2 + 7) / 8 * 8;
-    p.o_m = p.o_ch + ((size_t)d * 2 + 7) / 8 * 8;
-    p.bytes = p.o_m + (size_t)kBcBlock * 4 * 2;
+    p.o_ch = p.o_h + ((size_t)kBcBlock * p.hstride * eb + 7) / 8 * 8;
+    p.o_m = p.o_ch + ((size_t)d * eb + 7) / 8 * 8;
+    p.bytes = p.o_m + (size_t)kBcBlock * 4 * eb;
     return p;
 }
 
-template <typename T>
+template <typename T, int OP>
 __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ rows, uint64_t n, uint32_t d,
                                                          const double *__restrict__ center, double scale,
-                                                         uint32_t dp, bool vec, uint16_t *__restrict__ op,
+                                                         uint32_t dp, bool vec, void *__restrict__ op_out,
                                                          float *__restrict__ norms, float *__restrict__ xn,
                                                          float4 *__restrict__ blk, float *__restrict__ cent) {
+    using El = BcElem<OP>;
+    using E = typename El::E;
+    constexpr uint32_t kEpc = 16 / sizeof(E);  // elements per 16-byte chunk
     extern __shared__ __align__(16) unsigned char bc_raw[];
-    const BcSmem P = bc_smem_plan(d);
+    const BcSmem P = bc_smem_plan(d, sizeof(E));
     double *xs = reinterpret_cast<double *>(bc_raw + P.o_x);    // [kBcBlock][xstride]
     double *cs = reinterpret_cast<double *>(bc_raw + P.o_c);    // [d]
     double *pmin = reinterpret_cast<double *>(bc_raw + P.o_min);  // [parts][d]
     double *pmax = reinterpret_cast<double *>(bc_raw + P.o_max);
-    uint16_t *hs = reinterpret_cast<uint16_t *>(bc_raw + P.o_h);  // [kBcBlock][d] FP16 bits of h
-    uint16_t *chs = reinterpret_cast<uint16_t *>(bc_raw + P.o_ch);  // [d] FP16 bits of c
-    uint16_t *ms = reinterpret_cast<uint16_t *>(bc_raw + P.o_m);    // [kBcBlock][4] FP16 bits of m1 m2 m3
+    E *hs = reinterpret_cast<E *>(bc_raw + P.o_h);    // [kBcBlock][d] operand bits of h
+    E *chs = reinterpret_cast<E *>(bc_raw + P.o_ch);  // [d] operand bits of c
+    E *ms = reinterpret_cast<E *>(bc_raw + P.o_m);    // [kBcBlock][4] operand bits of m1 m2 m3
     __shared__ float red_x[kBcBlock / 32], red_p[kBcBlock / 32];
     const uint64_t r0 = (uint64_t)blockIdx.x * kBcBlock;
     const uint32_t nr = r0 >= n ? 0u : (n - r0 < kBcBlock ? (uint32_t)(n - r0) : kBcBlock);
@@ -1208,21 +1233,20 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
             lo = fmin(lo, pmin[part * d + t]);
             hi = fmax(hi, pmax[part * d + t]);
         }
-        const __half ch = __double2half(nr ? 0.5 * lo + 0.5 * hi : 0.0);
-        cs[t] = (double)__half2float(ch);
-        chs[t] = __half_as_ushort(ch);
+        double c;
+        chs[t] = El::round(nr ? 0.5 * lo + 0.5 * hi : 0.0, &c);
+        cs[t] = c;
     }
     __syncthreads();
     // 3. per rank: residual (rounded once), q = |h|^2 + 2 h.c, |h|, pieces of q / 2
     const uint32_t r = threadIdx.x;
     float my_x = 0.f, my_p = 0.f;
-    uint16_t m16[3] = {0, 0, 0};
+    E mb0 = 0, mb1 = 0, mb2 = 0;
     if (r < nr) {
         double hh = 0.0, hc = 0.0;
         for (uint32_t t = 0; t < d; ++t) {
-            const __half hv = __double2half(xs[r * P.xstride + t] - cs[t]);
-            const double h = (double)__half2float(hv);
-            hs[r * P.hstride + t] = __half_as_ushort(hv);
+            double h;
+            hs[r * P.hstride + t] = El::round(xs[r * P.xstride + t] - cs[t], &h);
             hh = fma(h, h, hh);
             hc = fma(h, cs[t], hc);
         }
@@ -1231,48 +1255,54 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
         my_p = fabsf((float)q) * (1.0f + 2.4e-7f);
         my_x = (float)sqrt(hh) * (1.0f + 2.4e-7f);
         if (xn) xn[r0 + r] = my_x;
+        // q / 2 in three pieces: FP16 at scales 2^15, 2^4, 2^-7 (the A side's
+        // constants); TF32 at scale 1
+        const double s1 = OP == 2 ? 0x1p15 : 1.0, s2 = OP == 2 ? 0x1p4 : 1.0, s3 = OP == 2 ? 0x1p-7 : 1.0;
+        double b1, b2, b3;
         const double v1 = 0.5 * q;
-        const __half h1 = __double2half(v1 * 0x1p-15);
-        const double v2 = v1 - (double)__half2float(h1) * 0x1p15;
-        const __half h2 = __double2half(v2 * 0x1p-4);
-        const double v3 = v2 - (double)__half2float(h2) * 0x1p4;
-        const __half h3 = __double2half(v3 * 0x1p7);
-        m16[0] = __half_as_ushort(h1);
-        m16[1] = __half_as_ushort(h2);
-        m16[2] = __half_as_ushort(h3);
+        mb0 = El::round(v1 / s1, &b1);
+        const double v2 = v1 - b1 * s1;
+        mb1 = El::round(v2 / s2, &b2);
+        const double v3 = v2 - b2 * s2;
+        mb2 = El::round(v3 / s3, &b3);
+        (void)b3;
     } else {
         norms[r0 + r] = kPadNorm;
         if (xn) xn[r0 + r] = 0.f;
     }
-    ms[4 * r] = m16[0];
-    ms[4 * r + 1] = m16[1];
-    ms[4 * r + 2] = m16[2];
+    ms[4 * r] = mb0;
+    ms[4 * r + 1] = mb1;
+    ms[4 * r + 2] = mb2;
     __syncthreads();
     // 4. the rows [h | h | c m | h a] as 16-byte chunks, consecutive threads on
-    // consecutive chunks (FP16 bits copied, no conversion)
-    const uint16_t a16[3] = {__half_as_ushort(__double2half(-0x1p15)), __half_as_ushort(__double2half(-0x1p4)),
-                             __half_as_ushort(__double2half(-0x1p-7))};
+    // consecutive chunks (operand bits copied, no conversion)
+    double unused;
+    const E ab0 = El::round(OP == 2 ? -0x1p15 : -1.0, &unused), ab1 = El::round(OP == 2 ? -0x1p4 : -1.0, &unused),
+            ab2 = El::round(OP == 2 ? -0x1p-7 : -1.0, &unused);
     // chunk e = (row rr, chunk q of the row), q = (block b, chunk within it);
     // the indices advance by kBcBlock chunks per step without divisions
-    const uint32_t cpb = dp / 8, cpr = 4 * cpb;  // 16-byte chunks per block, per row (4 dp halves)
+    const uint32_t cpb = dp / kEpc, cpr = 4 * cpb;  // 16-byte chunks per block, per row (4 dp elements)
     const uint32_t step_r = kBcBlock / cpr, step_q = kBcBlock - step_r * cpr;
     uint32_t rr = threadIdx.x / cpr, q = threadIdx.x - rr * cpr;
     for (uint32_t e = threadIdx.x; e < kBcBlock * cpr; e += kBcBlock) {
-        const uint32_t b = (q >= cpb) + (q >= 2 * cpb) + (q >= 3 * cpb), t0 = 8 * (q - b * cpb);
+        const uint32_t b = (q >= cpb) + (q >= 2 * cpb) + (q >= 3 * cpb), t0 = kEpc * (q - b * cpb);
         uint32_t w[4] = {0u, 0u, 0u, 0u};
         if (rr < nr) {
 #pragma unroll
-            for (int z = 0; z < 8; ++z) {
+            for (uint32_t z = 0; z < kEpc; ++z) {
                 const uint32_t t = t0 + z;
                 uint32_t bits = 0;
                 if (t < d)
                     bits = b == 2 ? chs[t] : hs[rr * P.hstride + t];
                 else if (t < d + 3)
-                    bits = b == 2 ? ms[4 * rr + (t - d)] : (b == 3 ? a16[t - d] : 0u);
-                w[z >> 1] |= bits << (16 * (z & 1));
+                    bits = b == 2 ? ms[4 * rr + (t - d)] : (b == 3 ? (t == d ? ab0 : (t == d + 1 ? ab1 : ab2)) : 0u);
+                if (sizeof(E) == 2)
+                    w[z >> 1] |= bits << (16 * (z & 1));
+                else
+                    w[z] = bits;
             }
         }
-        reinterpret_cast<uint4 *>(op)[(r0 + rr) * cpr + q] = make_uint4(w[0], w[1], w[2], w[3]);
+        reinterpret_cast<uint4 *>(op_out)[(r0 + rr) * cpr + q] = make_uint4(w[0], w[1], w[2], w[3]);
         rr += step_r;
         q += step_q;
         if (q >= cpr) q -= cpr, ++rr;
@@ -1302,23 +1332,27 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
     }
 }
 
-void launch_bc_prepare(const SortedSet &s, const double *center, double scale, uint16_t *op, float *norms,
-                       float *xn, float4 *blk, float *cent, cudaStream_t st, int *launches) {
+void launch_bc_prepare(const SortedSet &s, const double *center, double scale, void *op, float *norms, float *xn,
+                       float4 *blk, float *cent, cudaStream_t st, int *launches) {
     if (s.npad_tc == 0) return;
     const unsigned blocks = (unsigned)(s.npad_tc / kBcBlock);
-    const size_t smem = bc_smem_plan(s.d).bytes;
+    const uint32_t eb = bc_elem_bytes(s.bc_form);
+    const size_t smem = bc_smem_plan(s.d, eb).bytes;
     // the block's rows start at r0 d coordinates: 16-byte loads when that and the base allow
     const bool vec = ((uintptr_t)s.rows & 15u) == 0 && ((uint64_t)kBcBlock * s.d * s.dtype_bytes) % 16 == 0;
-    const int smem_max = (int)bc_smem_plan(kBcMaxDim).bytes;
-    if (s.dtype_bytes == 8) {
-        ensure_max_dynamic_smem((const void *)k_bc_prepare<double>, smem_max);
-        k_bc_prepare<double><<<blocks, kBcBlock, smem, st>>>(static_cast<const double *>(s.rows), s.n, s.d, center,
-                                                             scale, s.bc_dp, vec, op, norms, xn, blk, cent);
+    const int smem_max = (int)bc_smem_plan(kBcMaxDim, 4).bytes;
+#define HJ_BC_PREP(T, OPV)                                                                                        \
+    do {                                                                                                          \
+        ensure_max_dynamic_smem((const void *)k_bc_prepare<T, OPV>, smem_max);                                    \
+        k_bc_prepare<T, OPV><<<blocks, kBcBlock, smem, st>>>(static_cast<const T *>(s.rows), s.n, s.d, center,    \
+                                                             scale, s.bc_dp, vec, op, norms, xn, blk, cent);      \
+    } while (0)
+    if (s.bc_form == HJ_FORM_TC_TF32) {
+        if (s.dtype_bytes == 8) HJ_BC_PREP(double, 0); else HJ_BC_PREP(float, 0);
     } else {
-        ensure_max_dynamic_smem((const void *)k_bc_prepare<float>, smem_max);
-        k_bc_prepare<float><<<blocks, kBcBlock, smem, st>>>(static_cast<const float *>(s.rows), s.n, s.d, center,
-                                                            scale, s.bc_dp, vec, op, norms, xn, blk, cent);
+        if (s.dtype_bytes == 8) HJ_BC_PREP(double, 2); else HJ_BC_PREP(float, 2);
     }
+#undef HJ_BC_PREP
     if (launches) *launches += 1;
 }
 

@@ -45,24 +45,26 @@ def eps_for(x, nbrs, seed=0):
     return W.calibrate_eps(x, x.shape[0], nbrs, sample=min(4000, x.shape[0]))
 
 
+@pytest.mark.parametrize("form", ["fp16", "tf32"])
 @pytest.mark.parametrize("n,d", [(20000, 28), (9000, 64), (12000, 8), (5003, 3), (3001, 1), (1000 + 37, 16)])
-def test_self_counts_block_forced(hj, n, d):
+def test_self_counts_block_forced(hj, n, d, form):
     x = tight_clusters(n, d, 100 + d)
     eps = eps_for(x, 40)
     want = oracle.self_count_brute(x.astype(np.float64), eps)
-    got, st = hj.self_join_count(x, eps, form="fp16", centring="block", return_stats=True)
-    assert got == want, (n, d, got, want)
+    got, st = hj.self_join_count(x, eps, form=form, centring="block", return_stats=True)
+    assert got == want, (n, d, form, got, want)
     assert st["tc_centring"] == "block"
-    assert st["form_used"] == "tc_fp16"
+    assert st["form_used"] == "tc_" + form
 
 
+@pytest.mark.parametrize("form", ["fp16", "tf32"])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
-def test_join_counts_block_forced(hj, dtype):
+def test_join_counts_block_forced(hj, dtype, form):
     a = tight_clusters(7001, 20, 5, dtype=dtype)
     b = tight_clusters(9100, 20, 5, dtype=dtype)[::-1].copy()
     eps = eps_for(a, 30)
     want = oracle.join_count_brute(a.astype(np.float64), b.astype(np.float64), eps)
-    got, st = hj.join_count(a, b, eps, form="fp16", centring="block", return_stats=True)
+    got, st = hj.join_count(a, b, eps, form=form, centring="block", return_stats=True)
     assert got == want
     assert st["tc_centring"] == "block"
 
@@ -77,7 +79,8 @@ def test_uniform_and_dense_block_forced(hj):
         assert hj.self_join_count(x, eps, form="fp16", centring="block") == want, eps
 
 
-def test_lattice_ties_at_eps(hj):
+@pytest.mark.parametrize("form", ["fp16", "tf32"])
+def test_lattice_ties_at_eps(hj, form):
     """Points on a 0.125 lattice (exact in binary): many pairs lie exactly at
     eps, where only the FP64 test decides; every such pair must reach the band
     (or be certain) and the count must be the FP64 count."""
@@ -85,23 +88,24 @@ def test_lattice_ties_at_eps(hj):
     x = (rng.integers(0, 9, (6000, 6)) * 0.125 + 3.0).astype(np.float64)
     for eps in (0.125, 0.25, np.sqrt(2) * 0.125, 0.375):
         want = oracle.self_count_brute(x, eps)
-        assert hj.self_join_count(x, eps, form="fp16", centring="block") == want, eps
-        assert hj.self_join_count(x.astype(np.float32), eps, form="fp16", centring="block") == \
+        assert hj.self_join_count(x, eps, form=form, centring="block") == want, eps
+        assert hj.self_join_count(x.astype(np.float32), eps, form=form, centring="block") == \
             oracle.self_count_brute(x.astype(np.float32).astype(np.float64), eps), eps
 
 
-def test_scaling_and_offsets(hj):
+@pytest.mark.parametrize("form", ["fp16", "tf32"])
+def test_scaling_and_offsets(hj, form):
     """Offsets far from zero and a dim whose range dwarfs the others (FP16
     subnormal residuals)."""
     rng = np.random.default_rng(9)
     y = tight_clusters(6000, 16, 9, dtype=np.float64) + 1e9
     eps = eps_for(y - 1e9, 40)
-    assert hj.self_join_count(y, eps, form="fp16", centring="block") == oracle.self_count_brute(y, eps)
+    assert hj.self_join_count(y, eps, form=form, centring="block") == oracle.self_count_brute(y, eps)
     z = rng.random((5000, 10))
     z[:, 0] *= 1e6
     z[:, 1:] *= 1e-3
     for eps in (3e3, 4e4):
-        assert hj.self_join_count(z, eps, form="fp16", centring="block") == oracle.self_count_brute(z, eps)
+        assert hj.self_join_count(z, eps, form=form, centring="block") == oracle.self_count_brute(z, eps)
 
 
 def test_auto_picks_block_for_clustered_small_eps(hj):
@@ -147,7 +151,7 @@ def test_unsupported_combinations(hj):
         hj.self_join_count(x, 0.05, form="fp16", centring="block")
     y = tight_clusters(2000, 8, 1)
     with pytest.raises(hj.HJError):
-        hj.self_join_count(y, 0.05, form="tf32", centring="block")
+        hj.self_join_count(y, 0.05, form="bf16x3", centring="block")
     with pytest.raises(hj.HJError):
         hj.self_join_count(y, 0.05, form="fp16", centring=7)
     # the plain form ignores the option
@@ -155,7 +159,8 @@ def test_unsupported_combinations(hj):
         oracle.self_count_brute(y.astype(np.float64), 0.05)
 
 
-def test_estimates_all_pairs_loose_bound(hj):
+@pytest.mark.parametrize("form", ["fp16", "tf32"])
+def test_estimates_all_pairs_loose_bound(hj, form):
     """Every pair estimated (one cell): the error stays within the bound of
     the residual model with the loosest residual, the diameter of the data's
     bounding box, and the estimates are real tensor-core results."""
@@ -163,14 +168,15 @@ def test_estimates_all_pairs_loose_bound(hj):
     for d in (5, 28, 64):
         a = (rng.standard_normal((600, d)) * 2.0 + 5.0).astype(np.float32)
         b = (rng.standard_normal((800, d)) * 2.0 + 5.0).astype(np.float32)
-        est = hj.tc_estimates(a, b, "fp16", centring="block").astype(np.float64)
+        est = hj.tc_estimates(a, b, form, centring="block").astype(np.float64)
         ex = exact_dist2(a, b)
         both = np.concatenate([a, b]).astype(np.float64)
         half = 0.5 * (both.max(0) - both.min(0))
         R = float(np.sqrt((half ** 2).sum()))  # |c| <= R (centres inside the box)
         H = 2.0 * R                             # |h| <= diameter of the box
-        dp = -(-(d + 3) // 8) * 8                 # block width of the operand rows
-        kpad = -(-(3 * dp) // 16) * 16            # product terms the MMAs sum
+        g, kstep = (8, 16) if form == "fp16" else (4, 8)
+        dp = -(-(d + 3) // g) * g                 # block width of the operand rows
+        kpad = -(-(3 * dp) // kstep) * kstep      # product terms the MMAs sum
         S = 1.5 * (H * H + 2 * H * R)           # cross terms and the folded q / 2
         rho = 2 * 2.0 ** -11 * H
         bound = 2 * kpad * 2.0 ** -22 * S + 2 * rho * np.sqrt(ex) + rho * rho + 1e-5 * (1 + ex)
