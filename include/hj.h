@@ -88,11 +88,11 @@ typedef enum {
     HJ_CENTRING_AUTO = 0,
     /* One centre for the whole join (the per-dim midpoint of the data). */
     HJ_CENTRING_GLOBAL = 1,
-    /* A centre per 128-point block of the EGO order, exact in FP16, and each
-     * point stored as that centre plus its FP16 residual; the operand rows
-     * carry the residual and centre cross terms as extra K columns (3d of
-     * them), so the error band scales with the residual norms. FP16 and
-     * TF32 forms, d <= 64. */
+    /* A centre per 128-point block of the EGO order, exact in the operand
+     * type, and each point stored as that centre plus its residual rounded
+     * once; the operand rows carry the residual and centre cross terms and
+     * the point's norm as extra K columns (about 3d of them), so the error
+     * band scales with the residual norms. FP16 and TF32 forms, d <= 64. */
     HJ_CENTRING_BLOCK = 2
 } hj_centring;
 
