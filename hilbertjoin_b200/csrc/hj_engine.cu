@@ -140,7 +140,7 @@ enum {
     kSlotTmaxAA, kSlotTmaxAB, kSlotTmaxBA, kSlotTmaxBB, kSlotBand, kSlotCenter, kSlotGminA, kSlotGminB,
     kSlotItemCnt, kSlotPairKeys, kSlotPairPerm, kSlotPairTmp, kSlotPairHist, kSlotPairOut, kSlotDimCost,
     kSlotGridOrd, kSlotBcOpA, kSlotBcOpB, kSlotBcNormA, kSlotBcNormB, kSlotBcXnA, kSlotBcXnB, kSlotBcBlkA,
-    kSlotBcBlkB, kSlotBcCentA, kSlotBcCentB, kSlotScanTiles,
+    kSlotBcBlkB, kSlotBcCentA, kSlotBcCentB, kSlotScanTiles, kSlotBcOpLoA, kSlotBcOpLoB,
     kSlotEngineEnd
 };
 static_assert(kSlotEngineEnd <= kSlotIndexFirst, "engine slots overlap the index stage's");
@@ -329,13 +329,18 @@ static int prepare_block_centring(Ctx *c, cudaStream_t st, SortedSet *s, bool is
     s->bc_form = form;
     s->bc_dp = bc_dp(s->d, form);
     s->bc_op = slot_alloc_impl(c, st, is_b ? kSlotBcOpB : kSlotBcOpA, npad * 4 * s->bc_dp * bc_elem_bytes(form));
+    s->bc_op_lo = form == HJ_FORM_TC_BF16X3
+                      ? slot_alloc_impl(c, st, is_b ? kSlotBcOpLoB : kSlotBcOpLoA, npad * 4 * s->bc_dp * 2)
+                      : nullptr;
     s->bc_norms = (float *)slot_alloc_impl(c, st, is_b ? kSlotBcNormB : kSlotBcNormA, npad * 4);
     s->bc_xn = (float *)slot_alloc_impl(c, st, is_b ? kSlotBcXnB : kSlotBcXnA, npad * 4);
     s->bc_blk = (float4 *)slot_alloc_impl(c, st, is_b ? kSlotBcBlkB : kSlotBcBlkA, nblk * sizeof(float4));
     s->bc_cent = (float *)slot_alloc_impl(c, st, is_b ? kSlotBcCentB : kSlotBcCentA, nblk * kBcCentStride * 4);
-    if (!s->bc_op || !s->bc_norms || !s->bc_xn || !s->bc_blk || !s->bc_cent)
+    if (!s->bc_op || (form == HJ_FORM_TC_BF16X3 && !s->bc_op_lo) || !s->bc_norms || !s->bc_xn || !s->bc_blk ||
+        !s->bc_cent)
         return fail(HJ_ERR_OOM, "out of device memory (block-centred operands)");
-    launch_bc_prepare(*s, center, scale, s->bc_op, s->bc_norms, s->bc_xn, s->bc_blk, s->bc_cent, st, launches);
+    launch_bc_prepare(*s, center, scale, s->bc_op, s->bc_op_lo, s->bc_norms, s->bc_xn, s->bc_blk, s->bc_cent, st,
+                      launches);
     return check_cuda("block-centred operands");
 }
 
@@ -575,13 +580,14 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
         // (FP16 form, d <= 64) when asked for, or when the global centre would
         // send more than an eighth of the block pairs to the FP64 kernel.
         const int centring = opts ? opts->tc_centring : HJ_CENTRING_AUTO;
-        const bool bc_ok = (form == HJ_FORM_TC_FP16 || form == HJ_FORM_TC_TF32) && d <= kBcMaxDim;
+        const bool bc_ok = d <= kBcMaxDim;  // every tensor-core form
         // block-centred operands of both forms: the largest coordinate below 2^10
         const double bc_scale = std::ldexp(P.op_scale, -kBcScaleShift);
         auto enable_bc = [&]() -> int {
             if (int r = prepare_block_centring(c, st, &A, false, A.center, bc_scale, form, &launches)) return r;
             if (in.self) {
-                B.bc_op = A.bc_op, B.bc_dp = A.bc_dp, B.bc_form = A.bc_form, B.bc_norms = A.bc_norms;
+                B.bc_op = A.bc_op, B.bc_op_lo = A.bc_op_lo, B.bc_dp = A.bc_dp, B.bc_form = A.bc_form;
+                B.bc_norms = A.bc_norms;
                 B.bc_xn = A.bc_xn, B.bc_blk = A.bc_blk, B.bc_cent = A.bc_cent;
             } else if (int r = prepare_block_centring(c, st, &B, true, B.center, bc_scale, form, &launches)) {
                 return r;
@@ -602,7 +608,7 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
             cudaMemcpyAsync(c->d_job, c->h_job, sizeof(TcJob), cudaMemcpyHostToDevice, st);
         };
         if (centring == HJ_CENTRING_BLOCK) {
-            if (!bc_ok) return fail(HJ_ERR_UNSUPPORTED, "per-block centring needs the FP16 or TF32 form and d <= 64");
+            if (!bc_ok) return fail(HJ_ERR_UNSUPPORTED, "per-block centring needs d <= 64");
             if (int r = enable_bc()) return r;
         }
         // the FP16 form works in scaled units: norms, eps^2 and the bound times op_scale^2
@@ -668,8 +674,10 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
             }
             const uint64_t cand_tc = idx_tc.tile_pairs * (uint64_t)kTcTileA * kTcTileB;
             // first band queue: 1/4096 of the candidates (1/512 with block
-            // centres, whose wider tiles stay on the tensor cores)
-            uint64_t cap = std::max<uint64_t>(1ull << 20, cand_tc / (bc ? 512 : 4096));
+            // centres, whose wider tiles stay on the tensor cores; 1/256 for
+            // BF16x3, whose bound adds three products per K step)
+            const uint64_t div = !bc ? 4096 : (form == HJ_FORM_TC_BF16X3 ? 256 : 512);
+            uint64_t cap = std::max<uint64_t>(1ull << 20, cand_tc / div);
             const uint64_t cap_limit = std::max<uint64_t>(1ull << 27, cand_tc / 64);
             bool done = false, fallback = false;
             for (int grow = 0; grow < 4; ++grow) {
@@ -1066,7 +1074,7 @@ uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dt
                                     bool block_centring) {
     const uint64_t W = (6ull * d + 31) / 32 + 1;
     const bool tc = form_is_tc(form) || form == HJ_FORM_AUTO;
-    const bool bc = block_centring && form != HJ_FORM_PLAIN_FP64 && form != HJ_FORM_TC_BF16X3 && d <= kBcMaxDim;
+    const bool bc = block_centring && form != HJ_FORM_PLAIN_FP64 && d <= kBcMaxDim;
     auto per_set = [&](uint64_t n) -> uint64_t {
         const uint64_t npad = hj_ceil_div(std::max<uint64_t>(n, 1), kTcTileB) * kTcTileB;
         uint64_t b = n * d * (uint64_t)dtype_bytes;          // sorted rows
@@ -1075,6 +1083,7 @@ uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dt
         if (tc) b += npad * (hj_ceil_div(d, 64) * 64) * 4 + npad * 8;  // operands (widest form), norms
         if (bc)  // block-centred operand rows, q, |h|, blocks
             b += npad * 4 * bc_dp(d, HJ_FORM_TC_TF32) * 4 + npad * 8 + (npad / kBcBlock) * (16 + kBcCentStride * 4);
+        // (TF32 rows, 4 bytes a column, bound the BF16 hi + lo pair too)
         return b;
     };
     uint64_t b = per_set(na) + (self ? 0 : per_set(nb));
@@ -1086,7 +1095,8 @@ uint64_t engine_join_bytes_estimate(uint64_t na, uint64_t nb, uint32_t d, int dt
     b += tiles * (uint64_t)kMaxCombos * 8 + tiles * 64 * 16 + na * W * 8;
     if (tc) {
         const double cand = (double)na * (double)nb;
-        b += (uint64_t)std::max(1048576.0, cand / (bc ? 512.0 : 4096.0)) * kBandEntryBytes;
+        b += (uint64_t)std::max(1048576.0, cand / (bc ? (form == HJ_FORM_TC_BF16X3 ? 256.0 : 512.0) : 4096.0)) *
+             kBandEntryBytes;
     }
     return b + (16ull << 20);
 }

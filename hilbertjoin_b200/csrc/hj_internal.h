@@ -110,6 +110,7 @@ struct SortedSet {
     // the B operand is the window at column 0, the A operand the window at column
     // bc_dp, both 3 bc_dp wide
     void *bc_op = nullptr;
+    void *bc_op_lo = nullptr;  // BF16x3: the low BF16 halves of the same rows
     uint32_t bc_dp = 0;
     int bc_form = 0;
     float *bc_norms = nullptr;    // q = |h|^2 + 2 h.c per rank (FP32; padding rows kPadNorm)
@@ -118,7 +119,7 @@ struct SortedSet {
     float *bc_cent = nullptr;     // per block: c in FP32 (FP16 values), kBcCentStride floats, zero padded
 };
 
-// Per-block centring of the FP16 (or TF32) operands. Every 128-rank block of
+// Per-block centring of the FP16 (or TF32, or BF16 hi + lo) operands. Every 128-rank block of
 // a sorted set (one A tile, half a B tile) gets a centre c whose coordinates
 // are FP16 (or TF32) values in the operand units ((x - center) * scale, the
 // largest coordinate below 2^10), the midpoint of the block's range rounded;
@@ -186,8 +187,8 @@ BcConsts bc_constants(int form, uint32_t d, double T, double op_scale);
 // Block centres, the operand rows ([npad][4 dp]), q, |h| and block summaries
 // of a sorted set from its sorted rows. center = the global per-dim shift,
 // scale = the block-centred operand scale.
-void launch_bc_prepare(const SortedSet &s, const double *center, double scale, void *op, float *norms, float *xn,
-                       float4 *blk, float *cent, cudaStream_t st, int *launches);
+void launch_bc_prepare(const SortedSet &s, const double *center, double scale, void *op, void *op_lo, float *norms,
+                       float *xn, float4 *blk, float *cent, cudaStream_t st, int *launches);
 
 constexpr float kPadNorm = 1.0e30f;
 

@@ -974,20 +974,23 @@ uint32_t tc_kterms(int form, uint32_t kcols) { return tc_ksteps(form, kcols) * (
 //   theta_t: the FP64 pair test sums d squares of exact differences with FMAs,
 //     relative error below (d + 2) 2^-53 of dist2 ~ eps^2: 2 (d + 2) 2^-53 T.
 BcConsts bc_constants(int form, uint32_t d, double T, double op_scale) {
-    const double s2 = op_scale * op_scale, kpad = (double)tc_kterms(form, bc_cols(d, form));
+    // BF16x3: three MMAs per K step; the dropped lo.lo products are below 2^-18 S
+    const double s2 = op_scale * op_scale,
+                 kpad = (double)tc_kterms(form, bc_cols(d, form)) * (form == HJ_FORM_TC_BF16X3 ? 3.0 : 1.0);
     auto up = [](double v) {
         const float f = (float)v;
         return (double)f >= v ? f : std::nextafter(f, INFINITY);
     };
     BcConsts k;
-    k.kp21 = up(2.0 * kpad * std::ldexp(1.0, -22));
+    k.kp21 = up(2.0 * kpad * std::ldexp(1.0, -22) + (form == HJ_FORM_TC_BF16X3 ? 2.0 * std::ldexp(1.0, -18) : 0.0));
     k.eps = up(std::sqrt(T * s2) * (1.0 + 1e-12));
-    k.rho_u = up(1.001 * std::ldexp(1.0, -11));
+    // FP16 / TF32 round once to 11 significant bits; the BF16 hi + lo pair keeps v to 2^-18
+    k.rho_u = up(1.001 * std::ldexp(1.0, form == HJ_FORM_TC_BF16X3 ? -18 : -11));
     // the subnormal spacing of the operand type (half of it per rounding: FP16
     // 2^-25, TF32 2^-150) and the FP64 shift of coordinates below 2^10 (2^-52 of
     // 2^10, generously 2^-37)
     const double floor_abs =
-        (form == HJ_FORM_TC_FP16 ? std::ldexp(1.0, -25) : std::ldexp(1.0, -149)) + std::ldexp(1.0, -37);
+        (form == HJ_FORM_TC_FP16 ? std::ldexp(1.0, -25) : std::ldexp(1.0, -140)) + std::ldexp(1.0, -37);
     k.rho_c = up(2.0 * std::sqrt((double)d) * floor_abs);
     k.u_norm = up(std::ldexp(1.0, -23) + std::ldexp(1.0, -33));
     k.u_d = up(16.0 * std::ldexp(1.0, -24));
@@ -1035,9 +1038,9 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
                    uint32_t *d_err, int num_sms, cudaStream_t st, std::string *err, const BcConsts *bc,
                    unsigned long long *d_band_holes) {
     if (idx.n_items == 0) return 0;
-    if (bc && ((form != HJ_FORM_TC_FP16 && form != HJ_FORM_TC_TF32) || A.d > kBcMaxDim || !A.bc_op || !B.bc_op ||
-               A.bc_dp != B.bc_dp || A.bc_form != form || B.bc_form != form)) {
-        *err = "per-block centring needs the FP16 or TF32 form, d <= 64 and the centred layouts";
+    if (bc && (A.d > kBcMaxDim || !A.bc_op || !B.bc_op || A.bc_dp != B.bc_dp || A.bc_form != form ||
+               B.bc_form != form || (form == HJ_FORM_TC_BF16X3 && (!A.bc_op_lo || !B.bc_op_lo)))) {
+        *err = "per-block centring needs d <= 64 and the centred layouts of the form";
         return 1;
     }
     const TcLayout L = tc_layout(form, bc ? bc_cols(A.d, form) : A.d);
@@ -1049,12 +1052,17 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
     if (bc) {
         // rows of 4 dp columns; A reads the window from column dp (the producer's
         // x offset), B from column 0; past the row end the copy fills zeros
-        const CUtensorMapDataType ty =
-            form == HJ_FORM_TC_TF32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+        const CUtensorMapDataType ty = form == HJ_FORM_TC_TF32    ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                       : form == HJ_FORM_TC_BF16X3 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                                   : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
         if (!make_map(&ma, A.bc_op, ty, A.npad_tc, 4 * A.bc_dp, kTcTileA, err)) return 1;
         if (!make_map(&mb, B.bc_op, ty, B.npad_tc, 4 * B.bc_dp, kTcTileB, err)) return 1;
         ma2 = ma;
         mb2 = mb;
+        if (form == HJ_FORM_TC_BF16X3) {
+            if (!make_map(&ma2, A.bc_op_lo, ty, A.npad_tc, 4 * A.bc_dp, kTcTileA, err)) return 1;
+            if (!make_map(&mb2, B.bc_op_lo, ty, B.npad_tc, 4 * B.bc_dp, kTcTileB, err)) return 1;
+        }
     } else if (form == HJ_FORM_TC_TF32) {
         if (!make_map(&ma, A.tf32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, A.npad_tc, A.kpad_tf32, kTcTileA, err)) return 1;
         if (!make_map(&mb, B.tf32, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, B.npad_tc, B.kpad_tf32, kTcTileB, err)) return 1;
@@ -1113,6 +1121,9 @@ int launch_join_tc(const SortedSet &A, const SortedSet &B, int form, const TcJob
     if (bc && form == HJ_FORM_TC_TF32) {
         ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_TF32, true>, 225 * 1024);
         k_join_tc<HJ_FORM_TC_TF32, true><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
+    } else if (bc && form == HJ_FORM_TC_BF16X3) {
+        ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_BF16X3, true>, 225 * 1024);
+        k_join_tc<HJ_FORM_TC_BF16X3, true><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);
     } else if (bc) {
         ensure_max_dynamic_smem((const void *)k_join_tc<HJ_FORM_TC_FP16, true>, 225 * 1024);
         k_join_tc<HJ_FORM_TC_FP16, true><<<(unsigned)grid, kTcThreads, L.smem, st>>>(ma, ma2, mb, mb2, a);

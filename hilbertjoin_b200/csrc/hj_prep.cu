@@ -1137,6 +1137,16 @@ template <> struct BcElem<0> {  // TF32
         return __float_as_uint(f);
     }
 };
+template <> struct BcElem<1> {  // BF16 hi + lo (BF16x3): hi in the low 16 bits, lo in the high 16 bits;
+    using E = uint32_t;         // the stored value hi + lo is within 2^-18 of v
+    __device__ static E round(double v, double *back) {
+        const __nv_bfloat16 hi = __double2bfloat16(v);
+        const double h = (double)__bfloat162float(hi);
+        const __nv_bfloat16 lo = __double2bfloat16(v - h);  // v - h exact in FP64
+        *back = h + (double)__bfloat162float(lo);
+        return (uint32_t)__bfloat16_as_ushort(hi) | ((uint32_t)__bfloat16_as_ushort(lo) << 16);
+    }
+};
 
 // Shared memory of k_bc_prepare for dimension d and element size eb: the rows
 // in FP64 with an odd row stride (fewer bank conflicts when a thread walks its
@@ -1167,11 +1177,13 @@ template <typename T, int OP>
 __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ rows, uint64_t n, uint32_t d,
                                                          const double *__restrict__ center, double scale,
                                                          uint32_t dp, bool vec, void *__restrict__ op_out,
-                                                         float *__restrict__ norms, float *__restrict__ xn,
-                                                         float4 *__restrict__ blk, float *__restrict__ cent) {
+                                                         void *__restrict__ op_lo, float *__restrict__ norms,
+                                                         float *__restrict__ xn, float4 *__restrict__ blk,
+                                                         float *__restrict__ cent) {
     using El = BcElem<OP>;
     using E = typename El::E;
-    constexpr uint32_t kEpc = 16 / sizeof(E);  // elements per 16-byte chunk
+    constexpr bool kSplit = OP == 1;                          // BF16 hi / lo into two row buffers
+    constexpr uint32_t kEpc = kSplit ? 8u : 16 / sizeof(E);  // elements per 16-byte chunk (of each buffer)
     extern __shared__ __align__(16) unsigned char bc_raw[];
     const BcSmem P = bc_smem_plan(d, sizeof(E));
     double *xs = reinterpret_cast<double *>(bc_raw + P.o_x);    // [kBcBlock][xstride]
@@ -1256,7 +1268,7 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
         my_x = (float)sqrt(hh) * (1.0f + 2.4e-7f);
         if (xn) xn[r0 + r] = my_x;
         // q / 2 in three pieces: FP16 at scales 2^15, 2^4, 2^-7 (the A side's
-        // constants); TF32 at scale 1
+        // constants); TF32 and BF16 hi + lo at scale 1
         const double s1 = OP == 2 ? 0x1p15 : 1.0, s2 = OP == 2 ? 0x1p4 : 1.0, s3 = OP == 2 ? 0x1p-7 : 1.0;
         double b1, b2, b3;
         const double v1 = 0.5 * q;
@@ -1286,7 +1298,7 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
     uint32_t rr = threadIdx.x / cpr, q = threadIdx.x - rr * cpr;
     for (uint32_t e = threadIdx.x; e < kBcBlock * cpr; e += kBcBlock) {
         const uint32_t b = (q >= cpb) + (q >= 2 * cpb) + (q >= 3 * cpb), t0 = kEpc * (q - b * cpb);
-        uint32_t w[4] = {0u, 0u, 0u, 0u};
+        uint32_t w[4] = {0u, 0u, 0u, 0u}, wl[4] = {0u, 0u, 0u, 0u};
         if (rr < nr) {
 #pragma unroll
             for (uint32_t z = 0; z < kEpc; ++z) {
@@ -1296,13 +1308,18 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
                     bits = b == 2 ? chs[t] : hs[rr * P.hstride + t];
                 else if (t < d + 3)
                     bits = b == 2 ? ms[4 * rr + (t - d)] : (b == 3 ? (t == d ? ab0 : (t == d + 1 ? ab1 : ab2)) : 0u);
-                if (sizeof(E) == 2)
+                if (kSplit) {
+                    w[z >> 1] |= (bits & 0xffffu) << (16 * (z & 1));
+                    wl[z >> 1] |= (bits >> 16) << (16 * (z & 1));
+                } else if (sizeof(E) == 2) {
                     w[z >> 1] |= bits << (16 * (z & 1));
-                else
+                } else {
                     w[z] = bits;
+                }
             }
         }
         reinterpret_cast<uint4 *>(op_out)[(r0 + rr) * cpr + q] = make_uint4(w[0], w[1], w[2], w[3]);
+        if (kSplit) reinterpret_cast<uint4 *>(op_lo)[(r0 + rr) * cpr + q] = make_uint4(wl[0], wl[1], wl[2], wl[3]);
         rr += step_r;
         q += step_q;
         if (q >= cpr) q -= cpr, ++rr;
@@ -1332,11 +1349,11 @@ __global__ void __launch_bounds__(kBcBlock) k_bc_prepare(const T *__restrict__ r
     }
 }
 
-void launch_bc_prepare(const SortedSet &s, const double *center, double scale, void *op, float *norms, float *xn,
-                       float4 *blk, float *cent, cudaStream_t st, int *launches) {
+void launch_bc_prepare(const SortedSet &s, const double *center, double scale, void *op, void *op_lo, float *norms,
+                       float *xn, float4 *blk, float *cent, cudaStream_t st, int *launches) {
     if (s.npad_tc == 0) return;
     const unsigned blocks = (unsigned)(s.npad_tc / kBcBlock);
-    const uint32_t eb = bc_elem_bytes(s.bc_form);
+    const uint32_t eb = s.bc_form == HJ_FORM_TC_FP16 ? 2u : 4u;  // shared-memory element (BF16: hi and lo)
     const size_t smem = bc_smem_plan(s.d, eb).bytes;
     // the block's rows start at r0 d coordinates: 16-byte loads when that and the base allow
     const bool vec = ((uintptr_t)s.rows & 15u) == 0 && ((uint64_t)kBcBlock * s.d * s.dtype_bytes) % 16 == 0;
@@ -1345,10 +1362,13 @@ void launch_bc_prepare(const SortedSet &s, const double *center, double scale, v
     do {                                                                                                          \
         ensure_max_dynamic_smem((const void *)k_bc_prepare<T, OPV>, smem_max);                                    \
         k_bc_prepare<T, OPV><<<blocks, kBcBlock, smem, st>>>(static_cast<const T *>(s.rows), s.n, s.d, center,    \
-                                                             scale, s.bc_dp, vec, op, norms, xn, blk, cent);      \
+                                                             scale, s.bc_dp, vec, op, op_lo, norms, xn, blk,      \
+                                                             cent);                                               \
     } while (0)
     if (s.bc_form == HJ_FORM_TC_TF32) {
         if (s.dtype_bytes == 8) HJ_BC_PREP(double, 0); else HJ_BC_PREP(float, 0);
+    } else if (s.bc_form == HJ_FORM_TC_BF16X3) {
+        if (s.dtype_bytes == 8) HJ_BC_PREP(double, 1); else HJ_BC_PREP(float, 1);
     } else {
         if (s.dtype_bytes == 8) HJ_BC_PREP(double, 2); else HJ_BC_PREP(float, 2);
     }

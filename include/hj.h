@@ -83,8 +83,8 @@ typedef enum {
 typedef enum {
     /* HJ_CENTRING_BLOCK when, with one global centre, more than an eighth of
      * the block pairs would run on the FP64 kernel (the norm expansion's
-     * cancellation limit: eps small against the spread of the data), the
-     * form is FP16 or TF32 and d <= 64; HJ_CENTRING_GLOBAL otherwise. */
+     * cancellation limit: eps small against the spread of the data) and
+     * d <= 64; HJ_CENTRING_GLOBAL otherwise. */
     HJ_CENTRING_AUTO = 0,
     /* One centre for the whole join (the per-dim midpoint of the data). */
     HJ_CENTRING_GLOBAL = 1,
@@ -92,7 +92,7 @@ typedef enum {
      * type, and each point stored as that centre plus its residual rounded
      * once; the operand rows carry the residual and centre cross terms and
      * the point's norm as extra K columns (about 3d of them), so the error
-     * band scales with the residual norms. FP16 and TF32 forms, d <= 64. */
+     * band scales with the residual norms. Every tensor-core form, d <= 64. */
     HJ_CENTRING_BLOCK = 2
 } hj_centring;
 

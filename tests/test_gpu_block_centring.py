@@ -45,7 +45,7 @@ def eps_for(x, nbrs, seed=0):
     return W.calibrate_eps(x, x.shape[0], nbrs, sample=min(4000, x.shape[0]))
 
 
-@pytest.mark.parametrize("form", ["fp16", "tf32"])
+@pytest.mark.parametrize("form", ["fp16", "tf32", "bf16x3"])
 @pytest.mark.parametrize("n,d", [(20000, 28), (9000, 64), (12000, 8), (5003, 3), (3001, 1), (1000 + 37, 16)])
 def test_self_counts_block_forced(hj, n, d, form):
     x = tight_clusters(n, d, 100 + d)
@@ -57,7 +57,7 @@ def test_self_counts_block_forced(hj, n, d, form):
     assert st["form_used"] == "tc_" + form
 
 
-@pytest.mark.parametrize("form", ["fp16", "tf32"])
+@pytest.mark.parametrize("form", ["fp16", "tf32", "bf16x3"])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_join_counts_block_forced(hj, dtype, form):
     a = tight_clusters(7001, 20, 5, dtype=dtype)
@@ -79,7 +79,7 @@ def test_uniform_and_dense_block_forced(hj):
         assert hj.self_join_count(x, eps, form="fp16", centring="block") == want, eps
 
 
-@pytest.mark.parametrize("form", ["fp16", "tf32"])
+@pytest.mark.parametrize("form", ["fp16", "tf32", "bf16x3"])
 def test_lattice_ties_at_eps(hj, form):
     """Points on a 0.125 lattice (exact in binary): many pairs lie exactly at
     eps, where only the FP64 test decides; every such pair must reach the band
@@ -93,7 +93,7 @@ def test_lattice_ties_at_eps(hj, form):
             oracle.self_count_brute(x.astype(np.float32).astype(np.float64), eps), eps
 
 
-@pytest.mark.parametrize("form", ["fp16", "tf32"])
+@pytest.mark.parametrize("form", ["fp16", "tf32", "bf16x3"])
 def test_scaling_and_offsets(hj, form):
     """Offsets far from zero and a dim whose range dwarfs the others (FP16
     subnormal residuals)."""
@@ -151,15 +151,13 @@ def test_unsupported_combinations(hj):
         hj.self_join_count(x, 0.05, form="fp16", centring="block")
     y = tight_clusters(2000, 8, 1)
     with pytest.raises(hj.HJError):
-        hj.self_join_count(y, 0.05, form="bf16x3", centring="block")
-    with pytest.raises(hj.HJError):
         hj.self_join_count(y, 0.05, form="fp16", centring=7)
     # the plain form ignores the option
     assert hj.self_join_count(y, 0.05, form="plain", centring="block") == \
         oracle.self_count_brute(y.astype(np.float64), 0.05)
 
 
-@pytest.mark.parametrize("form", ["fp16", "tf32"])
+@pytest.mark.parametrize("form", ["fp16", "tf32", "bf16x3"])
 def test_estimates_all_pairs_loose_bound(hj, form):
     """Every pair estimated (one cell): the error stays within the bound of
     the residual model with the loosest residual, the diameter of the data's
@@ -174,9 +172,11 @@ def test_estimates_all_pairs_loose_bound(hj, form):
         half = 0.5 * (both.max(0) - both.min(0))
         R = float(np.sqrt((half ** 2).sum()))  # |c| <= R (centres inside the box)
         H = 2.0 * R                             # |h| <= diameter of the box
-        g, kstep = (8, 16) if form == "fp16" else (4, 8)
+        g, kstep = (4, 8) if form == "tf32" else (8, 16)
         dp = -(-(d + 3) // g) * g                 # block width of the operand rows
         kpad = -(-(3 * dp) // kstep) * kstep      # product terms the MMAs sum
+        if form == "bf16x3":
+            kpad *= 3                             # three products per K step
         S = 1.5 * (H * H + 2 * H * R)           # cross terms and the folded q / 2
         rho = 2 * 2.0 ** -11 * H
         bound = 2 * kpad * 2.0 ** -22 * S + 2 * rho * np.sqrt(ex) + rho * rho + 1e-5 * (1 + ex)
