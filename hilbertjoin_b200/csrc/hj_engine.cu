@@ -319,10 +319,10 @@ static int ensure_plain_tiles(Ctx *c, cudaStream_t st, SortedSet *s, bool is_b, 
     return check_cuda("plain layout");
 }
 
-// Per-block-centred FP16 / TF32 operands of a sorted set (HJ_CENTRING_BLOCK):
-// the operand rows whose windows serve as A and as B, q and |h| per rank,
-// block summaries and centres. scale = the FP16 form's operand scale times
-// 2^-kBcScaleShift (the largest coordinate below 2^10, for both forms).
+// Per-block-centred operands of a sorted set (HJ_CENTRING_BLOCK; FP16, TF32 or
+// BF16 hi + lo): the operand rows whose windows serve as A and as B, q and |h|
+// per rank, block summaries and centres. scale = the FP16 form's operand scale
+// times 2^-kBcScaleShift (the largest coordinate below 2^10, every form).
 static int prepare_block_centring(Ctx *c, cudaStream_t st, SortedSet *s, bool is_b, const double *center,
                                   double scale, int form, int *launches) {
     const uint64_t npad = s->npad_tc, nblk = npad / kBcBlock;
@@ -577,8 +577,8 @@ static int run_join(Ctx *c, const JoinIn &in, const hj_opts *opts, uint64_t *cou
         cudaEventRecord(c->ev[5], st);
     } else {
         // Operand centring: one global centre, or a centre per 128-rank block
-        // (FP16 form, d <= 64) when asked for, or when the global centre would
-        // send more than an eighth of the block pairs to the FP64 kernel.
+        // (d <= 64) when asked for, or when the global centre would send more
+        // than an eighth of the block pairs to the FP64 kernel.
         const int centring = opts ? opts->tc_centring : HJ_CENTRING_AUTO;
         const bool bc_ok = d <= kBcMaxDim;  // every tensor-core form
         // block-centred operands of both forms: the largest coordinate below 2^10

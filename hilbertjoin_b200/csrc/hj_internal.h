@@ -119,16 +119,16 @@ struct SortedSet {
     float *bc_cent = nullptr;     // per block: c in FP32 (FP16 values), kBcCentStride floats, zero padded
 };
 
-// Per-block centring of the FP16 (or TF32, or BF16 hi + lo) operands. Every 128-rank block of
-// a sorted set (one A tile, half a B tile) gets a centre c whose coordinates
-// are FP16 (or TF32) values in the operand units ((x - center) * scale, the
-// largest coordinate below 2^10), the midpoint of the block's range rounded;
-// every rank is stored as that centre plus its residual h = fl(x - c),
-// rounded to the operand type. With q = |h|^2 + 2 h.c
-// per rank and three pieces of q / 2 (FP16: m1 2^15 + m2 2^4 + m3 2^-7; TF32:
-// m1 + m2 + m3; to 2^-33 |q|), a row holds four blocks of dp = roundup(d + 3,
-// 8) columns (TF32: roundup(d + 3, 4); zero padded),
-//     [h | h | c m1 m2 m3 | h a1 a2 a3],   (a1, a2, a3) = (-2^15, -2^4, -2^-7) (TF32: -1, -1, -1),
+// Per-block centring of the tensor-core operands (FP16, TF32, or BF16 hi + lo
+// pairs). Every 128-rank block of a sorted set (one A tile, half a B tile) gets
+// a centre c whose coordinates are values of the operand type in the operand
+// units ((x - center) * scale, the largest coordinate below 2^10), the
+// midpoint of the block's range rounded; every rank is stored as that centre
+// plus its residual h = fl(x - c), rounded to the operand type. With
+// q = |h|^2 + 2 h.c per rank and three pieces of q / 2 (FP16: m1 2^15 +
+// m2 2^4 + m3 2^-7; TF32 and BF16: m1 + m2 + m3; to 2^-33 |q|), a row holds four
+// blocks of dp = roundup(d + 3, 8) columns (TF32: roundup(d + 3, 4); zero padded),
+//     [h | h | c m1 m2 m3 | h a1 a2 a3],   (a1, a2, a3) = (-2^15, -2^4, -2^-7) (else -1, -1, -1),
 // and the operands are two windows of 3 dp columns of the same rows:
 //     B = columns [0, 3dp) = [h | h | c m],   A = columns [dp, 4dp) = [h | c m | h a].
 // Column by column the products are h_i.h_j, c_i.h_j (m_i meets B's zero pad),
@@ -138,8 +138,9 @@ struct SortedSet {
 // (The A window's last atom reaches past the row end: the TMA fills zeros.)
 // The accumulator alone orders the columns of a row (no per-column norm), so
 // the epilogue's maximum over 32 columns is exact. The only rounding of the
-// points is h's (relative 2^-11 per coordinate): it moves a point by
-// rho <= 2^-11 |h| (plus the subnormal floor), and distances by rho_i + rho_j.
+// points is h's (relative 2^-11 per coordinate for FP16 and TF32, 2^-18 for the
+// BF16 pair): it moves a point by rho <= 2^-11 |h| (plus the subnormal floor),
+// and distances by rho_i + rho_j.
 // The error bound (bc_tau) is therefore linear in the residual norms instead
 // of quadratic in the distance from one global centre, which keeps clustered
 // data with eps far below its spread on the tensor cores.
