@@ -138,6 +138,10 @@ def _opts(form, active_dims, ref_compat, device, stream, shard=None, reorder_dim
           centring="auto") -> Opts:
     o = Opts()
     lib().hj_opts_init(ctypes.byref(o))
+    if isinstance(form, str) and form not in FORMS:
+        raise ValueError(f"unknown form {form!r}: one of {sorted(FORMS)}")
+    if isinstance(centring, str) and centring not in CENTRINGS:
+        raise ValueError(f"unknown centring {centring!r}: one of {sorted(CENTRINGS)}")
     o.form = FORMS[form] if isinstance(form, str) else int(form)
     o.active_dims = -1 if active_dims is None else int(active_dims)
     o.ref_compat = int(bool(ref_compat))
@@ -203,8 +207,13 @@ def join_count(a, b, eps: float, form="plain", active_dims=None, ref_compat=Fals
     """Number of ordered pairs (p in a, q in b) with |p-q| <= eps."""
     o = Stats()
     c = ctypes.c_uint64(0)
+    if _is_torch_cuda(a) != _is_torch_cuda(b):
+        raise ValueError("a and b must both be CUDA tensors or both host arrays")
     if _is_torch_cuda(a):
+        import torch
         xa, xb = a.contiguous(), b.contiguous()
+        if xa.dim() != 2 or xb.dim() != 2 or xa.dtype not in (torch.float32, torch.float64):
+            raise ValueError("a and b must be 2-D float32/float64 tensors")
         if xa.dtype != xb.dtype or xa.shape[1] != xb.shape[1]:
             raise ValueError("a and b must have the same dtype and dimension")
         opts = _opts(form, active_dims, ref_compat, xa.device.index if device is None else device,
