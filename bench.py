@@ -596,11 +596,12 @@ def main():
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
-        if fixture is not None and counts[0] != fixture:
-            raise SystemExit(f"count {counts[0]} differs from the oracle's {fixture} for this workload")
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+    # after the ranks have left the process group, so that none waits on a rank that stopped
+    if fixture is not None and counts[0] != fixture:
+        raise SystemExit(f"count {counts[0]} differs from the oracle's {fixture} for this workload")
 
 
 if __name__ == "__main__":
