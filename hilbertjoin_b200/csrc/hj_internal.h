@@ -138,7 +138,7 @@ struct SortedSet {
 // (The A window's last atom reaches past the row end: the TMA fills zeros.)
 // The accumulator alone orders the columns of a row (no per-column norm), so
 // the epilogue's maximum over 32 columns is exact. The only rounding of the
-// points is h's (relative 2^-11 per coordinate for FP16 and TF32, 2^-18 for the
+// points is h's (relative 2^-11 per coordinate for FP16 and TF32, 2^-17 for the
 // BF16 pair): it moves a point by rho <= 2^-11 |h| (plus the subnormal floor),
 // and distances by rho_i + rho_j.
 // The error bound (bc_tau) is therefore linear in the residual norms instead

@@ -974,7 +974,9 @@ uint32_t tc_kterms(int form, uint32_t kcols) { return tc_ksteps(form, kcols) * (
 //   theta_t: the FP64 pair test sums d squares of exact differences with FMAs,
 //     relative error below (d + 2) 2^-53 of dist2 ~ eps^2: 2 (d + 2) 2^-53 T.
 BcConsts bc_constants(int form, uint32_t d, double T, double op_scale) {
-    // BF16x3: three MMAs per K step; the dropped lo.lo products are below 2^-18 S
+    // BF16x3: three MMAs per K step. A BF16 value has 8 significant bits, so
+    // |lo| <= 2^-8 |v| and the dropped lo.lo products stay below 2^-16 S
+    // (1.001 covers S being taken over the stored hi + lo), doubled for s.
     const double s2 = op_scale * op_scale,
                  kpad = (double)tc_kterms(form, bc_cols(d, form)) * (form == HJ_FORM_TC_BF16X3 ? 3.0 : 1.0);
     auto up = [](double v) {
@@ -982,10 +984,12 @@ BcConsts bc_constants(int form, uint32_t d, double T, double op_scale) {
         return (double)f >= v ? f : std::nextafter(f, INFINITY);
     };
     BcConsts k;
-    k.kp21 = up(2.0 * kpad * std::ldexp(1.0, -22) + (form == HJ_FORM_TC_BF16X3 ? 2.0 * std::ldexp(1.0, -18) : 0.0));
+    k.kp21 = up(2.0 * kpad * std::ldexp(1.0, -22) +
+                (form == HJ_FORM_TC_BF16X3 ? 2.0 * 1.001 * std::ldexp(1.0, -16) : 0.0));
     k.eps = up(std::sqrt(T * s2) * (1.0 + 1e-12));
-    // FP16 / TF32 round once to 11 significant bits; the BF16 hi + lo pair keeps v to 2^-18
-    k.rho_u = up(1.001 * std::ldexp(1.0, form == HJ_FORM_TC_BF16X3 ? -18 : -11));
+    // FP16 / TF32 round once to 11 significant bits; the BF16 hi + lo pair keeps v
+    // to 2^-17 (hi to 2^-8 |v|, and lo to half a unit of the last of its 8 bits)
+    k.rho_u = up(1.001 * std::ldexp(1.0, form == HJ_FORM_TC_BF16X3 ? -17 : -11));
     // the subnormal spacing of the operand type (half of it per rounding: FP16
     // 2^-25, TF32 2^-150) and the FP64 shift of coordinates below 2^10 (2^-52 of
     // 2^10, generously 2^-37)

@@ -1138,7 +1138,7 @@ template <> struct BcElem<0> {  // TF32
     }
 };
 template <> struct BcElem<1> {  // BF16 hi + lo (BF16x3): hi in the low 16 bits, lo in the high 16 bits;
-    using E = uint32_t;         // the stored value hi + lo is within 2^-18 of v
+    using E = uint32_t;         // the stored value hi + lo is within 2^-17 |v| of v
     __device__ static E round(double v, double *back) {
         const __nv_bfloat16 hi = __double2bfloat16(v);
         const double h = (double)__bfloat162float(hi);

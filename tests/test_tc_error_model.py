@@ -134,3 +134,30 @@ def test_fp16_subnormal_absolute_error():
     err = np.abs(v.astype(np.float16).astype(np.float64) - v)
     assert err.max() <= 2.0 ** -25
     assert err.max() > 0.9 * 2.0 ** -25
+
+
+def rn_sig_bits(v, p):
+    """v rounded to nearest (ties to even) to p significant bits (FP64 emulation)."""
+    m, e = np.frexp(v)
+    return np.ldexp(np.rint(np.ldexp(m, p)), e - p)
+
+
+def test_bf16_pair_from_fp64_keeps_17_bits():
+    """The block-centred BF16x3 operands: hi = bf16(v), lo = bf16(v - hi) from
+    FP64. The pair keeps v to 2^-17 |v| (the rho_u of that form), and
+    |lo| <= 2^-8 |v|, so a dropped lo*lo product is below 2^-16 of |v w|."""
+    rng = np.random.default_rng(17)
+    n = 1_000_000
+    v = rng.uniform(-1, 1, n) * np.ldexp(1.0, rng.integers(-20, 10, n))
+    w = rng.uniform(-1, 1, n) * np.ldexp(1.0, rng.integers(-20, 10, n))
+    vh = rn_sig_bits(v, 8)
+    vl = rn_sig_bits(v - vh, 8)
+    wh = rn_sig_bits(w, 8)
+    wl = rn_sig_bits(w - wh, 8)
+    res = np.abs(v - vh - vl) / np.abs(v)
+    assert res.max() <= 2.0 ** -17 and res.max() > 0.9 * 2.0 ** -17
+    lolo = np.abs(vl * wl) / np.abs((vh + vl) * (wh + wl))
+    assert lolo.max() <= 1.001 * 2.0 ** -16 and lolo.max() > 0.9 * 2.0 ** -16
+    # the emulation is CUDA's rounding for values in BF16's normal range
+    x32 = v.astype(np.float32)
+    assert np.array_equal(rn_sig_bits(x32.astype(np.float64), 8), bf16_rn(x32).astype(np.float64))
