@@ -79,7 +79,7 @@ typedef enum {
     HJ_FORM_TC_FP16 = 4
 } hj_form;
 
-/* Operand centring of the FP16 tensor-core form (hj_opts.tc_centring). */
+/* Operand centring of the tensor-core forms (hj_opts.tc_centring). */
 typedef enum {
     /* HJ_CENTRING_BLOCK when, with one global centre, more than an eighth of
      * the block pairs would run on the FP64 kernel (the norm expansion's
