@@ -341,7 +341,7 @@ typedef struct {
                                      requests (same dtype, within the budget) and runs them as one
                                      batch (hj_batch_*: one persistent launch); 0 or 1 = one
                                      request per worker */
-    int32_t block_centring;       /* 0: the requests' FP16 joins use one global centre
+    int32_t block_centring;       /* 0: the requests' tensor-core joins use one global centre
                                      (HJ_CENTRING_GLOBAL); nonzero: HJ_CENTRING_AUTO, and admission
                                      counts the block-centred operands and band queue of every
                                      request that could use them (d <= 64) */
