@@ -73,7 +73,7 @@ struct Request {
 struct hj_server {
     hj_server_opts opts{};
     int device = 0;
-    int centring = HJ_CENTRING_GLOBAL;  // of the requests' FP16 joins (hj_server_opts.block_centring)
+    int centring = HJ_CENTRING_GLOBAL;  // of the requests' tensor-core joins (hj_server_opts.block_centring)
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<uint64_t> queue;
