@@ -1,8 +1,9 @@
 #!/usr/bin/env bash
 # Builds the hilbertJoin reference from its own sources (read in place under
-# REF_DIR, default /root/reference) into oracle/_ref/, for use as a parity
-# oracle and as the CPU baseline. Nothing from the reference is copied into
-# this repository; only the binaries land in oracle/_ref/ (git-ignored).
+# REF_DIR, default: the directory `reference` beside this repository) into
+# oracle/_ref/, for use as a parity oracle and as the CPU baseline. Nothing
+# from the reference is copied into this repository; only the binaries land in
+# oracle/_ref/ (git-ignored).
 #
 # The reference needs MKL (only for its default data generator) and Boost
 # lockfree (only for its dead pair-queue path); oracle/shim/ stands in for both.
@@ -13,7 +14,7 @@
 # so one binary per (KBLOCK, NUM_THREADS) pair is built.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF_DIR="${REF_DIR:-/root/reference}"
+REF_DIR="${REF_DIR:-$(cd "$HERE/../.." && pwd)/reference}"
 OUT="$HERE/_ref"
 if [ ! -f "$REF_DIR/hilbertjoin/egojoin.cpp" ]; then
     echo "reference sources not found under $REF_DIR; skipping" >&2
