@@ -161,3 +161,45 @@ def test_bf16_pair_from_fp64_keeps_17_bits():
     # the emulation is CUDA's rounding for values in BF16's normal range
     x32 = v.astype(np.float32)
     assert np.array_equal(rn_sig_bits(x32.astype(np.float64), 8), bf16_rn(x32).astype(np.float64))
+
+
+@pytest.mark.parametrize("form", ["bf16x3", "tf32", "fp16"])
+@pytest.mark.parametrize("d", [3, 28, 64, 256])
+def test_global_centre_operand_terms(form, d):
+    """The one-centre forms without the accumulation term: centred FP64 values,
+    FP32 norms, operands as the gather writes them (TF32 and BF16 from the FP32
+    value, FP16 from FP64 after an exact power-of-two scale), products summed
+    exactly. |s - dist2| stays within the operand part of c_rel (|a|^2 + |b|^2):
+    1.25 (p + 14 2^-24 + d 2^-50) with p = 2 2^-11 + 2^-22 (TF32, FP16) or
+    3.1 2^-16 (BF16x3)."""
+    rng = np.random.default_rng(d + {"bf16x3": 0, "tf32": 1000, "fp16": 2000}[form])
+    n = 300
+    x = rng.standard_normal((n, d)) * np.ldexp(1.0, rng.integers(-3, 4, d)) + rng.uniform(-50, 50, d)
+    c = x - (0.5 * x.min(0) + 0.5 * x.max(0))
+    if form == "fp16":
+        s_exp = 14 - int(np.floor(np.log2(np.abs(c).max())))
+        c = np.ldexp(c, s_exp)  # exact
+        ops = (c.astype(np.float16).astype(np.float64),)
+    else:
+        f = c.astype(np.float32)
+        if form == "tf32":
+            ops = (tf32_rn(f).astype(np.float64),)
+        else:
+            hi = bf16_rn(f)
+            ops = (hi.astype(np.float64), bf16_rn(f - hi).astype(np.float64))
+    norms = (c * c).sum(1).astype(np.float32).astype(np.float64)
+    if len(ops) == 1:
+        dot = ops[0] @ ops[0].T
+    else:
+        hi, lo = ops
+        dot = hi @ hi.T + hi @ lo.T + lo @ hi.T
+    s = norms[:, None] + norms[None, :] - 2 * dot
+    ex = ((c[:, None, :] - c[None, :, :]) ** 2).sum(-1)
+    u24 = 2.0 ** -24
+    p = 2 * 2.0 ** -11 + 2.0 ** -22 if form != "bf16x3" else 3.1 * 2.0 ** -16
+    c_rel = 1.25 * (p + 2 * u24 + 12 * u24 + d * 2.0 ** -50)
+    bound = c_rel * (norms[:, None] + norms[None, :])
+    ratio = np.abs(s - ex) / bound
+    print(f"{form} d={d}: max |s - dist2| / operand bound = {ratio.max():.3f}")
+    assert ratio.max() <= 1.0, float(ratio.max())
+    assert ratio.max() > 0.01  # the operand part is not vacuous
