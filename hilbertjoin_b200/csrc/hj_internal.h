@@ -139,8 +139,8 @@ struct SortedSet {
 // The accumulator alone orders the columns of a row (no per-column norm), so
 // the epilogue's maximum over 32 columns is exact. The only rounding of the
 // points is h's (relative 2^-11 per coordinate for FP16 and TF32, 2^-17 for the
-// BF16 pair): it moves a point by rho <= 2^-11 |h| (plus the subnormal floor),
-// and distances by rho_i + rho_j.
+// BF16 pair): it moves a point by rho <= 2^-11 |h| (2^-17 |h| for the pair; plus
+// the subnormal floor), and distances by rho_i + rho_j.
 // The error bound (bc_tau) is therefore linear in the residual norms instead
 // of quadratic in the distance from one global centre, which keeps clustered
 // data with eps far below its spread on the tensor cores.
