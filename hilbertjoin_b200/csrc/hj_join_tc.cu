@@ -991,10 +991,12 @@ BcConsts bc_constants(int form, uint32_t d, double T, double op_scale) {
     // to 2^-17 (hi to 2^-8 |v|, and lo to half a unit of the last of its 8 bits)
     k.rho_u = up(1.001 * std::ldexp(1.0, form == HJ_FORM_TC_BF16X3 ? -17 : -11));
     // the subnormal spacing of the operand type (half of it per rounding: FP16
-    // 2^-25, TF32 2^-150) and the FP64 shift of coordinates below 2^10 (2^-52 of
-    // 2^10, generously 2^-37)
-    const double floor_abs =
-        (form == HJ_FORM_TC_FP16 ? std::ldexp(1.0, -25) : std::ldexp(1.0, -140)) + std::ldexp(1.0, -37);
+    // 2^-25, BF16 2^-134, TF32 2^-150, taken as 2^-140) and the FP64 shift of
+    // coordinates below 2^10 (2^-52 of 2^10, generously 2^-37)
+    const double sub = form == HJ_FORM_TC_FP16     ? std::ldexp(1.0, -25)
+                       : form == HJ_FORM_TC_BF16X3 ? std::ldexp(1.0, -134)
+                                                   : std::ldexp(1.0, -140);
+    const double floor_abs = sub + std::ldexp(1.0, -37);
     k.rho_c = up(2.0 * std::sqrt((double)d) * floor_abs);
     k.u_norm = up(std::ldexp(1.0, -23) + std::ldexp(1.0, -33));
     k.u_d = up(16.0 * std::ldexp(1.0, -24));
