@@ -172,3 +172,94 @@ def test_bf16x3_windows_within_the_pair_bound(d):
         # before the correction) are exceeded by some pairs
         old = rho * np.sqrt(ex) + (rho / 2) ** 2 + 2 * 2.0 ** -18 * S + 1e-9 * (1 + ex)
         assert (np.abs(s - ex) > old).any()
+
+
+def _trunc(x, e):
+    unit = np.ldexp(1.0, e - 24)
+    return np.trunc(x / unit) * unit
+
+
+def _mma_model(acc, prods):
+    """One tensor-core step of the accumulation model (Fasi et al. 2021): the
+    accumulator and the exact products aligned to the largest exponent and
+    truncated to 24 bits, summed, the sum truncated to FP32."""
+    terms = np.concatenate([acc[..., None], prods], axis=-1)
+    _, e = np.frexp(np.abs(terms).max(-1))
+    tot = _trunc(terms, e[..., None]).sum(-1)
+    _, e2 = np.frexp(np.abs(tot))
+    return _trunc(tot, e2)
+
+
+def _bc_tau_model(form, d, dp, eps_op, xa, ca, pa, xb, cb, qb, D):
+    """bc_constants and bc_tau restated (FP64 here; the kernel rounds the
+    constants up to FP32)."""
+    cols = 3 * dp
+    K = -(-cols // 16) * 16 * (3 if form == "bf16x3" else 1)
+    kp21 = 2 * K * 2.0 ** -22 + (2 * 1.001 * 2.0 ** -16 if form == "bf16x3" else 0.0)
+    rho_u = 1.001 * 2.0 ** (-17 if form == "bf16x3" else -11)
+    floor = (2.0 ** -25 if form == "fp16" else 2.0 ** -134) + 2.0 ** -37
+    rho_c = 2 * np.sqrt(d) * floor
+    u_norm, u_d = 2.0 ** -23 + 2.0 ** -33, 16 * 2.0 ** -24
+    theta = 2 * (d + 2) * 2.0 ** -53 * eps_op ** 2 + 2.0 ** -29
+    S = xa * (xb + cb) + ca * xb + 0.5005 * qb
+    rho = rho_u * (xa + xb) + 2 * rho_c
+    E = kp21 * S + u_norm * (pa + qb) + u_d * D
+    return 1.25 * (2 * E + 2 * eps_op * rho + 2 * rho * rho + theta)
+
+
+@pytest.mark.parametrize("form", ["fp16", "bf16x3"])
+@pytest.mark.parametrize("d", [3, 28, 64])
+def test_emulated_kernel_classification_is_sound(form, d):
+    """End to end under the accumulation model: the block-centred rows, the
+    MMAs emulated step by step (16 products per step; BF16x3 as hi.hi, hi.lo,
+    lo.hi per K step into one accumulator), s in FP32 terms, and the band
+    half-width tau of bc_constants / bc_tau. Every pair the band calls certain
+    ("s + tau <= eps^2" inside, "s - tau > eps^2" outside) is on that side of
+    eps^2 by the exact distance, and most pairs near eps are certain."""
+    rng = np.random.default_rng(7 * d + (form == "bf16x3"))
+    k = 2
+    means = rng.random((k, d))
+    lab = np.repeat(np.arange(k), 128)
+    x = means[lab] + 0.004 * rng.standard_normal((lab.size, d))
+    if form == "fp16":
+        X, R, q, cent, dp = bc_rows(x)
+        Rh, Rl = R, np.zeros_like(R)
+    else:
+        X, Rh, Rl, q, cent, dp = bc_rows_bf16(x)
+    n = x.shape[0]
+    cols = 3 * dp
+    K = -(-cols // 16) * 16
+    pad = np.zeros((Rh.shape[0], K + 64))
+    Rh, Rl = np.concatenate([Rh, pad], 1), np.concatenate([Rl, pad], 1)
+    Ah, Al = Rh[:n, dp:dp + K], Rl[:n, dp:dp + K]
+    Bh, Bl = Rh[:n, 0:K], Rl[:n, 0:K]
+    passes = [(Ah, Bh)] if form == "fp16" else [(Ah, Bh), (Ah, Bl), (Al, Bh)]
+    w = np.zeros((n, n))
+    for s0 in range(0, K, 16):
+        for P, Q in passes:
+            prods = P[:, None, s0:s0 + 16] * Q[None, :, s0:s0 + 16]  # exact in FP64
+            w = _mma_model(w, prods)
+    bi = np.arange(n) // 128
+    cA = cent[bi]
+    D = ((cA[:, None, :] - cA[None, :, :]) ** 2).sum(-1)
+    q32 = q[:n].astype(np.float32).astype(np.float64)
+    s = q32[:, None] + D.astype(np.float32).astype(np.float64) - 2 * w
+    ex = ((X[:, None, :] - X[None, :, :]) ** 2).sum(-1)
+    h = X - cA
+    hn = np.sqrt((h * h).sum(1))
+    cn = np.sqrt((cent * cent).sum(1))
+    qa = np.abs(q[:n])
+    blocks = n // 128
+    xb = np.array([hn[b * 128:(b + 1) * 128].max() for b in range(blocks)])[bi]
+    qb = np.array([qa[b * 128:(b + 1) * 128].max() for b in range(blocks)])[bi]
+    same = bi[:, None] == bi[None, :]
+    eps2 = float(np.quantile(ex[same & (ex > 0)], 0.3))  # many pairs near eps
+    eps_op = np.sqrt(eps2)
+    tau = _bc_tau_model(form, d, dp, eps_op, hn[:, None], cn[bi][:, None], qa[:, None], xb[None, :],
+                        cn[bi][None, :], qb[None, :], D)
+    inside = s + tau <= eps2
+    outside = s - tau > eps2
+    assert not (inside & (ex > eps2)).any()
+    assert not (outside & (ex <= eps2)).any()
+    near = np.abs(ex - eps2) < 0.5 * eps2
+    assert (inside | outside)[near].mean() > 0.5, float((inside | outside)[near].mean())
